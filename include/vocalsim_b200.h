@@ -1,0 +1,227 @@
+/*
+ * vocalsim_b200.h -- C ABI of the B200 2.5D FDTD vocal-tract solver.
+ *
+ * The reference project (Debasishray19/VocalSim-2p5D-FDTD) exposes its time
+ * stepping path as C++ classes: SimulationParams -> FDTDSolver::setupWaveSolver
+ * -> FDTDEngineCPU / FDTDEngineEigen::startSolverEngine.  This header is the
+ * plain-C boundary that replaces that path.  Every entry point below names the
+ * reference interface it stands in for (file:line inside the reference tree).
+ *
+ * Conventions
+ *   - Every function returns a vs_status (0 = ok).  vs_last_error() gives text.
+ *   - The caller owns every host buffer passed in; a solver/batch handle owns
+ *     its device memory.  One handle must not be used from two host threads at
+ *     once; distinct handles are independent.
+ *   - Frame arrays are row-major frameH x frameW (row 0 = top, as in the
+ *     reference's PV_N[row * frameW + col]).
+ *   - Nothing here falls back to the CPU: when no CUDA device is present the
+ *     device entry points return VS_ERR_CUDA.  vs_build_maps() is host-only.
+ */
+#ifndef VOCALSIM_B200_H_
+#define VOCALSIM_B200_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VS_ABI_VERSION 1
+
+typedef enum vs_status {
+    VS_OK               = 0,
+    VS_ERR_INVALID_ARG  = 1,  /* bad pointer, size or enum value                 */
+    VS_ERR_GEOMETRY     = 2,  /* area function unusable (empty, area <= 0, ...)  */
+    VS_ERR_CUDA         = 3,  /* CUDA runtime / launch error, or no device       */
+    VS_ERR_TIMEOUT      = 4,  /* a bounded device wait gave up                   */
+    VS_ERR_NONFINITE    = 5,  /* NaN/Inf detected in the listener trace          */
+    VS_ERR_ALLOC        = 6,  /* host or device allocation failed                */
+    VS_ERR_UNSUPPORTED  = 7,  /* option outside the implemented scope            */
+    VS_ERR_NEGATIVE_SQRT= 8   /* depth formula met a negative radicand; the
+                                 reference traps here (TubeDepth.cu:273-288)     */
+} vs_status;
+
+/* Cell type codes, identical to the reference enum CellTypes
+ * (include/SolverParams.h:21-35). */
+enum {
+    VS_CELL_WALL = 0, VS_CELL_AIR = 1, VS_CELL_EXCITATION = 2,
+    VS_CELL_PML0 = 3, VS_CELL_PML1 = 4, VS_CELL_PML2 = 5, VS_CELL_PML3 = 6,
+    VS_CELL_PML4 = 7, VS_CELL_PML5 = 8, VS_CELL_DYNAMIC = 9, VS_CELL_DEAD = 10,
+    VS_CELL_NOPRESSURE = 11, VS_CELL_HEAD = 12
+};
+
+/* Source types, as FDTDSolver::source_type (FDTDSolver.cu:80,
+ * GlottalExcitations.cu:17-44).  VS_SRC_GAUSS_STD is an addition: the same
+ * Gaussian written with a standard deviation, exp(-(t-tp)^2 / (2 s^2)). */
+enum { VS_SRC_SINE = 0, VS_SRC_GAUSS = 1, VS_SRC_TMM = 2, VS_SRC_GAUSS_STD = 3 };
+
+/* Engine arithmetic.  Both reference engines run the same update; they round
+ * the pressure denominator differently: FDTDEngineCPU.cpp:330 uses
+ * (1 + sigma) * dP, FDTDEngineEigen.cpp:251 uses sigma * dP + dP. */
+enum { VS_ENGINE_CPU = 1, VS_ENGINE_EIGEN = 2 };
+
+/* Listener placement. */
+enum { VS_LISTENER_REFERENCE = 0, VS_LISTENER_EXPLICIT = 1 };
+
+/* Run parameters.  Replaces SimulationParams(10 args) (SimulationParams.cu:36-57)
+ * plus the constants the reference hard-codes (SimulationParams.cu:7-34,
+ * GlottalExcitations.cu:19-32, TwoMassModel.cpp:52, FDTDSolver.cu:614).
+ * vs_params_init() fills every field with the reference's value. */
+typedef struct vs_params {
+    int32_t fdtd_solver_type;      /* 0 = 2D, 1 = 2.5D                                   */
+    int32_t simulation_type;       /* 0 = open space (43 x 341 domain), 1 = tube         */
+    int32_t cross_sectional_shape; /* 1 = circular, 2 = elliptical 3:1                   */
+    int32_t mouth_radiation_cond;  /* 0 = open end, 1 = Dirichlet p = 0 column           */
+    int32_t srate_mul;             /* fs = 44100 * srate_mul                             */
+    int32_t source_type;           /* VS_SRC_*                                           */
+    int32_t pml_flag;              /* 0 = off, 1 = six graded PML layers                 */
+    int32_t engine;                /* VS_ENGINE_*                                        */
+    float   audio_dur;             /* seconds; sets num_steps when num_steps <= 0        */
+    int32_t pad0;
+    int64_t num_steps;             /* > 0: explicit step count (overrides audio_dur)     */
+    /* sources */
+    float   gauss_peak_s;          /* reference: 0.646f / 10 kHz                          */
+    float   gauss_width_s;         /* reference form: width w in exp(-((t-tp)/w)^2)       */
+    float   gauss_amp;             /* reference: 0.025                                    */
+    float   sine_freq_hz;          /* reference: 440                                      */
+    float   sine_amp;              /* reference: 25                                       */
+    float   tmm_ps_pa;             /* two-mass subglottal pressure; reference 686.46      */
+    /* walls */
+    float   mu3d;                  /* wall reflection parameter; <= 0 -> reference value
+                                      (0.025 in 2.5D, 0.005 in 2D; FDTDSolver.cu:614)   */
+    float   wall_coupling;         /* wall_pressure_coupling_coeff; reference 0          */
+    /* depth */
+    float   uniform_depth_m;       /* > 0: tube air cells get this depth before the
+                                      reference smoothing / clamp                        */
+    int32_t depth_fma;             /* 1: circular depth radicand r^2 - d^2 as one fused
+                                      multiply-add, as nvcc contracts the reference
+                                      kernel (TubeDepth.cu:355-370); 0: two roundings    */
+    /* listener */
+    int32_t listener_mode;         /* VS_LISTENER_*                                      */
+    int32_t listener_x, listener_y;/* used when listener_mode == VS_LISTENER_EXPLICIT    */
+    int32_t reserved[8];
+} vs_params;
+
+/* Area function: n sections of (length cm, area cm^2), the pairs the reference
+ * reads from the data/tube-geometry text files (TubeGeometry.cu:83-88). */
+typedef struct vs_geometry {
+    int32_t      n_sections;
+    int32_t      pad0;
+    const float* section_length_cm;
+    const float* section_area_cm2;
+} vs_geometry;
+
+/* Everything about a built grid that a caller needs to size buffers. */
+typedef struct vs_dims {
+    int32_t frame_h, frame_w;        /* FDTDSolver::frameH / frameW                     */
+    int32_t listener_x, listener_y;  /* FDTDSolver::listenerX / listenerY               */
+    int32_t excitation_x, excitation_y;
+    int32_t tube_length_cells;       /* TubeGeometry::tube_length_incells (0 open space)*/
+    int32_t tube_start_x, tube_end_x, tube_mid_y;
+    int64_t num_steps;               /* FDTDSolver::num_steps                           */
+    int64_t interior_cells;          /* (frameH-2) * (frameW-2)                         */
+    float   dt, ds;                  /* SimulationParams::dt / ds                       */
+    float   z_inv_val;               /* FDTDSolver.cu:617                               */
+    int32_t pad0;
+} vs_dims;
+
+typedef struct vs_solver vs_solver;
+typedef struct vs_batch  vs_batch;
+
+/* Library version (VS_ABI_VERSION). */
+int vs_version(void);
+
+/* Fill *p with the reference's defaults: 2.5D, tube, circular, open mouth,
+ * srate_mul 15, Gaussian source, PML on, FDTDEngineCPU arithmetic, 100 ms
+ * (main.cu:160-187 uses 100 ms; reference source constants from
+ * GlottalExcitations.cu:19-32 and TwoMassModel.cpp:52). */
+int vs_params_init(vs_params* p);
+
+/* Host-only: build the grid maps that FDTDSolver::setupWaveSolver produces
+ * (FDTDSolver.cu:289-476: TubeGeometry.cu:53-612, TubeDepth.cu:95-762,
+ * FDTDSolver.cu:553-649,816-857,1058-1070).  Any output pointer may be NULL.
+ * cell_type, depth_* and z_inv are frameH*frameW arrays; call once with all
+ * NULL to learn the dims.  cell_type matches the reference's GridCellComponents
+ * ::cell_type values; depths match depthP/X/Y; z_inv matches the z_inv map. */
+int vs_build_maps(const vs_params* p, const vs_geometry* g, vs_dims* dims,
+                  int32_t* cell_type, float* depth_p, float* depth_x,
+                  float* depth_y, float* z_inv);
+
+/* Host-only: the per-step excitation table of GlottalExcitations::
+ * setExcitationVelocity (GlottalExcitations.cu:9-52); zeros for the two-mass
+ * source, whose velocity is computed on the device each step. */
+int vs_source_table(const vs_params* p, int64_t num_steps, float* out);
+
+/* Build the grid and place it on the current CUDA device.  Replaces
+ * FDTDSolver(SimulationParams) + setupWaveSolver() + the engine constructor
+ * (FDTDSolver.cu:71-83,289-476; FDTDEngineCPU.cpp:4-103).  State starts at
+ * zero, as GridCellComponents initValue (FDTDSolver.cu:569). */
+int vs_create(const vs_params* p, const vs_geometry* g, vs_solver** out);
+
+/* Dims of a created solver. */
+int vs_get_dims(const vs_solver* s, vs_dims* dims);
+
+/* Advance `steps` time steps from the current state and write the listener
+ * pressure of each step to `trace` (a device pointer when trace_on_device is
+ * nonzero, else host memory).  Replaces FDTDEngineCPU::startSolverEngine
+ * (FDTDEngineCPU.cpp:222-304) and FDTDEngineEigen::startSolverEngine
+ * (FDTDEngineEigen.cpp:121-189); record_pressure[t] == trace[t]. */
+int vs_run(vs_solver* s, int64_t steps, float* trace, int trace_on_device);
+
+/* Zero the fields and the two-mass state and restart at step 0. */
+int vs_reset(vs_solver* s);
+
+/* Copy the current P, Vx, Vy frames (frameH*frameW floats each) to host
+ * buffers; NULL skips a field.  Stands in for the PV_N readback the reference
+ * uses for validation (FDTDEngineCPU.cpp:500-531). */
+int vs_get_fields(const vs_solver* s, float* p, float* vx, float* vy);
+
+/* Use this CUDA stream (a cudaStream_t) for every later call on s; NULL means
+ * the handle's own stream. */
+int vs_set_stream(vs_solver* s, void* cuda_stream);
+
+/* Release device memory and the handle.  Replaces FDTDEngineCPU::freeCUDAMemory
+ * (FDTDEngineCPU.cpp:199-219). */
+void vs_destroy(vs_solver* s);
+
+/* ---- batches: many independent tubes in one launch sequence ------------- */
+
+/* Build n tubes (params[i], geoms[i]) and pack them into one device arena.
+ * No reference counterpart: the reference runs one tube per process
+ * (main.cu:203-232). */
+int vs_batch_create(int32_t n, const vs_params* params, const vs_geometry* geoms,
+                    vs_batch** out);
+
+/* Dims of tube i of a batch. */
+int vs_batch_get_dims(const vs_batch* b, int32_t i, vs_dims* dims);
+
+/* Advance every tube `steps` time steps; traces is n x steps, row i = tube i.
+ * Each row equals what vs_run gives for that tube alone. */
+int vs_batch_run(vs_batch* b, int64_t steps, float* traces, int traces_on_device);
+
+/* Zero all fields and restart every tube at step 0. */
+int vs_batch_reset(vs_batch* b);
+
+/* Select the tile shape used by the step kernel (index into the compiled
+ * shape table, see vs_tile_shape) or -1 for the autotuned choice. */
+int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
+
+/* Time every compiled tile shape on `steps` steps and keep the fastest.  The
+ * state is reset afterwards.  best_index / best_ms may be NULL. */
+int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* best_ms);
+
+/* Number of compiled tile shapes, and the rows x cols of shape i. */
+int vs_tile_shape_count(void);
+int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
+
+void vs_batch_destroy(vs_batch* b);
+
+/* Last error text of this host thread (never NULL). */
+const char* vs_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOCALSIM_B200_H_ */

@@ -1,0 +1,203 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so) and of the
+reference pieces compiled from the reference tree (oracle/_ref/libvsref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, never by the solver package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+REPO = ORACLE_DIR.parent
+sys.path.insert(0, str(REPO / "vocalsim-2p5d-fdtd_b200" / "python"))
+from vocalsim_b200.abi import VsDims, VsGeometry, VsParams  # noqa: E402  (struct layout only)
+
+LIB = ORACLE_DIR / "_build" / "liboracle.so"
+REF_LIB = ORACLE_DIR / "_ref" / "libvsref.so"
+REFERENCE_TREE = Path("/root/reference")
+
+_orc = None
+_ref = None
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle (and the reference pieces when the tree is present)."""
+    if force or not LIB.exists():
+        subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+    if REFERENCE_TREE.exists() and (force or not REF_LIB.exists()):
+        subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "-f", "Makefile.ref",
+                        f"REF={REFERENCE_TREE}"], check=True)
+
+
+def lib() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        vp, vg, vd = C.POINTER(VsParams), C.POINTER(VsGeometry), C.POINTER(VsDims)
+        fp, dp, ip = C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int32)
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_params_init.argtypes = [vp]
+        L.orc_maps.argtypes = [vp, vg, vd, ip, ip, fp, fp, fp, fp, dp]
+        L.orc_coeffs.argtypes = [vp, vg, fp]
+        L.orc_consts.argtypes = [C.c_int, fp]
+        L.orc_tables.argtypes = [C.c_int, fp, fp, fp]
+        L.orc_step_count.argtypes = [C.c_float, C.c_float]
+        L.orc_step_count.restype = C.c_longlong
+        L.orc_source_f32.argtypes = [vp, C.c_longlong, fp]
+        L.orc_tmm_f32.argtypes = [C.c_float, C.c_int, fp, C.c_longlong, fp]
+        L.orc_tmm_f64.argtypes = [C.c_float, C.c_int, dp, C.c_longlong, dp]
+        L.orc_run_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, fp]
+        L.orc_run_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, dp]
+        _orc = L
+    return _orc
+
+
+def ref_lib() -> C.CDLL | None:
+    """The reference's own compiled pieces, or None when not built here."""
+    global _ref
+    if _ref is None:
+        if not REF_LIB.exists():
+            return None
+        L = C.CDLL(str(REF_LIB))
+        fp = C.POINTER(C.c_float)
+        L.vsref_tmm.argtypes = [C.c_int, fp, C.c_longlong, fp]
+        L.vsref_excitation.argtypes = [C.c_int, C.c_int, C.c_double, fp]
+        L.vsref_solver_tables.argtypes = [C.c_int, C.c_float, C.c_float, fp, fp, fp]
+        L.vsref_step_count.argtypes = [C.c_float, C.c_float]
+        L.vsref_step_count.restype = C.c_longlong
+        L.vsref_sim_params.argtypes = [C.c_int, fp]
+        _ref = L
+    return _ref
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"oracle {where}: status {rc}: {lib().orc_last_error().decode()}")
+
+
+def params(**kw) -> VsParams:
+    """Reference default parameters, with keyword overrides."""
+    p = VsParams()
+    lib().orc_params_init(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class Geometry:
+    """Owns the float32 arrays a VsGeometry points at."""
+
+    def __init__(self, length_cm, area_cm2):
+        self.length = np.ascontiguousarray(length_cm, dtype=np.float32)
+        self.area = np.ascontiguousarray(area_cm2, dtype=np.float32)
+        assert self.length.shape == self.area.shape
+        self.g = VsGeometry(len(self.length), 0, _fp(self.length), _fp(self.area))
+
+    def ref(self):
+        return C.byref(self.g)
+
+
+def maps(p: VsParams, g: Geometry | None):
+    d = VsDims()
+    gp = g.ref() if g is not None else None
+    _check(lib().orc_maps(C.byref(p), gp, C.byref(d), None, None, None, None, None, None, None), "maps")
+    n = d.frame_h * d.frame_w
+    t = np.zeros(n, np.int32); b = np.zeros(n, np.int32)
+    dP = np.zeros(n, np.float32); dX = np.zeros(n, np.float32); dY = np.zeros(n, np.float32)
+    z = np.zeros(n, np.float32)
+    margin = C.c_double(0)
+    ip = C.POINTER(C.c_int32)
+    _check(lib().orc_maps(C.byref(p), gp, C.byref(d), t.ctypes.data_as(ip), b.ctypes.data_as(ip),
+                          _fp(dP), _fp(dX), _fp(dY), _fp(z), C.byref(margin)), "maps")
+    shp = (d.frame_h, d.frame_w)
+    return dict(dims=d.as_dict(), cell_type=t.reshape(shp), bst=b.reshape(shp), depth_p=dP.reshape(shp),
+                depth_x=dX.reshape(shp), depth_y=dY.reshape(shp), z_inv=z.reshape(shp),
+                scan_margin=margin.value)
+
+
+COEFF_NAMES = ["N_out", "N_in", "minVxBeta", "minVyBeta", "maxVxSigmaPrimedt", "maxVySigmaPrimedt",
+               "betaVxSqr_dt_inv_rho_inv_ds", "betaVySqr_dt_inv_rho_inv_ds", "pressureSigmaPrimedt",
+               "areWeNotExcitationVx", "areWeNotExcitationVy", "excitationWeightVx",
+               "excitationWeightVy", "xor_val1", "xor_val2", "xor_val3", "xor_val4"]
+
+
+def coeffs(p: VsParams, g: Geometry | None) -> dict:
+    m = maps(p, g)
+    H, W = m["dims"]["frame_h"], m["dims"]["frame_w"]
+    out = np.zeros(17 * (H - 2) * (W - 2), np.float32)
+    _check(lib().orc_coeffs(C.byref(p), g.ref() if g is not None else None, _fp(out)), "coeffs")
+    out = out.reshape(17, H - 2, W - 2)
+    return {k: out[i] for i, k in enumerate(COEFF_NAMES)}
+
+
+def run(p: VsParams, g: Geometry | None, steps: int, precision: str = "f32", fields: bool = False):
+    """Trace (and optionally final P/Vx/Vy frames) of `steps` steps from rest."""
+    m = maps(p, g)["dims"]
+    n = m["frame_h"] * m["frame_w"]
+    gp = g.ref() if g is not None else None
+    if precision == "f32":
+        tr = np.zeros(steps, np.float32)
+        F = [np.zeros(n, np.float32) for _ in range(3)] if fields else [None] * 3
+        _check(lib().orc_run_f32(C.byref(p), gp, steps, _fp(tr), *[(_fp(a) if a is not None else None) for a in F]),
+               "run_f32")
+    else:
+        tr = np.zeros(steps, np.float64)
+        F = [np.zeros(n, np.float64) for _ in range(3)] if fields else [None] * 3
+        _check(lib().orc_run_f64(C.byref(p), gp, steps, _dp(tr), *[(_dp(a) if a is not None else None) for a in F]),
+               "run_f64")
+    if not fields:
+        return tr
+    shp = (m["frame_h"], m["frame_w"])
+    return tr, [a.reshape(shp) for a in F]
+
+
+def source(p: VsParams, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    _check(lib().orc_source_f32(C.byref(p), n, _fp(out)), "source")
+    return out
+
+
+def tmm(ps: float, srate_mul: int, p1: np.ndarray, precision: str = "f32") -> np.ndarray:
+    if precision == "f32":
+        p1 = np.ascontiguousarray(p1, np.float32)
+        ug = np.zeros_like(p1)
+        lib().orc_tmm_f32(ps, srate_mul, _fp(p1), len(p1), _fp(ug))
+    else:
+        p1 = np.ascontiguousarray(p1, np.float64)
+        ug = np.zeros_like(p1)
+        lib().orc_tmm_f64(ps, srate_mul, _dp(p1), len(p1), _dp(ug))
+    return ug
+
+
+def consts(srate_mul: int) -> np.ndarray:
+    out = np.zeros(11, np.float32)
+    lib().orc_consts(srate_mul, _fp(out))
+    return out
+
+
+def tables(srate_mul: int):
+    b = np.zeros(13, np.float32); s = np.zeros(13, np.float32); d = np.zeros(4, np.float32)
+    lib().orc_tables(srate_mul, _fp(b), _fp(s), _fp(d))
+    return b, s, d
+
+
+def step_count(audio_dur: float, dt: float) -> int:
+    return int(lib().orc_step_count(audio_dur, dt))

@@ -1,0 +1,117 @@
+"""GPU parity: the sm_100a step kernel (through the C ABI) against the oracle.
+
+The kernel evaluates the reference engine's expressions with round-to-nearest
+intrinsics in the reference operand order, so on the same maps its FP32
+trace and fields must EQUAL the oracle's FP32 restatement of
+FDTDEngineCPU / FDTDEngineEigen (value equality; +0 and -0 compare equal).
+Against the double-precision restatement the tolerance is the north-star
+bound: relative L2 <= 1e-4.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import vocalsim_b200 as V
+from vocalsim_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+REL_L2_TOL = 1e-4
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def both(kw, L=None, A=None):
+    go = O.Geometry(L, A) if L is not None else None
+    gv = V.Geometry(L, A) if L is not None else None
+    return O.params(**kw), go, V.params(**kw), gv
+
+
+CASES = {
+    # BASELINE config 1 geometry: 17.5 cm x 3 cm, uniform 2 cm depth, mu 0.005
+    "uniform_gauss": (dict(mu3d=0.005, uniform_depth_m=0.02), S.uniform_tube()),
+    "uniform_gauss_std_explicit_listener": (
+        dict(mu3d=0.005, uniform_depth_m=0.02, source_type=3, gauss_peak_s=5e-4, gauss_width_s=1e-4,
+             listener_mode=1, listener_x=244, listener_y=28), S.uniform_tube()),
+    "vowel_ellipse_tmm": (dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0), S.vowel_tube(3)),
+    "vowel_circle_dirichlet": (dict(mouth_radiation_cond=1), S.vowel_tube(5)),
+    "vowel_eigen": (dict(cross_sectional_shape=2, engine=2), S.vowel_tube(7)),
+    "vowel_2d_sine": (dict(fdtd_solver_type=0, source_type=0), S.vowel_tube(9)),
+    "vowel_wall_coupling": (dict(cross_sectional_shape=2, wall_coupling=0.5), S.vowel_tube(11)),
+    "batch_tube_mul30": (dict(cross_sectional_shape=2, srate_mul=30), S.batch_tube(4)[:2]),
+    "dirichlet_nopml": (dict(mouth_radiation_cond=1, pml_flag=0, source_type=2), S.vowel_tube(13)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_trace_and_fields_equal_fp32_oracle(name, cuda_ok):
+    kw, (L, A) = CASES[name]
+    steps = 1500
+    po, go, pv, gv = both(kw, L, A)
+    ref_tr, ref_f = O.run(po, go, steps, "f32", fields=True)
+    s = V.Solver(pv, gv)
+    tr = s.run(steps)
+    P, Vx, Vy = s.fields()
+    assert np.array_equal(tr, ref_tr), f"trace differs, max |d| = {np.abs(tr - ref_tr).max()}"
+    assert np.array_equal(P, ref_f[0])
+    assert np.array_equal(Vx, ref_f[1])
+    assert np.array_equal(Vy, ref_f[2])
+    assert np.any(tr != 0)
+
+
+def test_open_space(cuda_ok):
+    po, go, pv, gv = both(dict(simulation_type=0))
+    ref = O.run(po, None, 400, "f32")
+    tr = V.Solver(pv, None).run(400)
+    assert np.array_equal(tr, ref)
+
+
+def test_chunked_runs_equal_one_run(cuda_ok):
+    kw, (L, A) = CASES["vowel_ellipse_tmm"]
+    _, _, pv, gv = both(kw, L, A)
+    s = V.Solver(pv, gv)
+    whole = s.run(700)
+    s.reset()
+    parts = np.concatenate([s.run(128), s.run(1), s.run(300), s.run(271)])
+    assert np.array_equal(whole, parts)
+
+
+def test_every_tile_shape_gives_the_same_bits(cuda_ok):
+    tubes = [S.batch_tube(i)[:2] for i in range(3)]
+    ps = [V.params(cross_sectional_shape=2, source_type=2 if i == 1 else 1) for i in range(3)]
+    gs = [V.Geometry(L, A) for L, A in tubes]
+    b = V.Batch(ps, gs)
+    ref = None
+    for k in range(len(V.tile_shapes())):
+        b.reset()
+        b.set_tile(k)
+        tr = b.run(300)
+        if ref is None:
+            ref = tr
+        assert np.array_equal(tr, ref), f"tile shape {k}"
+
+
+def test_batch_rows_equal_single_tubes_and_oracle(cuda_ok):
+    n = 6
+    tubes = [S.batch_tube(i)[:2] for i in range(n)]
+    kws = [dict(cross_sectional_shape=2, source_type=2 if i % 3 == 0 else 1, tmm_ps_pa=800.0) for i in range(n)]
+    b = V.Batch([V.params(**k) for k in kws], [V.Geometry(L, A) for L, A in tubes])
+    tr = b.run(600)
+    for i in (0, 1, 5):
+        single = V.Solver(V.params(**kws[i]), V.Geometry(*tubes[i])).run(600)
+        assert np.array_equal(tr[i], single)
+        assert np.array_equal(tr[i], O.run(O.params(**kws[i]), O.Geometry(*tubes[i]), 600, "f32"))
+
+
+def test_config1_full_length_rel_l2_vs_double(cuda_ok):
+    """33 075 steps; FP32 GPU trace vs the FP64 restatement."""
+    kw = dict(mu3d=0.005, uniform_depth_m=0.02, num_steps=33075)
+    L, A = S.uniform_tube()
+    po, go, pv, gv = both(kw, L, A)
+    tr = V.Solver(pv, gv).run(33075)
+    ref64 = O.run(po, go, 33075, "f64")
+    assert rel_l2(tr, ref64) <= REL_L2_TOL

@@ -1,0 +1,521 @@
+// vs_capi.cpp -- the C ABI of libvocalsim_b200 (include/vocalsim_b200.h).
+//
+// A vs_batch owns one device arena holding every tube's planes, the tube
+// descriptors, the tile work list, the run state and the trace buffer.  A
+// vs_solver is a batch of one.  Time steps are issued as CUDA graphs of
+// kChunk step launches (captured once per tile shape) plus direct launches
+// for the remainder.
+#include "vs_device.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace vsb {
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+struct CudaFail {
+    cudaError_t err;
+    const char* where;
+};
+
+void ck(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) throw CudaFail{e, where};
+}
+
+constexpr int kChunk = 128;   // steps per captured graph
+constexpr size_t kAlign = 256;
+
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+}  // namespace
+}  // namespace vsb
+
+using namespace vsb;
+
+struct vs_batch {
+    std::vector<TubeGrid> grids;
+    std::vector<TubeDev> h_tubes;
+    std::vector<size_t> src_off;           // arena offset of each tube's source table
+    std::vector<int64_t> src_len;
+    std::vector<char*> state_base;         // per tube: start of its mutable planes
+    std::vector<size_t> state_bytes;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    float* src_arena = nullptr;            // source tables live in their own buffer
+    size_t src_bytes = 0;
+    TubeDev* d_tubes = nullptr;
+    Tile* d_tiles = nullptr;
+    int ntiles = 0;
+    int tiles_shape = -1;
+    RunState* d_rs = nullptr;
+    float* d_trace = nullptr;
+    int64_t trace_cap = 0;                 // floats
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int shape = -1;                        // chosen tile shape (-1 = not chosen)
+    cudaGraphExec_t graph = nullptr;
+    int graph_shape = -1;
+    int64_t step = 0;                      // host mirror of RunState::step
+    int device = 0;
+
+    ~vs_batch() { release(); }
+
+    void release() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        if (arena) cudaFree(arena);
+        if (src_arena) cudaFree(src_arena);
+        if (d_tubes) cudaFree(d_tubes);
+        if (d_tiles) cudaFree(d_tiles);
+        if (d_rs) cudaFree(d_rs);
+        if (d_trace) cudaFree(d_trace);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+        arena = nullptr; src_arena = nullptr; d_tubes = nullptr; d_tiles = nullptr;
+        d_rs = nullptr; d_trace = nullptr; stream = nullptr;
+    }
+};
+
+struct vs_solver {
+    vs_batch* b = nullptr;
+};
+
+namespace vsb {
+namespace {
+
+// Default tile shape when no autotune ran: 8 x 64 balances halo overhead and
+// the number of CTAs on small single tubes.
+constexpr int kDefaultShape = 2;
+
+int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
+
+void upload_sources(vs_batch* b, int64_t need) {
+    // (Re)build every tube's excitation table so that it covers steps [0, need).
+    bool ok = true;
+    for (size_t i = 0; i < b->grids.size(); ++i)
+        if (!b->grids[i].tmm && b->src_len[i] < need) ok = false;
+    if (ok && b->src_arena) return;
+    size_t total = 0;
+    std::vector<size_t> off(b->grids.size(), 0);
+    for (size_t i = 0; i < b->grids.size(); ++i) {
+        TubeGrid& g = b->grids[i];
+        if (g.tmm) continue;
+        const int64_t len = std::max<int64_t>(need, (int64_t)g.source.size());
+        if ((int64_t)g.source.size() < len) {
+            vs_params p;
+            std::memcpy(&p, &g.src_params, sizeof(p));
+            build_source(&p, g.dt, len, g.source);
+        }
+        off[i] = total;
+        total += align_up((size_t)len * sizeof(float));
+    }
+    if (b->src_arena) { cudaFree(b->src_arena); b->src_arena = nullptr; }
+    if (total) ck(cudaMalloc(&b->src_arena, total), "cudaMalloc(source tables)");
+    for (size_t i = 0; i < b->grids.size(); ++i) {
+        TubeGrid& g = b->grids[i];
+        TubeDev& t = b->h_tubes[i];
+        if (g.tmm) { t.src = nullptr; t.src_len = 0; b->src_len[i] = INT64_MAX; continue; }
+        float* dst = (float*)((char*)b->src_arena + off[i]);
+        ck(cudaMemcpy(dst, g.source.data(), g.source.size() * sizeof(float), cudaMemcpyHostToDevice),
+           "upload source table");
+        t.src = dst;
+        t.src_len = (int64_t)g.source.size();
+        b->src_len[i] = t.src_len;
+    }
+    ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev),
+                  cudaMemcpyHostToDevice), "upload tube descriptors");
+}
+
+void build_tiles(vs_batch* b, int shape) {
+    if (b->tiles_shape == shape && b->d_tiles) return;
+    const TileShape ts = tile_shape(shape);
+    std::vector<Tile> tiles;
+    for (size_t i = 0; i < b->grids.size(); ++i) {
+        const TubeGrid& g = b->grids[i];
+        for (int r0 = 1; r0 <= g.H - 2; r0 += ts.rows) {
+            for (int c0 = 0; c0 <= g.W - 2; c0 += ts.cols) {
+                int has_exc = 0;
+                for (int r = r0; r < std::min(r0 + ts.rows, g.H) && !has_exc; ++r)
+                    for (int c = c0; c < std::min(c0 + ts.cols, g.W); ++c)
+                        if (g.cell_type[(size_t)r * g.W + c] == VS_CELL_EXCITATION) { has_exc = 1; break; }
+                tiles.push_back({(int32_t)i, r0, c0, has_exc});
+            }
+        }
+    }
+    // largest tubes first keeps the tail of a launch short when tubes differ
+    if (b->d_tiles) { cudaFree(b->d_tiles); b->d_tiles = nullptr; }
+    ck(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile)), "cudaMalloc(tiles)");
+    ck(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice),
+       "upload tiles");
+    b->ntiles = (int)tiles.size();
+    b->tiles_shape = shape;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; b->graph_shape = -1; }
+}
+
+void ensure_graph(vs_batch* b) {
+    if (b->graph && b->graph_shape == b->shape) return;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaSuccess;
+    for (int i = 0; i < kChunk && err == cudaSuccess; ++i)
+        err = launch_step(b->shape, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream);
+    if (err == cudaSuccess) err = launch_advance(b->d_rs, kChunk, b->stream);
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    ck(err, "capture step launches");
+    ck(e2, "end capture");
+    cudaError_t e3 = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    ck(e3, "instantiate graph");
+    b->graph_shape = b->shape;
+}
+
+void upload_static(vs_batch* b) {
+    // depth planes and code bytes, padded to the row pitch; written once
+    for (size_t i = 0; i < b->grids.size(); ++i) {
+        const TubeGrid& g = b->grids[i];
+        const TubeDev& t = b->h_tubes[i];
+        const size_t pl = (size_t)g.H * g.pitch;
+        std::vector<float> buf(pl);
+        auto up = [&](const std::vector<float>& src, const float* dst) {
+            std::fill(buf.begin(), buf.end(), 0.0f);
+            for (int r = 0; r < g.H; ++r)
+                std::memcpy(&buf[(size_t)r * g.pitch], &src[(size_t)r * g.W], g.W * sizeof(float));
+            ck(cudaMemcpy((void*)dst, buf.data(), pl * sizeof(float), cudaMemcpyHostToDevice), "upload depth");
+        };
+        up(g.dP, t.dP);
+        up(g.dX, t.dX);
+        up(g.dY, t.dY);
+        ck(cudaMemcpy((void*)t.code, g.code.data(), g.code.size(), cudaMemcpyHostToDevice), "upload codes");
+    }
+}
+
+void reset_state(vs_batch* b) {
+    // fields, wall state and the two-mass state all restart at zero
+    for (size_t i = 0; i < b->grids.size(); ++i)
+        ck(cudaMemsetAsync(b->state_base[i], 0, b->state_bytes[i], b->stream), "zero state");
+    RunState rs{};
+    ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "reset run state");
+    ck(cudaStreamSynchronize(b->stream), "reset sync");
+    b->step = 0;
+}
+
+void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_batch* b) {
+    ck(cudaGetDevice(&b->device), "cudaGetDevice");
+    b->grids.resize(n);
+    for (int i = 0; i < n; ++i) {
+        build_tube(&params[i], geoms ? &geoms[i] : nullptr, b->grids[i], 0);
+        std::memcpy(&b->grids[i].src_params, &params[i], sizeof(vs_params));
+    }
+    // arena layout: per tube, planes of H*pitch floats (+ codes) + two-mass state
+    size_t total = 0;
+    std::vector<size_t> base(n);
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
+        base[i] = total;
+        const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
+        total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState));
+    }
+    b->arena_bytes = total;
+    ck(cudaMalloc(&b->arena, total), "cudaMalloc(arena)");
+    b->h_tubes.resize(n);
+    b->src_len.assign(n, 0);
+    b->state_base.assign(n, nullptr);
+    b->state_bytes.assign(n, 0);
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
+        TubeDev& t = b->h_tubes[i];
+        std::memset(&t, 0, sizeof(t));
+        const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
+        char* p = b->arena + base[i];
+        auto next = [&](size_t bytes) { char* q = p; p += bytes; return q; };
+        // mutable state first (one memset resets it), read-only planes after
+        b->state_base[i] = p;
+        for (int k = 0; k < 2; ++k) t.P[k] = (float*)next(pl);
+        for (int k = 0; k < 2; ++k) t.Vx[k] = (float*)next(pl);
+        for (int k = 0; k < 2; ++k) t.Vy[k] = (float*)next(pl);
+        if (g.wall_ode) {
+            for (int k = 0; k < 2; ++k) t.w[k] = (float*)next(pl);
+            for (int k = 0; k < 2; ++k) t.z[k] = (float*)next(pl);
+        }
+        t.tmm = (TmmState*)next(align_up(2 * sizeof(TmmState)));
+        b->state_bytes[i] = (size_t)(p - b->state_base[i]);
+        t.dP = (const float*)next(pl);
+        t.dX = (const float*)next(pl);
+        t.dY = (const float*)next(pl);
+        t.code = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
+        t.H = g.H; t.W = g.W; t.pitch = g.pitch;
+        t.flags = (g.dirichlet ? TUBE_DIRICHLET : 0) | (g.eigen ? TUBE_EIGEN : 0) |
+                  (g.tmm ? TUBE_TMM : 0) | (g.wall_ode ? TUBE_WALL_ODE : 0);
+        t.lis_x = g.dims.listener_x; t.lis_y = g.dims.listener_y;
+        t.exc_x = g.dims.excitation_x; t.exc_y = g.dims.excitation_y;
+        t.K1 = g.K1; t.K2 = g.K2; t.bcoef = g.bcoef; t.zinv = g.zinv_val;
+        t.dt = g.dt; t.Mw = g.Mw; t.Bw = g.Bw; t.Kw = g.Kw; t.cpl = g.cpl;
+        t.dir0 = g.dir[0]; t.dir1 = g.dir[1]; t.dir2 = g.dir[2]; t.dir3 = g.dir[3];
+        for (int k = 0; k < 13; ++k) t.sigma[k] = g.sigma[k];
+        t.tmmc = g.tmmc;
+    }
+    ck(cudaMalloc(&b->d_tubes, n * sizeof(TubeDev)), "cudaMalloc(tubes)");
+    ck(cudaMalloc(&b->d_rs, sizeof(RunState)), "cudaMalloc(run state)");
+    ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    b->own_stream = true;
+    int64_t need = 0;
+    for (const TubeGrid& g : b->grids) need = std::max<int64_t>(need, g.dims.num_steps);
+    upload_sources(b, need);
+    upload_static(b);
+    reset_state(b);
+    b->shape = kDefaultShape;
+}
+
+void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
+    const int n = (int)b->grids.size();
+    if (b->shape < 0) b->shape = kDefaultShape;
+    build_tiles(b, b->shape);
+    upload_sources(b, b->step + steps);
+    const int64_t need = (int64_t)n * steps;
+    if (need > b->trace_cap) {
+        if (b->d_trace) cudaFree(b->d_trace);
+        b->d_trace = nullptr;
+        ck(cudaMalloc(&b->d_trace, need * sizeof(float)), "cudaMalloc(trace)");
+        b->trace_cap = need;
+    }
+    RunState rs{};
+    rs.step = b->step;
+    rs.run_start = b->step;
+    rs.trace = b->d_trace;
+    rs.trace_stride = steps;
+    ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
+    int64_t done = 0;
+    if (steps >= kChunk) {
+        ensure_graph(b);
+        for (; done + kChunk <= steps; done += kChunk) ck(cudaGraphLaunch(b->graph, b->stream), "graph launch");
+    }
+    const int rem = (int)(steps - done);
+    for (int i = 0; i < rem; ++i)
+        ck(launch_step(b->shape, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream), "step launch");
+    if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
+    b->step += steps;
+    if (traces) {
+        ck(cudaMemcpyAsync(traces, b->d_trace, need * sizeof(float),
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream),
+           "copy traces");
+    }
+    ck(cudaStreamSynchronize(b->stream), "run sync");
+    if (traces && !on_device) {
+        for (int64_t i = 0; i < need; ++i)
+            if (!std::isfinite(traces[i])) throw VsFailure{VS_ERR_NONFINITE, "non-finite listener pressure"};
+    }
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return VS_OK;
+    } catch (const VsFailure& e) {
+        return set_error(e.status, e.what);
+    } catch (const CudaFail& e) {
+        return set_error(VS_ERR_CUDA, std::string(e.where) + ": " + cudaGetErrorString(e.err));
+    } catch (const std::bad_alloc&) {
+        return set_error(VS_ERR_ALLOC, "host allocation failed");
+    }
+}
+
+}  // namespace
+}  // namespace vsb
+
+extern "C" {
+
+int vs_version(void) { return VS_ABI_VERSION; }
+
+const char* vs_last_error(void) { return vsb::g_last_error.c_str(); }
+
+int vs_params_init(vs_params* p) {
+    if (!p) return set_error(VS_ERR_INVALID_ARG, "null vs_params");
+    default_params(p);
+    return VS_OK;
+}
+
+int vs_build_maps(const vs_params* p, const vs_geometry* g, vs_dims* dims, int32_t* cell_type,
+                  float* depth_p, float* depth_x, float* depth_y, float* z_inv) {
+    return guarded([&] {
+        TubeGrid t;
+        build_tube(p, g, t, 1);
+        if (dims) *dims = t.dims;
+        const size_t n = (size_t)t.H * t.W;
+        if (cell_type) std::memcpy(cell_type, t.cell_type.data(), n * sizeof(int32_t));
+        if (depth_p) std::memcpy(depth_p, t.dP.data(), n * sizeof(float));
+        if (depth_x) std::memcpy(depth_x, t.dX.data(), n * sizeof(float));
+        if (depth_y) std::memcpy(depth_y, t.dY.data(), n * sizeof(float));
+        if (z_inv) std::memcpy(z_inv, t.zinv.data(), n * sizeof(float));
+    });
+}
+
+int vs_source_table(const vs_params* p, int64_t num_steps, float* out) {
+    if (!p || !out || num_steps < 0) return set_error(VS_ERR_INVALID_ARG, "vs_source_table arguments");
+    return guarded([&] {
+        const float dt = 1.0f / (float)(44100 * p->srate_mul);
+        std::vector<float> v;
+        build_source(p, dt, num_steps, v);
+        std::memcpy(out, v.data(), (size_t)num_steps * sizeof(float));
+    });
+}
+
+int vs_batch_create(int32_t n, const vs_params* params, const vs_geometry* geoms, vs_batch** out) {
+    if (!out || !params || n < 1) return set_error(VS_ERR_INVALID_ARG, "vs_batch_create arguments");
+    *out = nullptr;
+    std::unique_ptr<vs_batch> b(new (std::nothrow) vs_batch());
+    if (!b) return set_error(VS_ERR_ALLOC, "host allocation failed");
+    int st = guarded([&] { create_batch(n, params, geoms, b.get()); });
+    if (st == VS_OK) *out = b.release();
+    return st;
+}
+
+int vs_batch_get_dims(const vs_batch* b, int32_t i, vs_dims* dims) {
+    if (!b || !dims || i < 0 || i >= (int)b->grids.size()) return set_error(VS_ERR_INVALID_ARG, "vs_batch_get_dims");
+    *dims = b->grids[i].dims;
+    return VS_OK;
+}
+
+int vs_batch_run(vs_batch* b, int64_t steps, float* traces, int traces_on_device) {
+    if (!b || steps < 0) return set_error(VS_ERR_INVALID_ARG, "vs_batch_run arguments");
+    if (steps == 0) return VS_OK;
+    return guarded([&] { run_batch(b, steps, traces, traces_on_device); });
+}
+
+int vs_batch_reset(vs_batch* b) {
+    if (!b) return set_error(VS_ERR_INVALID_ARG, "null batch");
+    return guarded([&] { reset_state(b); });
+}
+
+int vs_batch_set_tile(vs_batch* b, int32_t tile_index) {
+    if (!b || tile_index < -1 || tile_index >= tile_shape_count())
+        return set_error(VS_ERR_INVALID_ARG, "tile index out of range");
+    b->shape = tile_index < 0 ? kDefaultShape : tile_index;
+    return VS_OK;
+}
+
+int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* best_ms) {
+    if (!b || steps < 1) return set_error(VS_ERR_INVALID_ARG, "vs_batch_autotune arguments");
+    return guarded([&] {
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        float best = 1e30f;
+        int best_i = kDefaultShape;
+        for (int s = 0; s < tile_shape_count(); ++s) {
+            b->shape = s;
+            run_batch(b, std::min<int64_t>(steps, kChunk), nullptr, 1);   // warm: tiles + graph
+            ck(cudaEventRecord(e0, b->stream), "record");
+            run_batch(b, steps, nullptr, 1);
+            ck(cudaEventRecord(e1, b->stream), "record");
+            ck(cudaEventSynchronize(e1), "sync");
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+            if (ms < best) { best = ms; best_i = s; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->shape = best_i;
+        build_tiles(b, best_i);
+        reset_state(b);
+        if (best_index) *best_index = best_i;
+        if (best_ms) *best_ms = best;
+    });
+}
+
+int vs_tile_shape_count(void) { return tile_shape_count(); }
+
+int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {
+    if (i < 0 || i >= tile_shape_count()) return set_error(VS_ERR_INVALID_ARG, "tile index out of range");
+    const TileShape s = tile_shape(i);
+    if (rows) *rows = s.rows;
+    if (cols) *cols = s.cols;
+    return VS_OK;
+}
+
+void vs_batch_destroy(vs_batch* b) { delete b; }
+
+int vs_create(const vs_params* p, const vs_geometry* g, vs_solver** out) {
+    if (!out || !p) return set_error(VS_ERR_INVALID_ARG, "vs_create arguments");
+    *out = nullptr;
+    vs_batch* b = nullptr;
+    int st = vs_batch_create(1, p, g, &b);
+    if (st != VS_OK) return st;
+    vs_solver* s = new (std::nothrow) vs_solver();
+    if (!s) { delete b; return set_error(VS_ERR_ALLOC, "host allocation failed"); }
+    s->b = b;
+    *out = s;
+    return VS_OK;
+}
+
+int vs_get_dims(const vs_solver* s, vs_dims* dims) {
+    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
+    return vs_batch_get_dims(s->b, 0, dims);
+}
+
+int vs_run(vs_solver* s, int64_t steps, float* trace, int trace_on_device) {
+    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
+    return vs_batch_run(s->b, steps, trace, trace_on_device);
+}
+
+int vs_reset(vs_solver* s) {
+    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
+    return vs_batch_reset(s->b);
+}
+
+int vs_get_fields(const vs_solver* s, float* p, float* vx, float* vy) {
+    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
+    const vs_batch* b = s->b;
+    return guarded([&] {
+        const TubeGrid& g = b->grids[0];
+        const TubeDev& t = b->h_tubes[0];
+        const int par = (int)(b->step & 1);
+        const float* src[3] = {t.P[par], t.Vx[par], t.Vy[par]};
+        float* dst[3] = {p, vx, vy};
+        for (int k = 0; k < 3; ++k) {
+            if (!dst[k]) continue;
+            ck(cudaMemcpy2DAsync(dst[k], g.W * sizeof(float), src[k], g.pitch * sizeof(float),
+                                 g.W * sizeof(float), g.H, cudaMemcpyDeviceToHost, b->stream),
+               "copy fields");
+        }
+        ck(cudaStreamSynchronize(b->stream), "fields sync");
+    });
+}
+
+int vs_set_stream(vs_solver* s, void* cuda_stream) {
+    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
+    vs_batch* b = s->b;
+    return guarded([&] {
+        ck(cudaStreamSynchronize(b->stream), "sync old stream");
+        if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+        if (cuda_stream) {
+            b->stream = (cudaStream_t)cuda_stream;
+            b->own_stream = false;
+        } else {
+            ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            b->own_stream = true;
+        }
+    });
+}
+
+void vs_destroy(vs_solver* s) {
+    if (!s) return;
+    delete s->b;
+    delete s;
+}
+
+}  // extern "C"

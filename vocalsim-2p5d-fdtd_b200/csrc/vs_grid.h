@@ -1,0 +1,75 @@
+// vs_grid.h -- host-side grid description shared by the map builder, the
+// C ABI and the CUDA launchers of libvocalsim_b200.
+#pragma once
+
+#include "../../include/vocalsim_b200.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace vsb {
+
+// Cell code byte stored per cell on the device: bits 0-3 = reference cell type
+// (0..12), bit 4 = "z_inv applies here" (boundary_segment_type != 0).
+constexpr uint8_t CODE_TYPE_MASK = 0x0f;
+constexpr uint8_t CODE_ZINV_BIT = 0x10;
+
+// Error carried out of the host builders into a vs_status.
+struct VsFailure {
+    int status;
+    std::string what;
+};
+
+// Constants of the two-mass vocal fold model (TwoMassModel.cpp:4-87), as the
+// float values the reference stores in its members.
+struct TmmConsts {
+    float mu, rho, m1, m2, d1, d2, k1, k2, kc, etak1, etak2, h1, h2, etah1, etah2;
+    float Ag01, Ag02, lg, r1o, r2o, r1c, r2c, A1, ps, srate;
+};
+
+// Two-mass model state carried from step to step (the members the reference
+// reads before writing in runTwoMassModel).
+struct TmmState {
+    float x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr;
+};
+
+// Everything the device needs for one tube, in host memory.
+struct TubeGrid {
+    vs_dims dims{};
+    int H = 0, W = 0;
+    int pitch = 0;                    // row pitch of every device plane, in elements
+    bool dirichlet = false;
+    bool eigen = false;
+    bool tmm = false;
+    bool wall_ode = false;            // 2.5D with a nonzero wall coupling
+    int srate_mul = 1;
+    float K1 = 0, K2 = 0;             // rho c^2 dt / ds, rho c^2 dt (FDTDSolver.cu:311-312)
+    float bcoef = 0;                  // dt / (rho ds): betaV*Sqr_dt_inv_rho_inv_ds for beta = 1
+    float zinv_val = 0;
+    float dt = 0, Mw = 0, Bw = 0, Kw = 0, cpl = 0;
+    float beta[16] = {0}, sigma[16] = {0};
+    float dir[4] = {0};
+    std::vector<int32_t> cell_type;   // H*W, reference values
+    std::vector<uint8_t> code;        // H*pitch, padding = dead
+    std::vector<float> zinv;          // H*W
+    std::vector<float> dP, dX, dY;    // H*W
+    std::vector<float> source;        // per-step excitation (empty for the two-mass source)
+    TmmConsts tmmc{};
+    vs_params src_params{};           // parameters the source table is rebuilt from
+};
+
+// Fill p with the reference's defaults.
+void default_params(vs_params* p);
+
+// Build a tube (or the open-space domain) exactly as FDTDSolver::setupWaveSolver.
+// `steps_for_source` > 0 sizes the source table; 0 uses dims.num_steps.
+void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source);
+
+// The per-step excitation table (GlottalExcitations::setExcitationVelocity).
+void build_source(const vs_params* p, float dt, int64_t n, std::vector<float>& out);
+
+// Two-mass model constants (setTwoMassModelParams) for a given subglottal pressure.
+TmmConsts tmm_consts(float ps, int srate_mul);
+
+}  // namespace vsb

@@ -1,0 +1,176 @@
+"""Python handles over the C ABI (ctypes): Geometry, Solver, Batch, build_maps.
+
+Every compute call goes through libvocalsim_b200.so; there is no Python or
+CPU fallback, and a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from .abi import VsDims, VsGeometry, VsParams, check, load_library
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def params(**overrides) -> VsParams:
+    """Reference defaults (vs_params_init) with keyword overrides."""
+    lib = load_library()
+    p = VsParams()
+    check(lib, lib.vs_params_init(C.byref(p)), "vs_params_init")
+    for k, v in overrides.items():
+        if not hasattr(p, k) or k in ("pad0", "reserved"):
+            raise KeyError(f"unknown vs_params field {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+class Geometry:
+    """An area function; keeps the float32 arrays the C struct points at alive."""
+
+    def __init__(self, length_cm, area_cm2):
+        self.length = np.ascontiguousarray(length_cm, dtype=np.float32).reshape(-1)
+        self.area = np.ascontiguousarray(area_cm2, dtype=np.float32).reshape(-1)
+        if self.length.shape != self.area.shape:
+            raise ValueError("length and area need the same number of sections")
+        self.struct = VsGeometry(len(self.length), 0, _fp(self.length), _fp(self.area))
+
+
+def build_maps(p: VsParams, g: Geometry | None) -> dict:
+    """Host-only map build (vs_build_maps): dims + cell_type/depth/z_inv frames."""
+    lib = load_library()
+    gp = C.byref(g.struct) if g is not None else None
+    d = VsDims()
+    check(lib, lib.vs_build_maps(C.byref(p), gp, C.byref(d), None, None, None, None, None), "vs_build_maps")
+    shp = (d.frame_h, d.frame_w)
+    ct = np.zeros(shp, np.int32)
+    dp, dx, dy, z = (np.zeros(shp, np.float32) for _ in range(4))
+    check(lib, lib.vs_build_maps(C.byref(p), gp, C.byref(d), ct.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 _fp(dp), _fp(dx), _fp(dy), _fp(z)), "vs_build_maps")
+    return dict(dims=d.as_dict(), cell_type=ct, depth_p=dp, depth_x=dx, depth_y=dy, z_inv=z)
+
+
+def source_table(p: VsParams, n: int) -> np.ndarray:
+    lib = load_library()
+    out = np.zeros(n, np.float32)
+    check(lib, lib.vs_source_table(C.byref(p), n, _fp(out)), "vs_source_table")
+    return out
+
+
+class Solver:
+    """One tube on the current CUDA device (vs_create / vs_run / vs_destroy)."""
+
+    def __init__(self, p: VsParams, g: Geometry | None):
+        self.lib = load_library()
+        self._g = g
+        self.h = C.c_void_p()
+        check(self.lib, self.lib.vs_create(C.byref(p), C.byref(g.struct) if g is not None else None,
+                                           C.byref(self.h)), "vs_create")
+        d = VsDims()
+        check(self.lib, self.lib.vs_get_dims(self.h, C.byref(d)), "vs_get_dims")
+        self.dims = d.as_dict()
+
+    def run(self, steps: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Advance `steps` steps; return the listener trace (host float32)."""
+        tr = out if out is not None else np.zeros(steps, np.float32)
+        check(self.lib, self.lib.vs_run(self.h, steps, tr.ctypes.data_as(C.c_void_p), 0), "vs_run")
+        return tr
+
+    def run_device(self, steps: int, device_ptr: int) -> None:
+        """Advance `steps` steps writing the trace to a device buffer."""
+        check(self.lib, self.lib.vs_run(self.h, steps, C.c_void_p(device_ptr), 1), "vs_run")
+
+    def reset(self) -> None:
+        check(self.lib, self.lib.vs_reset(self.h), "vs_reset")
+
+    def fields(self):
+        H, W = self.dims["frame_h"], self.dims["frame_w"]
+        P, Vx, Vy = (np.zeros((H, W), np.float32) for _ in range(3))
+        check(self.lib, self.lib.vs_get_fields(self.h, _fp(P), _fp(Vx), _fp(Vy)), "vs_get_fields")
+        return P, Vx, Vy
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.vs_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent tubes stepped together (vs_batch_*)."""
+
+    def __init__(self, ps: Sequence[VsParams], gs: Sequence[Geometry | None]):
+        self.lib = load_library()
+        n = len(ps)
+        if n != len(gs):
+            raise ValueError("one geometry per parameter set")
+        self._gs = list(gs)
+        parr = (VsParams * n)(*ps)
+        garr = (VsGeometry * n)()
+        for i, g in enumerate(gs):
+            if g is not None:
+                garr[i] = g.struct
+        self.n = n
+        self.h = C.c_void_p()
+        check(self.lib, self.lib.vs_batch_create(n, parr, garr, C.byref(self.h)), "vs_batch_create")
+        self.dims = []
+        for i in range(n):
+            d = VsDims()
+            check(self.lib, self.lib.vs_batch_get_dims(self.h, i, C.byref(d)), "vs_batch_get_dims")
+            self.dims.append(d.as_dict())
+
+    @property
+    def interior_cells(self) -> int:
+        return sum(d["interior_cells"] for d in self.dims)
+
+    def run(self, steps: int, out: np.ndarray | None = None) -> np.ndarray:
+        tr = out if out is not None else np.zeros((self.n, steps), np.float32)
+        check(self.lib, self.lib.vs_batch_run(self.h, steps, tr.ctypes.data_as(C.c_void_p), 0), "vs_batch_run")
+        return tr
+
+    def run_device(self, steps: int, device_ptr: int = 0) -> None:
+        """Advance without a host copy; device_ptr (n x steps floats) may be 0."""
+        check(self.lib, self.lib.vs_batch_run(self.h, steps, C.c_void_p(device_ptr) if device_ptr else None, 1),
+              "vs_batch_run")
+
+    def reset(self) -> None:
+        check(self.lib, self.lib.vs_batch_reset(self.h), "vs_batch_reset")
+
+    def set_tile(self, index: int) -> None:
+        check(self.lib, self.lib.vs_batch_set_tile(self.h, index), "vs_batch_set_tile")
+
+    def autotune(self, steps: int):
+        best = C.c_int32(-1)
+        ms = C.c_float(0)
+        check(self.lib, self.lib.vs_batch_autotune(self.h, steps, C.byref(best), C.byref(ms)), "vs_batch_autotune")
+        return best.value, ms.value
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.vs_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tile_shapes() -> list[tuple[int, int]]:
+    lib = load_library()
+    out = []
+    for i in range(lib.vs_tile_shape_count()):
+        r, c = C.c_int32(), C.c_int32()
+        check(lib, lib.vs_tile_shape(i, C.byref(r), C.byref(c)), "vs_tile_shape")
+        out.append((r.value, c.value))
+    return out
