@@ -1,0 +1,357 @@
+"""Benchmark of the B200 FDTD time-stepping path.
+
+Workload (one bench "step"): the batched forward -- 256 seeded tubes of
+uneven length (12-20 cm) and width (2-4 cm), 3:1 elliptical sections,
+Gaussian source, 6-cell PML, FP32 fields, 50 ms simulated (33 075 time
+steps) -- run through the C ABI.  Metric: Gcell-updates/s, one cell-update =
+one interior cell advanced one full step (P and V).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the reference's CPU engine (the oracle's restatement of
+FDTDEngineCPU; the reference engine itself does not build here) on the host
+cores over a bounded sample of the same workload.
+--profile-steps S builds the batch and runs S time steps, untimed, for ncu.
+Under torchrun every rank runs its own 256-tube batch (weak scaling; no
+collective on the data path) and rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "vocalsim-2p5d-fdtd_b200" / "python"))
+
+N_TUBES = 256
+SIM_STEPS = 33075                      # 50 ms at 44.1 kHz x 15
+BYTES_PER_CELL_UPDATE = 37             # P,Vx,Vy read+write (24) + dP,dX,dY (12) + code (1)
+METRIC = "Gcell-updates/s"
+PEAKS = REPO / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_params(rank: int, n_tubes: int):
+    from vocalsim_b200 import synthetic as S
+    import vocalsim_b200 as V
+    ps, gs = [], []
+    for i in range(n_tubes):
+        L, A, _, _ = S.batch_tube(rank * n_tubes + i)
+        ps.append(V.params(cross_sectional_shape=2, num_steps=SIM_STEPS))
+        gs.append(V.Geometry(L, A))
+    return ps, gs
+
+
+def hbm_peak():
+    if PEAKS.exists():
+        d = json.loads(PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- CPU reference
+def _cpu_worker(args):
+    seed, steps = args
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    from vocalsim_b200 import synthetic as S
+    L, A, _, _ = S.batch_tube(seed)
+    p = O.params(cross_sectional_shape=2, num_steps=SIM_STEPS)
+    g = O.Geometry(L, A)
+    cells = O.maps(p, g)["dims"]["interior_cells"]
+    t0 = time.perf_counter()
+    O.run(p, g, steps, "f32")
+    return cells * steps, time.perf_counter() - t0
+
+
+def cpu_reference(n_tubes: int, steps_per_tube: int, procs: int):
+    """Throughput of the FP32 CPU engine over `n_tubes` tubes x `steps_per_tube` steps, one process per core."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    work = [(i, steps_per_tube) for i in range(n_tubes)]
+    with ctx.Pool(procs) as pool:
+        pool.map(_cpu_worker, [(0, 10)] * procs)          # import + build cost outside the clock
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_worker, work, chunksize=1)
+        wall = time.perf_counter() - t0
+    cell_updates = sum(r[0] for r in res)
+    return cell_updates / wall / 1e9, wall, cell_updates
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample_steps(n_sample: int) -> int:
+    """Time steps per sampled tube so one sample is ~20 core-seconds of the CPU engine (~60 Mcell/s/core)."""
+    return int(min(5000, max(200, 20 * 6e7 / (n_sample * 13000))))
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    procs = host_cores()
+    n_sample = min(N_TUBES, max(procs, 16))
+    steps = cpu_sample_steps(n_sample)
+    per_step = []
+    for _ in range(args.warmup):
+        cpu_reference(procs, 50, procs)
+    for _ in range(args.steps):
+        g, wall, cu = cpu_reference(n_sample, steps, procs)
+        per_step.append((g, wall))
+    value = statistics.median(g for g, _ in per_step)
+    sample = (f"{n_sample} of the {N_TUBES} batch tubes x {steps} of {SIM_STEPS} time steps per bench step, "
+              f"one spawn process per host core")
+    return {
+        "metric": METRIC, "value": round(value, 4), "unit": "Gcell-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * statistics.median(w for _, w in per_step), 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded area functions)",
+        "config": {"workload": "batched forward, 256 tubes 12-20 cm x 2-4 cm, 50 ms (33075 steps), fs 661.5 kHz",
+                   "tubes": N_TUBES, "sim_steps": SIM_STEPS},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# --------------------------------------------------------------------------- GPU arm
+def run_b200(args, rank, world):
+    import torch
+    import vocalsim_b200 as V
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    ps, gs = workload_params(rank, args.tubes)
+    batch = V.Batch(ps, gs)
+    batch.set_stream(stream.cuda_stream)
+    cells = batch.interior_cells
+    sim_steps = args.sim_steps
+    if args.profile_steps:
+        if args.tile >= 0:
+            batch.set_tile(args.tile)
+        batch.run_device(args.profile_steps)
+        torch.cuda.synchronize()
+        return None
+    tile, tune_ms = batch.autotune(128)
+
+    def forward():
+        batch.reset()
+        batch.run_device(sim_steps)
+
+    for _ in range(args.warmup):
+        forward()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            forward()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    cell_updates_rank = cells * sim_steps
+    value = cell_updates_rank * world / (ms_step / 1e3) / 1e9
+    launches_per_forward = sim_steps + math.ceil(sim_steps / 128)
+    launch_ms = ms_step / sim_steps            # average per step-kernel launch incl. graph gaps
+    achieved_gbs = BYTES_PER_CELL_UPDATE * cells / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+
+    # ---- e2e: public API with host buffers: build + upload maps, run, download traces
+    e2e = None
+    if not args.no_e2e:
+        trace_host = torch.empty((args.tubes, sim_steps), dtype=torch.float32, pin_memory=True)
+        trace_np = trace_host.numpy()
+        e2e_ms = []
+        for i in range(args.steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b2 = V.Batch(ps, gs)
+            b2.set_tile(tile)
+            b2.run(sim_steps, out=trace_np)
+            b2.close()
+            dt = (time.perf_counter() - t0) * 1e3
+            if i > 0:
+                e2e_ms.append(dt)
+        e2e_step = statistics.median(e2e_ms)
+        h2d = sum(d["frame_h"] * ((d["frame_w"] + 31) // 32 * 32) * 13 for d in batch.dims) + \
+            sum(4 * sim_steps for _ in batch.dims)
+        d2h = 4 * sim_steps * args.tubes
+        e2e = {"value": round(cell_updates_rank * world / (e2e_step / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_step, 2)}
+
+    # ---- plain single-tube GPU path for the batched-vs-single ratio
+    single = None
+    if not args.no_single:
+        from vocalsim_b200 import synthetic as S
+        L, A = S.uniform_tube()
+        s = V.Solver(V.params(mu3d=0.005, uniform_depth_m=0.02, num_steps=SIM_STEPS), V.Geometry(L, A))
+        s.set_stream(stream.cuda_stream)
+        dtr = torch.empty(SIM_STEPS, dtype=torch.float32, device=dev)
+        s.run_device(SIM_STEPS, dtr.data_ptr())
+        torch.cuda.synchronize()
+        s.reset()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.run_device(SIM_STEPS, dtr.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        sms = a.elapsed_time(b)
+        single = {"workload": "uniform tube 17.5 x 3 cm, 57x253 frame, 33075 steps",
+                  "value": round(s.dims["interior_cells"] * SIM_STEPS / (sms / 1e3) / 1e9, 3),
+                  "unit": "Gcell-updates/s", "ms": round(sms, 2)}
+        s.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        procs = host_cores()
+        n_sample = min(args.tubes, max(procs, 16))
+        csteps = cpu_sample_steps(n_sample)
+        g, wall, _ = cpu_reference(n_sample, csteps, procs)
+        cpu = {"value": round(g, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": "port",
+               "sample": f"{n_sample} batch tubes x {csteps} of {SIM_STEPS} steps, FP32 restatement of FDTDEngineCPU, "
+                         f"one process per core ({wall:.1f} s)"}
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded area functions, no dataset)",
+        "config": {"workload": "batched forward, 256 tubes 12-20 cm x 2-4 cm, 3:1 elliptical, Gaussian, PML 6, "
+                               "50 ms (33075 steps) at fs 661.5 kHz; one step = one full forward",
+                   "tubes_per_gpu": args.tubes, "interior_cells_per_gpu": cells, "sim_steps": sim_steps,
+                   "tile": list(V.tile_shapes()[tile]), "parallelism": f"tube sharding x{world} (no collective)",
+                   "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_gbs / peak, 4), "traffic": None,
+                     "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell-update x {cells} cells per launch / "
+                             f"mean launch time {launch_ms * 1e3:.2f} us; peak {peak_kind}"},
+        "gpu_launches": args.steps * launches_per_forward,
+        "clocks": clocks.summary(),
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "single_tube": single,
+        "batched_vs_single": round(value / world / single["value"], 2) if single else None,
+        "grad_fwd_ratio": None,
+    }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--tubes", type=int, default=N_TUBES)
+    ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
+    ap.add_argument("--profile-steps", type=int, default=0)
+    ap.add_argument("--tile", type=int, default=-1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-single", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_b200(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -203,6 +203,10 @@ int vs_batch_run(vs_batch* b, int64_t steps, float* traces, int traces_on_device
 /* Zero all fields and restart every tube at step 0. */
 int vs_batch_reset(vs_batch* b);
 
+/* Use this CUDA stream (a cudaStream_t) for every later call on b; NULL means
+ * the handle's own stream. */
+int vs_batch_set_stream(vs_batch* b, void* cuda_stream);
+
 /* Select the tile shape used by the step kernel (index into the compiled
  * shape table, see vs_tile_shape) or -1 for the autotuned choice. */
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index);

@@ -96,9 +96,8 @@ struct vs_solver {
 namespace vsb {
 namespace {
 
-// Default tile shape when no autotune ran: 8 x 64 balances halo overhead and
-// the number of CTAs on small single tubes.
-constexpr int kDefaultShape = 2;
+// Default launch shape when no autotune ran: 16-row strips, 4 warps per CTA.
+constexpr int kDefaultShape = 1;
 
 int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
 
@@ -142,20 +141,21 @@ void upload_sources(vs_batch* b, int64_t need) {
 void build_tiles(vs_batch* b, int shape) {
     if (b->tiles_shape == shape && b->d_tiles) return;
     const TileShape ts = tile_shape(shape);
+    // strips: lanes on columns c0..c0+31 with c0 = cols*k - 1, committing
+    // c0+1..c0+cols; rows r0 .. r0+rows-1 of the interior
     std::vector<Tile> tiles;
     for (size_t i = 0; i < b->grids.size(); ++i) {
         const TubeGrid& g = b->grids[i];
         for (int r0 = 1; r0 <= g.H - 2; r0 += ts.rows) {
-            for (int c0 = 0; c0 <= g.W - 2; c0 += ts.cols) {
+            for (int c0 = -1; c0 + 1 <= g.W - 2; c0 += ts.cols) {
                 int has_exc = 0;
-                for (int r = r0; r < std::min(r0 + ts.rows, g.H) && !has_exc; ++r)
-                    for (int c = c0; c < std::min(c0 + ts.cols, g.W); ++c)
+                for (int r = r0; r < std::min(r0 + ts.rows, g.H - 1) && !has_exc; ++r)
+                    for (int c = std::max(c0 + 1, 0); c <= std::min(c0 + ts.cols, g.W - 1); ++c)
                         if (g.cell_type[(size_t)r * g.W + c] == VS_CELL_EXCITATION) { has_exc = 1; break; }
                 tiles.push_back({(int32_t)i, r0, c0, has_exc});
             }
         }
     }
-    // largest tubes first keeps the tail of a launch short when tubes differ
     if (b->d_tiles) { cudaFree(b->d_tiles); b->d_tiles = nullptr; }
     ck(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile)), "cudaMalloc(tiles)");
     ck(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice),
@@ -258,6 +258,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.dY = (const float*)next(pl);
         t.code = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
         t.H = g.H; t.W = g.W; t.pitch = g.pitch;
+        t.plane = (int64_t)(pl / sizeof(float));
         t.flags = (g.dirichlet ? TUBE_DIRICHLET : 0) | (g.eigen ? TUBE_EIGEN : 0) |
                   (g.tmm ? TUBE_TMM : 0) | (g.wall_ode ? TUBE_WALL_ODE : 0);
         t.lis_x = g.dims.listener_x; t.lis_y = g.dims.listener_y;
@@ -443,7 +444,7 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {
     if (i < 0 || i >= tile_shape_count()) return set_error(VS_ERR_INVALID_ARG, "tile index out of range");
     const TileShape s = tile_shape(i);
     if (rows) *rows = s.rows;
-    if (cols) *cols = s.cols;
+    if (cols) *cols = s.cols * s.warps;
     return VS_OK;
 }
 
@@ -496,9 +497,8 @@ int vs_get_fields(const vs_solver* s, float* p, float* vx, float* vy) {
     });
 }
 
-int vs_set_stream(vs_solver* s, void* cuda_stream) {
-    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
-    vs_batch* b = s->b;
+int vs_batch_set_stream(vs_batch* b, void* cuda_stream) {
+    if (!b) return set_error(VS_ERR_INVALID_ARG, "null batch");
     return guarded([&] {
         ck(cudaStreamSynchronize(b->stream), "sync old stream");
         if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -510,6 +510,11 @@ int vs_set_stream(vs_solver* s, void* cuda_stream) {
             b->own_stream = true;
         }
     });
+}
+
+int vs_set_stream(vs_solver* s, void* cuda_stream) {
+    if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
+    return vs_batch_set_stream(s->b, cuda_stream);
 }
 
 void vs_destroy(vs_solver* s) {

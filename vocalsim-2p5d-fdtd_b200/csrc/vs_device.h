@@ -33,6 +33,9 @@ struct TubeDev {
     const float* src;     // per-step excitation table (nullptr for the two-mass source)
     TmmState* tmm;        // [2], ping-ponged by step parity
     int64_t src_len;
+    int64_t plane;        // elements between consecutive planes: P[k] = P[0] + k*plane,
+                          // Vx[k] = P[0] + (2+k)*plane, Vy[k] = P[0] + (4+k)*plane,
+                          // dX = dP + plane, dY = dP + 2*plane
     int32_t H, W, pitch, flags;
     int32_t lis_x, lis_y, exc_x, exc_y;
     float K1, K2, bcoef, zinv;
@@ -53,14 +56,16 @@ struct RunState {
     int32_t pad;
 };
 
-// A tile of one tube processed by one CTA: rows [r0, r0+TR), cols [c0, c0+TC).
+// A strip of one tube processed by one warp: rows [r0, r0+rows), lanes on
+// columns c0 .. c0+31, committing columns c0+1 .. c0+cols.
 struct Tile {
     int32_t tube, r0, c0, has_exc;
 };
 
-// Host-side launch description of the compiled tile shapes.
+// Host-side description of a compiled launch shape: strip rows, committed
+// columns per strip, warps per CTA.
 struct TileShape {
-    int rows, cols;
+    int rows, cols, warps;
 };
 
 int tile_shape_count();

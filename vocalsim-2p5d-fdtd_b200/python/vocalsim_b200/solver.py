@@ -87,6 +87,10 @@ class Solver:
     def reset(self) -> None:
         check(self.lib, self.lib.vs_reset(self.h), "vs_reset")
 
+    def set_stream(self, stream_handle: int | None) -> None:
+        check(self.lib, self.lib.vs_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
+              "vs_set_stream")
+
     def fields(self):
         H, W = self.dims["frame_h"], self.dims["frame_w"]
         P, Vx, Vy = (np.zeros((H, W), np.float32) for _ in range(3))
@@ -144,6 +148,11 @@ class Batch:
 
     def reset(self) -> None:
         check(self.lib, self.lib.vs_batch_reset(self.h), "vs_batch_reset")
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        """Issue all later work on this cudaStream_t (an int handle, e.g. torch's stream.cuda_stream)."""
+        check(self.lib, self.lib.vs_batch_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
+              "vs_batch_set_stream")
 
     def set_tile(self, index: int) -> None:
         check(self.lib, self.lib.vs_batch_set_tile(self.h, index), "vs_batch_set_tile")
