@@ -221,6 +221,30 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
 
 void vs_batch_destroy(vs_batch* b);
 
+/* ---- running without allocating ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they step a tube: a real-time audio host calling from its processing
+ * thread, where an allocation may block for an unbounded time, or an
+ * application whose device memory is reserved by another allocator, so a
+ * direct cudaMalloc can fail.  The caller passes device buffers it already
+ * owns: the H x W maps of vs_build_maps (cell_type, depth_p/x/y, z_inv), the
+ * excitation table of vs_source_table (>= steps entries; NULL for the
+ * two-mass source), the dims vs_build_maps returned, and a device trace of
+ * `steps` floats.  The listener trace equals what vs_run gives for the same
+ * tube.  Everything else lives in a 16 MiB static device array that every
+ * GPU loading the library holds until exit; a frame larger than it (about
+ * 37 bytes x H x roundup(W, 32)) is rejected with VS_ERR_INVALID_ARG.  The
+ * call allocates nothing and returns once the work is queued on cuda_stream
+ * (a cudaStream_t; NULL = default stream); synchronise the stream before
+ * reading the trace.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture.
+ * Calls share the array: it is re-initialised on every call, and calls whose
+ * work overlaps on the GPU race on it. */
+int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int32_t* cell_type,
+                   const float* depth_p, const float* depth_x, const float* depth_y,
+                   const float* z_inv, const float* source, int64_t steps, float* trace,
+                   void* cuda_stream);
+
 /* Last error text of this host thread (never NULL). */
 const char* vs_last_error(void);
 

@@ -36,6 +36,13 @@ void ck(cudaError_t e, const char* where) {
     if (e != cudaSuccess) throw CudaFail{e, where};
 }
 
+}  // namespace
+
+// Error text for entry points defined in other files of the library.
+void record_error(const char* msg) { g_last_error = msg; }
+
+namespace {
+
 constexpr int kChunk = 128;   // steps per captured graph
 constexpr size_t kAlign = 256;
 

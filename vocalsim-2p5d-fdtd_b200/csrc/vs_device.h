@@ -76,6 +76,9 @@ TileShape tile_shape(int i);
 cudaError_t launch_step(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles,
                         RunState* rs, int local, cudaStream_t stream);
 
+// Set the text vs_last_error() returns on this host thread.
+void record_error(const char* msg);
+
 // RunState::step += k (the tail node of a captured chunk).
 cudaError_t launch_advance(RunState* rs, int k, cudaStream_t stream);
 
