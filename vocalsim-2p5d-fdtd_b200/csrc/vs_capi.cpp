@@ -45,6 +45,7 @@ namespace {
 
 constexpr int kChunk = 128;   // steps per captured graph
 constexpr size_t kAlign = 256;
+constexpr size_t kGuard = 1024;  // bytes of slack around the tube planes of an arena
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
@@ -78,6 +79,8 @@ struct vs_batch {
     int graph_shape = -1;
     int64_t step = 0;                      // host mirror of RunState::step
     int device = 0;
+    bool wall = false;                     // some tube has the coupled wall oscillator
+    int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
 
     ~vs_batch() { release(); }
 
@@ -103,8 +106,11 @@ struct vs_solver {
 namespace vsb {
 namespace {
 
-// Default launch shape when no autotune ran: 16-row strips, 4 warps per CTA.
+// Default launch shapes when no autotune ran: 16-row strips with 4 warps per
+// CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells.
 constexpr int kDefaultShape = 1;
+constexpr int kSmallShape = 8;
+constexpr int64_t kSmallGridCells = 200000;
 
 int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
 
@@ -145,21 +151,47 @@ void upload_sources(vs_batch* b, int64_t need) {
                   cudaMemcpyHostToDevice), "upload tube descriptors");
 }
 
+// Largest dynamic shared memory a CTA may use on this device.
+size_t smem_optin_limit(int device) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) return 0;
+    return (size_t)v;
+}
+
+bool shape_fits(const vs_batch* b, int shape) {
+    return shape_smem_bytes(shape, b->max_pitch) <= smem_optin_limit(b->device);
+}
+
 void build_tiles(vs_batch* b, int shape) {
     if (b->tiles_shape == shape && b->d_tiles) return;
     const TileShape ts = tile_shape(shape);
-    // strips: lanes on columns c0..c0+31 with c0 = cols*k - 1, committing
-    // c0+1..c0+cols; rows r0 .. r0+rows-1 of the interior
+    if (!shape_fits(b, shape)) throw VsFailure{VS_ERR_UNSUPPORTED, "launch shape needs more shared memory than the device has"};
+    ck(prepare_shape(shape, b->max_pitch), "kernel attributes");
     std::vector<Tile> tiles;
     for (size_t i = 0; i < b->grids.size(); ++i) {
         const TubeGrid& g = b->grids[i];
+        auto code_at = [&g](int r, int c) { return (int)g.code[(size_t)r * g.pitch + c]; };
         for (int r0 = 1; r0 <= g.H - 2; r0 += ts.rows) {
-            for (int c0 = -1; c0 + 1 <= g.W - 2; c0 += ts.cols) {
-                int has_exc = 0;
-                for (int r = r0; r < std::min(r0 + ts.rows, g.H - 1) && !has_exc; ++r)
-                    for (int c = std::max(c0 + 1, 0); c <= std::min(c0 + ts.cols, g.W - 1); ++c)
-                        if (g.cell_type[(size_t)r * g.W + c] == VS_CELL_EXCITATION) { has_exc = 1; break; }
-                tiles.push_back({(int32_t)i, r0, c0, has_exc});
+            if (ts.kind == SHAPE_BAND) {
+                // a band covers the full width of rows r0 .. r0+rows-1
+                Tile t{};
+                t.tube = (int32_t)i;
+                t.r0 = r0;
+                for (int r = r0; r < std::min(r0 + ts.rows, g.H - 1) && !t.has_exc; ++r)
+                    for (int c = 0; c < g.W; ++c)
+                        if ((code_at(r, c) & CODE_TYPE_MASK) == VS_CELL_EXCITATION) { t.has_exc = 1; break; }
+                tiles.push_back(t);
+                continue;
+            }
+            // strips start at c0 = kStripCommit*k - kStripLead and commit columns
+            // c0+kStripLead .. c0+kStripLead+kStripCommit-1; rows r0 .. r0+rows-1
+            for (int c0 = -kStripLead; c0 + kStripLead <= g.W - 2; c0 += kStripCommit) {
+                Tile t{};
+                t.tube = (int32_t)i;
+                t.r0 = r0;
+                t.c0 = c0;
+                classify_strip(code_at, g.H, g.W, r0, ts.rows, c0, t);
+                tiles.push_back(t);
             }
         }
     }
@@ -179,7 +211,7 @@ void ensure_graph(vs_batch* b) {
     ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
     for (int i = 0; i < kChunk && err == cudaSuccess; ++i)
-        err = launch_step(b->shape, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream);
+        err = launch_step(b->shape, b->wall, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch);
     if (err == cudaSuccess) err = launch_advance(b->d_rs, kChunk, b->stream);
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     ck(err, "capture step launches");
@@ -227,8 +259,10 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         build_tube(&params[i], geoms ? &geoms[i] : nullptr, b->grids[i], 0);
         std::memcpy(&b->grids[i].src_params, &params[i], sizeof(vs_params));
     }
-    // arena layout: per tube, planes of H*pitch floats (+ codes) + two-mass state
-    size_t total = 0;
+    // arena layout: per tube, planes of H*pitch floats (+ codes) + two-mass
+    // state, with kGuard bytes before the first and after the last tube: the
+    // step kernel reads one element before and up to 29 after a plane
+    size_t total = kGuard;
     std::vector<size_t> base(n);
     for (int i = 0; i < n; ++i) {
         const TubeGrid& g = b->grids[i];
@@ -236,7 +270,12 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
         total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState));
     }
+    total += kGuard;
     b->arena_bytes = total;
+    for (const TubeGrid& g : b->grids) {
+        b->wall = b->wall || g.wall_ode;
+        b->max_pitch = std::max(b->max_pitch, g.pitch);
+    }
     ck(cudaMalloc(&b->arena, total), "cudaMalloc(arena)");
     b->h_tubes.resize(n);
     b->src_len.assign(n, 0);
@@ -285,7 +324,10 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
     upload_sources(b, need);
     upload_static(b);
     reset_state(b);
-    b->shape = kDefaultShape;
+    // small grids (a single tube) need short strips to spread over the SMs
+    int64_t cells = 0;
+    for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
+    b->shape = cells < kSmallGridCells ? kSmallShape : kDefaultShape;
 }
 
 void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
@@ -313,7 +355,7 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     }
     const int rem = (int)(steps - done);
     for (int i = 0; i < rem; ++i)
-        ck(launch_step(b->shape, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream), "step launch");
+        ck(launch_step(b->shape, b->wall, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch), "step launch");
     if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
     b->step += steps;
     if (traces) {
@@ -322,6 +364,9 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
            "copy traces");
     }
     ck(cudaStreamSynchronize(b->stream), "run sync");
+    int32_t dev_error = 0;
+    ck(cudaMemcpy(&dev_error, &b->d_rs->error, sizeof(dev_error), cudaMemcpyDeviceToHost), "read run status");
+    if (dev_error != 0) throw VsFailure{dev_error, "a bounded device wait gave up; the state is not valid"};
     if (traces && !on_device) {
         for (int64_t i = 0; i < need; ++i)
             if (!std::isfinite(traces[i])) throw VsFailure{VS_ERR_NONFINITE, "non-finite listener pressure"};
@@ -412,7 +457,9 @@ int vs_batch_reset(vs_batch* b) {
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index) {
     if (!b || tile_index < -1 || tile_index >= tile_shape_count())
         return set_error(VS_ERR_INVALID_ARG, "tile index out of range");
-    b->shape = tile_index < 0 ? kDefaultShape : tile_index;
+    const int s = tile_index < 0 ? kDefaultShape : tile_index;
+    if (!shape_fits(b, s)) return set_error(VS_ERR_UNSUPPORTED, "launch shape needs more shared memory than the device has");
+    b->shape = s;
     return VS_OK;
 }
 
@@ -425,6 +472,7 @@ int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* be
         float best = 1e30f;
         int best_i = kDefaultShape;
         for (int s = 0; s < tile_shape_count(); ++s) {
+            if (!shape_fits(b, s)) continue;
             b->shape = s;
             run_batch(b, std::min<int64_t>(steps, kChunk), nullptr, 1);   // warm: tiles + graph
             ck(cudaEventRecord(e0, b->stream), "record");

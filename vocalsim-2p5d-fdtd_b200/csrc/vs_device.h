@@ -56,25 +56,95 @@ struct RunState {
     int32_t pad;
 };
 
-// A strip of one tube processed by one warp: rows [r0, r0+rows), lanes on
-// columns c0 .. c0+31, committing columns c0+1 .. c0+cols.
+// Strip geometry of the step kernel: lane i of a warp holds column c0 + i;
+// lanes 0 and 31 are halo, so a strip commits the kStripCommit columns
+// c0 + 1 .. c0 + 30, and strip k of a tube starts at c0 = 30 k - 1.
+constexpr int kStripCommit = 30;
+constexpr int kStripLead = 1;
+constexpr int kMaxStripRows = 62;
+
+// A strip of one tube processed by one warp: rows [r0, r0+rows), starting
+// column c0.  The masks classify its rows once, from the static cell types,
+// so the kernel branches uniformly instead of voting per row:
+//   p_rows     bit j: row r0-1+j has a computed cell whose type is not air
+//              (nonzero sigma or a no-pressure cell)
+//   v_beta1    bit j: committed row r0+j needs at least the beta = 1 update
+//   v_generic  bit j: committed row r0+j needs the full velocity update
 struct Tile {
     int32_t tube, r0, c0, has_exc;
+    uint64_t p_rows, v_beta1, v_generic;
 };
 
-// Host-side description of a compiled launch shape: strip rows, committed
-// columns per strip, warps per CTA.
+// Velocity class a committed cell needs, from the codes of the cell and of its
+// right and top neighbours.
+enum : int { V_PLAIN = 0, V_BETA1 = 1, V_GENERIC = 2 };
+
+__host__ __device__ inline bool beta_one(int t) {
+    // air, PML and no-pressure cells have beta = 1 (SolverParams.cu:5-27)
+    return t == VS_CELL_AIR || t == VS_CELL_NOPRESSURE || (t >= VS_CELL_PML0 && t <= VS_CELL_PML5);
+}
+
+__host__ __device__ inline int velocity_class(int kc, int kr, int kt) {
+    const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
+    if (kc & CODE_ZINV_BIT) return V_GENERIC;
+    if (tc == VS_CELL_AIR && tr == VS_CELL_AIR && tt == VS_CELL_AIR) return V_PLAIN;
+    return (beta_one(tc) && beta_one(tr) && beta_one(tt)) ? V_BETA1 : V_GENERIC;
+}
+
+// Masks and excitation flag of the strip (r0, rows, c0) of an H x W frame;
+// code(r, c) returns the code byte of a frame cell.
+template <class CodeAt>
+__host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0, int rows, int c0, Tile& t) {
+    t.p_rows = 0;
+    t.v_beta1 = 0;
+    t.v_generic = 0;
+    t.has_exc = 0;
+    const int rlast = (r0 + rows - 1 < H - 2) ? r0 + rows - 1 : H - 2;
+    const int cfirst = c0 + 1 > 1 ? c0 + 1 : 1;
+    const int plast = c0 + 31 < W - 2 ? c0 + 31 : W - 2;
+    const int vlast = c0 + kStripCommit < W - 2 ? c0 + kStripCommit : W - 2;
+    for (int r = r0 - 1; r <= rlast; ++r) {
+        if (r >= 1) {
+            for (int c = cfirst; c <= plast; ++c)
+                if ((code(r, c) & CODE_TYPE_MASK) != VS_CELL_AIR) { t.p_rows |= 1ull << (r - r0 + 1); break; }
+        }
+        if (r >= r0) {
+            int cls = V_PLAIN;
+            for (int c = cfirst; c <= vlast; ++c) {
+                const int kc = code(r, c);
+                const int k = velocity_class(kc, code(r, c + 1), code(r - 1, c));
+                cls = k > cls ? k : cls;
+                if ((kc & CODE_TYPE_MASK) == VS_CELL_EXCITATION) t.has_exc = 1;
+            }
+            if (cls >= V_BETA1) t.v_beta1 |= 1ull << (r - r0);
+            if (cls >= V_GENERIC) t.v_generic |= 1ull << (r - r0);
+        }
+    }
+}
+
+// Host-side description of a compiled launch shape.  Strips: rows per strip,
+// committed columns per strip, warps per CTA.  Bands: rows per band (a band
+// spans the full frame width; cols = 0), warps per CTA.
+enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1 };
+
 struct TileShape {
-    int rows, cols, warps;
+    int rows, cols, warps, kind;
 };
 
 int tile_shape_count();
 TileShape tile_shape(int i);
 
 // Launch one time step (local index `local` after RunState::step) of every
-// tile in `tiles` with the compiled tile shape `shape`.
-cudaError_t launch_step(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles,
-                        RunState* rs, int local, cudaStream_t stream);
+// strip or band in `tiles` with the compiled shape `shape`; `wall` selects
+// the kernel variant with the coupled wall oscillator (needed when any tube
+// has it); max_pitch sizes a band kernel's shared memory.
+cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* tiles, int ntiles,
+                        RunState* rs, int local, cudaStream_t stream, int max_pitch);
+
+// Dynamic shared memory a shape needs for frames of row pitch up to
+// max_pitch (0 for strips), and the one-time kernel attribute set-up for it.
+size_t shape_smem_bytes(int shape, int max_pitch);
+cudaError_t prepare_shape(int shape, int max_pitch);
 
 // Set the text vs_last_error() returns on this host thread.
 void record_error(const char* msg);

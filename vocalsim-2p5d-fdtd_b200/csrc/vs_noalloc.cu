@@ -37,7 +37,6 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 constexpr int kShape = 1;          // 16-row strips, 4 warps per CTA
-constexpr int kStripCols = 30;
 
 std::mutex g_mu;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
@@ -88,17 +87,20 @@ __global__ void pack_maps(const int32_t* __restrict__ cell_type, const float* __
 }
 
 // Strip work items of one tube, in the order vs_batch builds them.
-__global__ void make_strips(Tile* __restrict__ tiles, const int32_t* __restrict__ cell_type, int H, int W,
-                            int rows, int nstrips, int nitems) {
+__global__ void make_strips(Tile* __restrict__ tiles, const int32_t* __restrict__ cell_type,
+                            const float* __restrict__ zinv, int H, int W, int rows, int nstrips, int nitems) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nitems) return;
-    const int r0 = 1 + (i / nstrips) * rows;
-    const int c0 = -1 + (i % nstrips) * kStripCols;
-    int has_exc = 0;
-    for (int r = r0; r < min(r0 + rows, H - 1) && !has_exc; ++r)
-        for (int c = max(c0 + 1, 0); c <= min(c0 + kStripCols, W - 1); ++c)
-            if (cell_type[(int64_t)r * W + c] == VS_CELL_EXCITATION) { has_exc = 1; break; }
-    tiles[i] = {0, r0, c0, has_exc};
+    Tile t{};
+    t.tube = 0;
+    t.r0 = 1 + (i / nstrips) * rows;
+    t.c0 = -kStripLead + (i % nstrips) * kStripCommit;
+    auto code_at = [=](int r, int c) {
+        const int64_t s = (int64_t)r * W + c;
+        return (cell_type[s] & CODE_TYPE_MASK) | (zinv[s] != 0.0f ? CODE_ZINV_BIT : 0);
+    };
+    classify_strip(code_at, H, W, t.r0, rows, t.c0, t);
+    tiles[i] = t;
 }
 
 int fail(int status, const char* msg) {
@@ -129,7 +131,7 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     const size_t plane_bytes = up256((size_t)H * pitch * sizeof(float));
     const int nstate = wall ? 10 : 6;
     const int rows = tile_shape(kShape).rows;
-    const int nstrips = (W - 2) / kStripCols + 1;
+    const int nstrips = (W - 2) / kStripCommit + 1;
     const int nitems = ((H - 3) / rows + 1) * nstrips;
     size_t off = 256;                                        // guard ahead of the first plane
     const size_t off_state = off;             off += plane_bytes * nstate;
@@ -206,10 +208,10 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));
     pack_maps<<<592, 256, 0, st>>>(cell_type, depth_p, depth_x, depth_y, z_inv, d0, d0 + pe,
                                    d0 + 2 * pe, base + off_code, H, W, pitch);
-    make_strips<<<(nitems + 127) / 128, 128, 0, st>>>(d_tiles, cell_type, H, W, rows, nstrips, nitems);
+    make_strips<<<(nitems + 127) / 128, 128, 0, st>>>(d_tiles, cell_type, z_inv, H, W, rows, nstrips, nitems);
     e = cudaGetLastError();
     for (int64_t i = 0; i < steps && e == cudaSuccess; ++i)
-        e = launch_step(kShape, d_tube, d_tiles, nitems, d_rs, (int)i, st);
+        e = launch_step(kShape, wall, d_tube, d_tiles, nitems, d_rs, (int)i, st, pitch);
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));
     return VS_OK;
 }

@@ -47,7 +47,6 @@ __constant__ float c_airN[4] = {0.0f, 1.0f, 1.0f, 0.707106f};
 __constant__ float c_wallN[4] = {1.0f, 1.0f, 1.0f, 0.0f};
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kStride = 30;      // committed columns per strip
 
 // betaLookUpTable (FDTDSolver.cu:1047-1056) for beta in {0, 1}:
 // (air, air) -> 0, (air, wall) -> 1, (wall, air) -> 2, (wall, wall) -> 3.
@@ -143,6 +142,11 @@ __device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1
     return ugn;
 }
 
+// a / b for b > 0 with the signed zero returned directly when a is zero:
+// the same value as the division, without sending the zero fields of a cold
+// start through the slow path of the IEEE divide.
+__device__ __forceinline__ float fdiv_z(float a, float b) { return a == 0.0f ? a : fdiv(a, b); }
+
 // Velocity update of one cell, FDTDEngineCPU.cpp:364-410, with the 17
 // coefficient arrays of calculateSolverCoefficients (FDTDSolver.cu:652-801)
 // derived from the cell codes of the cell, its right and its top neighbour.
@@ -150,7 +154,7 @@ struct VelocityOut { float vx, vy; };
 
 __device__ __forceinline__ VelocityOut velocity_generic(
         int kc, int kr, int kt, float pc, float pr, float pt, float vx0, float vy0, float exeV,
-        const float* sig, float zval, float bco, float dir0, float dir1, float dir2, float dir3) {
+        const float* __restrict__ sig, float zval, float bco, float dir0, float dir1, float dir2, float dir3) {
     const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
     const float bc = c_beta[tc], br = c_beta[tr], bt = c_beta[tt];
     const int lut = beta_lut(br, bt);
@@ -181,11 +185,27 @@ __device__ __forceinline__ VelocityOut velocity_generic(
     vby = fmul(fmul(vby, nY), zinv);
     vx = fadd(vx, fmul(mSx, vbx));
     vy = fadd(vy, fmul(mSy, vby));
-    return {fdiv(vx, fadd(mBx, mSx)), fdiv(vy, fadd(mBy, mSy))};
+    return {fdiv_z(vx, fadd(mBx, mSx)), fdiv_z(vy, fadd(mBy, mSy))};
 }
 
-template <int TR>
-__global__ void __launch_bounds__(256, 4)
+// Row-marching strip kernel.  One warp owns a strip of 32 columns x TR rows:
+// lane i holds column c0 + i, strips overlap by two columns (stride 30), so
+// lane 0 only supplies the left depth flux and lane 31 only the right P'
+// neighbour, and lanes 1..30 commit.  Vertical neighbours (P' above, Vy*dY
+// below) stay in registers, horizontal ones move by shuffles: no shared
+// memory and no block barrier.  Each row's loads are issued one iteration
+// before their use.  The strip's row masks (Tile) pick, uniformly per row,
+// the pressure path (sigma = 0 or general) and the velocity class:
+//   V_PLAIN    air cell with air right and top neighbours: beta = 1,
+//              sigma = 0, no source, no boundary term; the reference's full
+//              expression reduces exactly to V - dt/(rho ds) * dP'
+//   V_BETA1    air / PML / no-pressure cells only: the source and boundary
+//              terms add exact zeros, leaving the PML division
+//   V_GENERIC  walls, excitation cells, admittance: the full expression
+// Every shortened path drops only operations whose operands are exact 0 / 1
+// (x*1, x+0, x/1), so values equal the full reference expression.
+template <int TR, int MINB, bool WALL>
+__global__ void __launch_bounds__(256, MINB)
 strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
              RunState* __restrict__ rs, int local) {
     const int lane = threadIdx.x & 31;
@@ -197,10 +217,13 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     const int par = (int)(n & 1);
     const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
     const int r0 = it.r0, x = it.c0 + lane;
-    const bool col_ok = x >= 0 && x < W;
     const bool col_in = x >= 1 && x <= W - 2;
-    const bool commit_lane = lane >= 1 && lane <= kStride;
-    // planes are laid out P0 P1 Vx0 Vx1 Vy0 Vy1 and dP dX dY, `plane` apart
+    const bool lane_calc = col_in && lane >= 1;
+    const bool lane_commit = lane_calc && lane <= kStripCommit;
+    // planes are laid out P0 P1 Vx0 Vx1 Vy0 Vy1 and dP dX dY, `plane` apart.
+    // Lanes read columns -1 .. W+28 of rows 0 .. H-1 without predicates: the
+    // arena keeps guard bytes around every tube, and values read outside the
+    // frame only reach lanes that neither compute nor commit them.
     const int64_t pl = T->plane;
     const float* __restrict__ Pin = T->P[0] + par * pl;
     float* __restrict__ Pout = T->P[0] + (par ^ 1) * pl;
@@ -212,10 +235,11 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     const float* __restrict__ dXp = dPp + pl;
     const float* __restrict__ dYp = dPp + 2 * pl;
     const uint8_t* __restrict__ code = T->code;
-    const float K1 = T->K1, K2 = T->K2, bco = T->bcoef, zval = T->zinv;
-    const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
-    const bool wall = flags & TUBE_WALL_ODE;
     const float* __restrict__ sig = T->sigma;
+    const float K1 = T->K1, bco = T->bcoef;
+    const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
+    const int lis_y = T->lis_y, lis_x = T->lis_x;
+    const uint64_t pmask = it.p_rows, vb1 = it.v_beta1, vgen = it.v_generic;
 
     // excitation velocity of this step (only strips holding excitation cells need it)
     float exeV = 0.0f;
@@ -227,7 +251,8 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                 TmmState s = T->tmm[par];
                 exeV = tmm_step(T->tmmc, s, Pin[(size_t)T->exc_y * pitch + T->exc_x]);
                 const int ex = T->exc_x - it.c0;
-                if (T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= 1 && ex <= kStride) T->tmm[par ^ 1] = s;
+                if (T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= kStripLead && ex < kStripLead + kStripCommit)
+                    T->tmm[par ^ 1] = s;
             }
             exeV = __shfl_sync(kFull, exeV, 0);
         } else {
@@ -236,126 +261,391 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     }
     const int rlast = min(r0 + TR - 1, H - 2);
 
-    // prologue: the row above the strip (r0 - 1) supplies P' and codes for the
-    // top neighbours of row r0; its own P' is recomputed, not committed.
+    // Row pipeline: iteration j (row r = r0 - 1 + j) computes P' of row r
+    // and, from row r0 on, commits it with V' of row r; it issues the loads
+    // of row r+1 (Vx, dX, P, dP, code) and row r+2 (Vy, dY).  The row above
+    // the strip supplies P' and codes for the top neighbours of row r0; its
+    // own P' is recomputed, not committed.
     int r = r0 - 1;
-    size_t o = (size_t)r * pitch + x;
-    float vy_c = 0.0f, uy_c = 0.0f;
-    if (col_ok) { vy_c = Vyin[o]; uy_c = fmul(vy_c, dYp[o]); }
-    float vx_c = 0.0f, ux_c = 0.0f, p_c = 0.0f, dp_c = 1.0f;
-    int k_c = VS_CELL_DEAD;
-    if (col_ok) {
-        vx_c = Vxin[o]; ux_c = fmul(vx_c, dXp[o]); p_c = Pin[o]; dp_c = dPp[o]; k_c = code[o];
-    }
+    int o = r * pitch + x;
+    float vx_c = __ldg(Vxin + o);
+    float ux_c = fmul(vx_c, __ldg(dXp + o));
+    float p_c = __ldg(Pin + o), dp_c = __ldg(dPp + o);
+    int k_c = __ldg(code + o);
+    float vy_c = __ldg(Vyin + o);
+    float uy_c = fmul(vy_c, __ldg(dYp + o));
+    float vy_n = __ldg(Vyin + o + pitch);
+    float uy_n = fmul(vy_n, __ldg(dYp + o + pitch));
     float p_above = 0.0f;
     int k_above = VS_CELL_DEAD;
 
-    for (; r <= rlast; ++r) {
-        // ---- issue next-row loads first (row r+1 fields, row r+2 Vy/dY)
-        const size_t on = o + pitch;
-        float vy_n = 0.0f, uy_n = 0.0f;
-        float vx_n = 0.0f, ux_n = 0.0f, p_n = 0.0f, dp_n = 1.0f;
-        int k_n = VS_CELL_DEAD;
-        if (col_ok) {                       // r + 1 <= H - 1 always holds here
-            vy_n = Vyin[on]; uy_n = fmul(vy_n, dYp[on]);
-            vx_n = Vxin[on]; ux_n = fmul(vx_n, dXp[on]); p_n = Pin[on]; dp_n = dPp[on]; k_n = code[on];
-        }
+    for (int j = 0; r <= rlast; ++j, ++r) {
+        // ---- loads for the next iterations
+        const int o1 = o + pitch;
+        // (read-only this step: the input planes are not the ones written)
+        const float vx_1 = __ldg(Vxin + o1), dx_1 = __ldg(dXp + o1);
+        const float p_1 = __ldg(Pin + o1), dp_1 = __ldg(dPp + o1);
+        const int k_1 = __ldg(code + o1);
+        float vy_2 = 0.0f, dy_2 = 0.0f;
+        if (r + 2 <= H - 1) { vy_2 = __ldg(Vyin + o1 + pitch); dy_2 = __ldg(dYp + o1 + pitch); }
+
         // ---- pressure of row r (FDTDEngineCPU.cpp:316-339)
         const float ux_l = __shfl_up_sync(kFull, ux_c, 1);
-        const bool in = col_in && r >= 1;
+        const bool calc = lane_calc && r >= 1;
         const int tc = k_c & CODE_TYPE_MASK;
-        const bool plain_p = (tc == VS_CELL_AIR) || !(in && lane >= 1);
-        float pn = 0.0f;
+        float num = fsub(fmul(p_c, dp_c), fmul(K1, fadd(fsub(ux_c, ux_l), fsub(uy_c, uy_n))));
         float w = 0.0f;
-        if (__all_sync(kFull, plain_p) && !wall) {
-            if (in && lane >= 1) {
-                // sigma = 0: (1 + 0) * dP == 0 * dP + dP == dP exactly
-                const float cx = fsub(ux_c, ux_l), cy = fsub(uy_c, uy_n);
-                pn = fdiv(fsub(fmul(p_c, dp_c), fmul(K1, fadd(cx, cy))), dp_c);
-            }
-        } else if (in && lane >= 1) {
-            const float cx = fsub(ux_c, ux_l), cy = fsub(uy_c, uy_n);
-            float num = fsub(fmul(p_c, dp_c), fmul(K1, fadd(cx, cy)));
-            if (wall) {
-                w = T->w[par][o];
-                num = fsub(num, fmul(K2, w));
-            }
+        if (WALL) {
+            if (calc) w = T->w[par][o];
+            num = fsub(num, fmul(T->K2, w));
+        }
+        const bool pgen = (pmask >> j) & 1;
+        float den = dp_c;                  // sigma = 0: (1 + 0) * dP == 0 * dP + dP == dP
+        if (pgen && tc != VS_CELL_AIR) {
             const float s = sig[tc];
-            const float den = eigen ? fadd(fmul(s, dp_c), dp_c) : fmul(fadd(1.0f, s), dp_c);
-            pn = fdiv(num, den);
-            if (dirichlet && tc == VS_CELL_NOPRESSURE) pn = 0.0f;
+            den = eigen ? fadd(fmul(s, dp_c), dp_c) : fmul(fadd(1.0f, s), dp_c);
+        }
+        float pn = 0.0f;
+        if (calc) {
+            pn = fdiv_z(num, den);
+            if (pgen && dirichlet && tc == VS_CELL_NOPRESSURE) pn = 0.0f;
         }
         // ---- commit row r and its velocity (FDTDEngineCPU.cpp:364-410)
         const float p_right = __shfl_down_sync(kFull, pn, 1);
         const int k_right = __shfl_down_sync(kFull, k_c, 1);
-        if (r >= r0) {
-            const bool mine = in && commit_lane;
-            if (mine) {
+        if (j >= 1) {
+            const int jv = j - 1;
+            if (lane_commit) {
                 Pout[o] = pn;
-                if (r == T->lis_y && x == T->lis_x)
+                if (r == lis_y && x == lis_x)
                     rs->trace[(int64_t)it.tube * rs->trace_stride + (n - rs->run_start)] = pn;
-                if (wall) {
+                if (WALL) {
                     // wall oscillator, FDTDEngineCPU.cpp:345-361
                     const float dt = T->dt;
                     const float zn = fadd(T->z[par][o], fmul(w, dt));
-                    const float wn = fdiv(fsub(fadd(fmul(T->Mw, w), fmul(fmul(T->cpl, dt), pn)),
-                                              fmul(fmul(dt, T->Kw), zn)),
-                                         fadd(T->Mw, fmul(dt, T->Bw)));
                     T->z[par ^ 1][o] = zn;
-                    T->w[par ^ 1][o] = wn;
+                    T->w[par ^ 1][o] = fdiv_z(fsub(fadd(fmul(T->Mw, w), fmul(fmul(T->cpl, dt), pn)),
+                                                   fmul(fmul(dt, T->Kw), zn)),
+                                              fadd(T->Mw, fmul(dt, T->Bw)));
                 }
             }
-            const int tr = k_right & CODE_TYPE_MASK, tt = k_above & CODE_TYPE_MASK;
-            const bool plain_v = !mine || (tc == VS_CELL_AIR && tr == VS_CELL_AIR && tt == VS_CELL_AIR &&
-                                           !(k_c & CODE_ZINV_BIT));
-            if (__all_sync(kFull, plain_v)) {
-                if (mine) {
-                    // beta = 1, sigma = 0, no source, no boundary term:
-                    // V' = V - (dt/(rho ds)) * dP' exactly as the full expression
-                    Vxout[o] = fsub(vx_c, fmul(bco, fsub(p_right, pn)));
-                    Vyout[o] = fsub(vy_c, fmul(bco, fsub(p_above, pn)));
+            float vx, vy;
+            if ((vgen >> jv) & 1) {
+                vx = 0.0f;
+                vy = 0.0f;
+                if (lane_commit) {
+                    const VelocityOut v = velocity_generic(k_c, k_right, k_above, pn, p_right, p_above, vx_c, vy_c,
+                                                           exeV, sig, T->zinv, bco, T->dir0, T->dir1, T->dir2,
+                                                           T->dir3);
+                    vx = v.vx;
+                    vy = v.vy;
                 }
-            } else if (mine) {
-                const VelocityOut v = velocity_generic(k_c, k_right, k_above, pn, p_right, p_above, vx_c, vy_c,
-                                                       exeV, sig, zval, bco, T->dir0, T->dir1, T->dir2, T->dir3);
-                Vxout[o] = v.vx;
-                Vyout[o] = v.vy;
+            } else {
+                vx = fsub(vx_c, fmul(bco, fsub(p_right, pn)));
+                vy = fsub(vy_c, fmul(bco, fsub(p_above, pn)));
+                if ((vb1 >> jv) & 1) {
+                    const float sc = sig[tc];
+                    vx = fdiv_z(vx, fadd(1.0f, fmaxf(sc, sig[k_right & CODE_TYPE_MASK])));
+                    vy = fdiv_z(vy, fadd(1.0f, fmaxf(sc, sig[k_above & CODE_TYPE_MASK])));
+                }
+            }
+            if (lane_commit) {
+                Vxout[o] = vx;
+                Vyout[o] = vy;
             }
         }
         // ---- shift the row pipeline
         p_above = pn; k_above = k_c;
         vy_c = vy_n; uy_c = uy_n;
-        vx_c = vx_n; ux_c = ux_n; p_c = p_n; dp_c = dp_n; k_c = k_n;
-        o = on;
+        vy_n = vy_2; uy_n = fmul(vy_2, dy_2);
+        vx_c = vx_1; ux_c = fmul(vx_1, dx_1); p_c = p_1; dp_c = dp_1; k_c = k_1;
+        o = o1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Band kernel: one CTA per band of R rows of a tube.  A band's rows are
+// contiguous in every plane (rows are `pitch` apart), so the rows r0-1 ..
+// r0+R of P, Vx, Vy, dP, dX, dY and the codes arrive with one bulk copy per
+// plane (cp.async.bulk, completion on an mbarrier) and no registers held in
+// flight.  The CTA then computes P' for rows r0-1 .. r0+R-1 into shared
+// memory and V' for rows r0 .. r0+R-1, with the same arithmetic as the
+// strip kernel (value-identical to the reference expressions), and stores
+// both to global memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// global -> shared bulk copy (no multicast); dst, src 16-byte aligned, bytes % 16 == 0
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Bounded wait on phase 0 of an mbarrier: gives up after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, 0)) return true;
+    return false;
+}
+
+constexpr uint32_t kWaitPolls = 1u << 22;
+constexpr int kBandThreads = 256;
+
+// Shared-memory bytes of a band kernel with R rows for a row pitch.
+__host__ __device__ inline size_t band_smem_bytes(int R, int pitch) {
+    const size_t plane = (size_t)(R + 2) * pitch * sizeof(float);
+    const size_t codes = ((size_t)(R + 2) * pitch + 127) / 128 * 128;
+    return 6 * plane + codes + (size_t)(R + 1) * pitch * sizeof(float);
+}
+
+template <int R, bool WALL>
+__global__ void __launch_bounds__(kBandThreads)
+band_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ bands, int nbands,
+            RunState* __restrict__ rs, int local) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    __shared__ float s_exe;
+    if ((int)blockIdx.x >= nbands) return;
+    const Tile bd = bands[blockIdx.x];
+    const TubeDev* __restrict__ T = tubes + bd.tube;
+    const int64_t n = rs->step + local;
+    const int par = (int)(n & 1);
+    const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
+    const int r0 = bd.r0;
+    const int rfirst = r0 - 1;                          // first row held in shared memory
+    const int rload = min(r0 + R, H - 1);               // last row held
+    const int nload = rload - rfirst + 1;
+    const int rcommit = min(r0 + R - 1, H - 2);         // last row this band commits
+    const int64_t pl = T->plane;
+    const float* __restrict__ Pin = T->P[0] + par * pl;
+    float* __restrict__ Pout = T->P[0] + (par ^ 1) * pl;
+    const float* __restrict__ Vxin = Pin + 2 * pl;
+    const float* __restrict__ Vyin = Pin + 4 * pl;
+    float* __restrict__ Vxout = Pout + 2 * pl;
+    float* __restrict__ Vyout = Pout + 4 * pl;
+    const float* __restrict__ dPp = T->dP;
+    const size_t plane_sm = (size_t)(R + 2) * pitch;
+    float* sP = reinterpret_cast<float*>(smem);
+    float* sVx = sP + plane_sm;
+    float* sVy = sVx + plane_sm;
+    float* sdP = sVy + plane_sm;
+    float* sdX = sdP + plane_sm;
+    float* sdY = sdX + plane_sm;
+    uint8_t* sK = reinterpret_cast<uint8_t*>(sdY + plane_sm);
+    float* sPn = reinterpret_cast<float*>(sK + (plane_sm + 127) / 128 * 128);
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const size_t off = (size_t)rfirst * pitch;
+        const uint32_t fbytes = (uint32_t)(nload * pitch * sizeof(float));
+        const uint32_t kbytes = (uint32_t)(((size_t)nload * pitch + 15) / 16 * 16);
+        mbar_expect_tx(&bar, 6 * fbytes + kbytes);
+        bulk_g2s(sP, Pin + off, fbytes, &bar);
+        bulk_g2s(sVx, Vxin + off, fbytes, &bar);
+        bulk_g2s(sVy, Vyin + off, fbytes, &bar);
+        bulk_g2s(sdP, dPp + off, fbytes, &bar);
+        bulk_g2s(sdX, dPp + pl + off, fbytes, &bar);
+        bulk_g2s(sdY, dPp + 2 * pl + off, fbytes, &bar);
+        bulk_g2s(sK, T->code + off, kbytes, &bar);
+        // excitation velocity of this step, while the copies are in flight
+        float e = 0.0f;
+        if (bd.has_exc) {
+            if (flags & TUBE_TMM) {
+                TmmState s = T->tmm[par];
+                e = tmm_step(T->tmmc, s, Pin[(size_t)T->exc_y * pitch + T->exc_x]);
+                if (T->exc_y >= r0 && T->exc_y <= rcommit) T->tmm[par ^ 1] = s;
+            } else {
+                e = n < T->src_len ? T->src[n] : 0.0f;
+            }
+        }
+        s_exe = e;
+    }
+    if (!mbar_wait_bounded(&bar, kWaitPolls)) {
+        // the copies did not land: flag the run, let them finish, and leave
+        if (threadIdx.x == 0) atomicExch(&rs->error, VS_ERR_TIMEOUT);
+        mbar_wait_bounded(&bar, kWaitPolls);
+        return;
+    }
+    __syncthreads();
+    const float exeV = s_exe;
+    const float* __restrict__ sig = T->sigma;
+    const float K1 = T->K1, bco = T->bcoef;
+    const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nseg = (W + 31) >> 5;
+
+    // ---- P' of rows rfirst .. rcommit (row index i = r - rfirst)
+    const int prow = rcommit - rfirst + 1;
+    for (int q = warp; q < prow * nseg; q += kBandThreads / 32) {
+        const int i = q / nseg;
+        const int c = (q - i * nseg) * 32 + lane;
+        const int r = rfirst + i;
+        float pn = 0.0f;
+        float w = 0.0f;
+        const int k = i * pitch + c;
+        if (r >= 1 && c >= 1 && c <= W - 2) {
+            const int tc = sK[k] & CODE_TYPE_MASK;
+            const float dp = sdP[k];
+            const float cx = fsub(fmul(sVx[k], sdX[k]), fmul(sVx[k - 1], sdX[k - 1]));
+            const float cy = fsub(fmul(sVy[k], sdY[k]), fmul(sVy[k + pitch], sdY[k + pitch]));
+            float num = fsub(fmul(sP[k], dp), fmul(K1, fadd(cx, cy)));
+            const int64_t o = (int64_t)r * pitch + c;
+            if (WALL) {
+                w = T->w[par][o];
+                num = fsub(num, fmul(T->K2, w));
+            }
+            float den = dp;                       // sigma = 0: (1 + 0) * dP == dP
+            if (tc != VS_CELL_AIR) {
+                const float s = sig[tc];
+                den = eigen ? fadd(fmul(s, dp), dp) : fmul(fadd(1.0f, s), dp);
+            }
+            pn = fdiv_z(num, den);
+            if (dirichlet && tc == VS_CELL_NOPRESSURE) pn = 0.0f;
+            if (r >= r0) {
+                Pout[o] = pn;
+                if (r == T->lis_y && c == T->lis_x)
+                    rs->trace[(int64_t)bd.tube * rs->trace_stride + (n - rs->run_start)] = pn;
+                if (WALL) {
+                    // wall oscillator, FDTDEngineCPU.cpp:345-361
+                    const float dt = T->dt;
+                    const float zn = fadd(T->z[par][o], fmul(w, dt));
+                    T->z[par ^ 1][o] = zn;
+                    T->w[par ^ 1][o] = fdiv_z(fsub(fadd(fmul(T->Mw, w), fmul(fmul(T->cpl, dt), pn)),
+                                                   fmul(fmul(dt, T->Kw), zn)),
+                                              fadd(T->Mw, fmul(dt, T->Bw)));
+                }
+            }
+        }
+        if (c < pitch) sPn[k] = pn;
+    }
+    __syncthreads();
+
+    // ---- V' of rows r0 .. rcommit
+    const int vrow = rcommit - r0 + 1;
+    for (int q = warp; q < vrow * nseg; q += kBandThreads / 32) {
+        const int i = 1 + q / nseg;
+        const int c = (q - (i - 1) * nseg) * 32 + lane;
+        if (c < 1 || c > W - 2) continue;
+        const int r = rfirst + i;
+        const int k = i * pitch + c;
+        const int kc = sK[k], kr = sK[k + 1], kt = sK[k - pitch];
+        const float pc = sPn[k], pr = sPn[k + 1], pt = sPn[k - pitch];
+        const float vx0 = sVx[k], vy0 = sVy[k];
+        const int cls = velocity_class(kc, kr, kt);
+        float vx, vy;
+        if (cls == V_GENERIC) {
+            const VelocityOut v = velocity_generic(kc, kr, kt, pc, pr, pt, vx0, vy0, exeV, sig, T->zinv, bco,
+                                                   T->dir0, T->dir1, T->dir2, T->dir3);
+            vx = v.vx;
+            vy = v.vy;
+        } else {
+            vx = fsub(vx0, fmul(bco, fsub(pr, pc)));
+            vy = fsub(vy0, fmul(bco, fsub(pt, pc)));
+            if (cls == V_BETA1) {
+                const float sc = sig[kc & CODE_TYPE_MASK];
+                vx = fdiv_z(vx, fadd(1.0f, fmaxf(sc, sig[kr & CODE_TYPE_MASK])));
+                vy = fdiv_z(vy, fadd(1.0f, fmaxf(sc, sig[kt & CODE_TYPE_MASK])));
+            }
+        }
+        const int64_t o = (int64_t)r * pitch + c;
+        Vxout[o] = vx;
+        Vyout[o] = vy;
     }
 }
 
 __global__ void advance_kernel(RunState* rs, int k) { rs->step += k; }
 
+using StepFn = void (*)(const TubeDev*, const Tile*, int, RunState*, int);
+
 struct ShapeEntry {
-    int rows, warps;
-    void (*fn)(const TubeDev*, const Tile*, int, RunState*, int);
+    int kind, rows, warps;
+    StepFn plain, wall;
 };
 
+#define VS_STRIP(R, WARPS, MINB) \
+    {SHAPE_STRIP, R, WARPS, strip_kernel<R, MINB, false>, strip_kernel<R, MINB, true>}
+#define VS_BAND(R) {SHAPE_BAND, R, kBandThreads / 32, band_kernel<R, false>, band_kernel<R, true>}
+
+// strips: (rows per strip, warps per CTA, CTAs per SM the register budget
+// targets); bands: rows per band (one CTA of 256 threads each)
 const ShapeEntry kShapes[] = {
-    {8, 4, strip_kernel<8>},   {16, 4, strip_kernel<16>}, {32, 4, strip_kernel<32>}, {64, 4, strip_kernel<64>},
-    {8, 8, strip_kernel<8>},   {16, 8, strip_kernel<16>}, {32, 8, strip_kernel<32>}, {64, 8, strip_kernel<64>},
+    VS_STRIP(4, 4, 4),  VS_STRIP(16, 4, 4), VS_STRIP(8, 4, 4),  VS_STRIP(32, 4, 4),
+    VS_STRIP(8, 8, 4),  VS_STRIP(16, 8, 4), VS_STRIP(32, 8, 4), VS_STRIP(2, 2, 4),
+    VS_STRIP(4, 2, 4),  VS_STRIP(8, 2, 4),  VS_STRIP(16, 4, 3), VS_STRIP(8, 4, 3),
+    VS_BAND(4),         VS_BAND(8),         VS_BAND(12),        VS_BAND(16),
 };
+#undef VS_STRIP
+#undef VS_BAND
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 }  // namespace
 
 int tile_shape_count() { return kNumShapes; }
 
-TileShape tile_shape(int i) { return {kShapes[i].rows, kStride, kShapes[i].warps}; }
+TileShape tile_shape(int i) {
+    const ShapeEntry& e = kShapes[i];
+    return {e.rows, e.kind == SHAPE_STRIP ? kStripCommit : 0, e.warps, e.kind};
+}
 
-cudaError_t launch_step(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles,
-                        RunState* rs, int local, cudaStream_t stream) {
+size_t shape_smem_bytes(int shape, int max_pitch) {
+    if (shape < 0 || shape >= kNumShapes || kShapes[shape].kind != SHAPE_BAND) return 0;
+    return band_smem_bytes(kShapes[shape].rows, max_pitch);
+}
+
+cudaError_t prepare_shape(int shape, int max_pitch) {
+    const size_t bytes = shape_smem_bytes(shape, max_pitch);
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kShapes[shape].plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kShapes[shape].wall, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return e;
+}
+
+cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* tiles, int ntiles,
+                        RunState* rs, int local, cudaStream_t stream, int max_pitch) {
     if (shape < 0 || shape >= kNumShapes) return cudaErrorInvalidValue;
     if (ntiles <= 0) return cudaSuccess;
-    const int wpb = kShapes[shape].warps;
-    const int blocks = (ntiles + wpb - 1) / wpb;
-    kShapes[shape].fn<<<blocks, wpb * 32, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    const ShapeEntry& e = kShapes[shape];
+    const StepFn fn = wall ? e.wall : e.plain;
+    if (e.kind == SHAPE_BAND) {
+        fn<<<ntiles, kBandThreads, band_smem_bytes(e.rows, max_pitch), stream>>>(tubes, tiles, ntiles, rs, local);
+    } else {
+        const int wpb = e.warps;
+        fn<<<(ntiles + wpb - 1) / wpb, wpb * 32, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    }
     return cudaGetLastError();
 }
 
