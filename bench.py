@@ -41,12 +41,27 @@ PEAKS = REPO / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 
 
+def rank_tube_seeds(rank: int, n_tubes: int) -> list[int]:
+    """Seeds of the tubes rank `rank` owns: every rank runs its own disjoint batch (weak scaling)."""
+    return [rank * n_tubes + i for i in range(n_tubes)]
+
+
+def max_over_ranks(ms: float, world: int, device=None) -> float:
+    """Slowest rank's time; the aggregate throughput divides all ranks' work by it."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload_params(rank: int, n_tubes: int):
     from vocalsim_b200 import synthetic as S
     import vocalsim_b200 as V
     ps, gs = [], []
-    for i in range(n_tubes):
-        L, A, _, _ = S.batch_tube(rank * n_tubes + i)
+    for seed in rank_tube_seeds(rank, n_tubes):
+        L, A, _, _ = S.batch_tube(seed)
         ps.append(V.params(cross_sectional_shape=2, num_steps=SIM_STEPS))
         gs.append(V.Geometry(L, A))
     return ps, gs
@@ -57,6 +72,16 @@ def hbm_peak():
         d = json.loads(PEAKS.read_text())
         return float(d["hbm_gbs"]), "measured"
     return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(cells: int):
+    """DRAM bytes (read + write) per step-kernel launch from the committed ncu summary, when it
+    was captured on this same workload (same interior cell count); else None."""
+    f = REPO / "profiles" / "strip_kernel_batch256.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    return int(d["dram_bytes_per_launch"]) if int(d.get("interior_cells", -1)) == int(cells) else None
 
 
 class ClockSampler:
@@ -222,11 +247,9 @@ def run_b200(args, rank, world):
         e1.record(stream)
         torch.cuda.synchronize()
     ms_total = e0.elapsed_time(e1)
-    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.barrier()
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_total = float(t.item())
+    ms_total = max_over_ranks(ms_total, world, dev)
     ms_step = ms_total / args.steps
     cell_updates_rank = cells * sim_steps
     value = cell_updates_rank * world / (ms_step / 1e3) / 1e9
@@ -301,7 +324,7 @@ def run_b200(args, rank, world):
                    "tile": list(V.tile_shapes()[tile]), "parallelism": f"tube sharding x{world} (no collective)",
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved_gbs / peak, 4), "traffic": None,
+                     "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells),
                      "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell-update x {cells} cells per launch / "
                              f"mean launch time {launch_ms * 1e3:.2f} us; peak {peak_kind}"},
         "gpu_launches": args.steps * launches_per_forward,
