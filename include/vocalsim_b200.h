@@ -221,6 +221,28 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
 
 void vs_batch_destroy(vs_batch* b);
 
+/* ---- gradients: checkpointed forward + reverse-time discrete adjoint -----
+ * No counterpart in the reference (it has no differentiation).  The adjoint
+ * covers table sources (Gaussian, sine) without wall coupling; the two-mass
+ * source and the coupled wall return VS_ERR_UNSUPPORTED. */
+
+/* Replace tube i's depth maps (frameH*frameW each, NULL keeps one) and its
+ * z_inv value; cell types stay.  Invalidates stored checkpoints. */
+int vs_batch_set_maps(vs_batch* b, int32_t tube, const float* depth_p, const float* depth_x,
+                      const float* depth_y, float z_inv);
+
+/* Forward `steps` steps from rest, keeping a state checkpoint every
+ * ckpt_every steps for vs_batch_adjoint; traces (host, n x steps) may be NULL. */
+int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces);
+
+/* Gradients of a loss L(traces) given dL/dtrace (host, n x steps of the last
+ * vs_batch_forward_ckpt): per-cell dL/d depth_p, depth_x, depth_y (host, the
+ * tubes' frames concatenated) and dL/d z_inv per tube (n).  Each segment of
+ * ckpt_every steps is recomputed from its checkpoint, then stepped backwards.
+ * Any output pointer may be NULL. */
+int vs_batch_adjoint(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, float* grad_depth_x,
+                     float* grad_depth_y, float* grad_z_inv);
+
 /* ---- running without allocating ------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * when they step a tube: a real-time audio host calling from its processing

@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
         L.orc_tmm_f64.argtypes = [C.c_float, C.c_int, dp, C.c_longlong, dp]
         L.orc_run_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, fp]
         L.orc_run_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, dp]
+        L.orc_run_maps_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, C.c_double, dp]
         _orc = L
     return _orc
 
@@ -167,6 +168,15 @@ def run(p: VsParams, g: Geometry | None, steps: int, precision: str = "f32", fie
         return tr
     shp = (m["frame_h"], m["frame_w"])
     return tr, [a.reshape(shp) for a in F]
+
+
+def run_maps_f64(p: VsParams, g: Geometry | None, steps: int, depth_p, depth_x, depth_y, z_inv: float) -> np.ndarray:
+    """Double-precision trace of the engine on the given depth maps and z_inv value."""
+    mp, mx, my = (np.ascontiguousarray(a, np.float64).reshape(-1) for a in (depth_p, depth_x, depth_y))
+    tr = np.zeros(steps, np.float64)
+    _check(lib().orc_run_maps_f64(C.byref(p), g.ref() if g is not None else None, steps, _dp(mp), _dp(mx), _dp(my),
+                                  float(z_inv), _dp(tr)), "run_maps_f64")
+    return tr
 
 
 def source(p: VsParams, n: int) -> np.ndarray:

@@ -741,7 +741,9 @@ struct Cell { T Pr, Vx, Vy; int cell_type; };
 
 template <typename T>
 int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long steps,
-               T* trace, T* outP, T* outVx, T* outVy) {
+               T* trace, T* outP, T* outVx, T* outVy,
+               const std::vector<double>* ovP = nullptr, const std::vector<double>* ovX = nullptr,
+               const std::vector<double>* ovY = nullptr, const std::vector<double>* ovZ = nullptr) {
     const int H = G.H, W = G.W, ir = H - 2, ic = W - 2;
     const size_t N = (size_t)H * W;
     std::vector<Cell<T>> PN(N), PN1(N);
@@ -749,6 +751,10 @@ int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long ste
     PN1 = PN;
     std::vector<T> dP(N), dX(N), dY(N), zinv(N);
     for (size_t i = 0; i < N; i++) { dP[i] = G.dP[i]; dX[i] = G.dX[i]; dY[i] = G.dY[i]; zinv[i] = G.zinv[i]; }
+    if (ovP) for (size_t i = 0; i < N; i++) dP[i] = (T)(*ovP)[i];
+    if (ovX) for (size_t i = 0; i < N; i++) dX[i] = (T)(*ovX)[i];
+    if (ovY) for (size_t i = 0; i < N; i++) dY[i] = (T)(*ovY)[i];
+    if (ovZ) for (size_t i = 0; i < N; i++) zinv[i] = (T)(*ovZ)[i];
     const size_t n = (size_t)ir * ic;
     auto cv = [&](const std::vector<float>& v) { return std::vector<T>(v.begin(), v.end()); };
     std::vector<T> Nout = cv(C.N_out), Nin = cv(C.N_in), mBx = cv(C.minVxB), mBy = cv(C.minVyB),
@@ -871,6 +877,12 @@ int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long ste
         if (outVy) outVy[i] = PN[i].Vy;
     }
     return VS_OK;
+}
+
+int run_engine_maps(const vs_params* p, const Grid& G, const Coeffs& C, long long steps,
+                    const std::vector<double>& mP, const std::vector<double>& mX, const std::vector<double>& mY,
+                    const std::vector<double>& mZ, double* trace) {
+    return run_engine<double>(p, G, C, steps, trace, nullptr, nullptr, nullptr, &mP, &mX, &mY, &mZ);
 }
 
 thread_local std::string g_err;
@@ -1023,6 +1035,24 @@ int orc_run_f32(const vs_params* p, const vs_geometry* g, long long steps, float
         Coeffs C;
         build_coeffs(G, C);
         return run_engine<float>(p, G, C, steps, trace, P, Vx, Vy);
+    } catch (const OracleError& e) { return fail(e); }
+}
+
+/* The double engine on caller-supplied depth maps (frameH*frameW each) and
+ * z_inv value (applied where the reference puts z_inv: boundary segment id
+ * != 0); cell types, listener and sources from (p, g).  Finite differences of
+ * this function check the adjoint's map and admittance gradients. */
+int orc_run_maps_f64(const vs_params* p, const vs_geometry* g, long long steps, const double* dP,
+                     const double* dX, const double* dY, double zinv_val, double* trace) {
+    try {
+        Grid G;
+        build_grid(p, g, G);
+        Coeffs C;
+        build_coeffs(G, C);
+        const size_t N = (size_t)G.H * G.W;
+        std::vector<double> mP(dP, dP + N), mX(dX, dX + N), mY(dY, dY + N), zin(N, 0.0);
+        for (size_t i = 0; i < N; i++) if (G.bst[i] != 0) zin[i] = zinv_val;
+        return run_engine_maps(p, G, C, steps, mP, mX, mY, zin, trace);
     } catch (const OracleError& e) { return fail(e); }
 }
 

@@ -1,0 +1,91 @@
+"""Adjoint gradients (vs_batch_forward_ckpt + vs_batch_adjoint) against
+central finite differences of the double-precision oracle.
+
+Loss: L = 1/2 sum_n w_n y_n^2 over the listener trace y.  The adjoint gives
+per-cell dL/d(depth_p, depth_x, depth_y) and dL/d z_inv; their directional
+derivative along a random relative perturbation of the maps must match the
+central difference [L(+h) - L(-h)] / 2h of the FP64 restatement with h = 1e-4
+(relative), within 1e-3 relative error.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import vocalsim_b200 as V
+from vocalsim_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+H_REL = 1e-4
+TOL = 1e-3
+
+
+def _loss(trace, w):
+    t = np.asarray(trace, np.float64)
+    return 0.5 * float(np.sum(w * t * t))
+
+
+def _check(kw, L, A, steps, every, parts, seed=0):
+    pv, gv = V.params(**kw), V.Geometry(L, A)
+    po, go = O.params(**kw), O.Geometry(L, A)
+    m = V.build_maps(pv, gv)
+    b = V.Batch([pv], [gv])
+    tr = b.forward_ckpt(steps, every)[0]
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(0.5, 1.5, steps)
+    grads, gz = b.adjoint((w * tr.astype(np.float64)).astype(np.float32)[None])
+    gP, gX, gY = grads[0]
+    shape = m["depth_p"].shape
+    interior = np.zeros(shape, bool)
+    interior[1:-1, 1:-1] = True
+    d = {k: (rng.uniform(-1, 1, shape) * interior if k in parts else np.zeros(shape)) for k in ("P", "X", "Y")}
+    dz = rng.uniform(-1, 1) if "Z" in parts else 0.0
+    base = {k: m[f"depth_{k.lower()}"].astype(np.float64) for k in ("P", "X", "Y")}
+    z0 = float(m["dims"]["z_inv_val"])
+    adj = (np.sum(gP * base["P"] * d["P"]) + np.sum(gX * base["X"] * d["X"]) + np.sum(gY * base["Y"] * d["Y"])
+           + float(gz[0]) * z0 * dz)
+
+    def loss_at(h):
+        mp = {k: base[k] * (1 + h * d[k]) for k in base}
+        t = O.run_maps_f64(po, go, steps, mp["P"], mp["X"], mp["Y"], z0 * (1 + h * dz))
+        return _loss(t, w)
+
+    fd = (loss_at(H_REL) - loss_at(-H_REL)) / (2 * H_REL)
+    assert abs(fd) > 0
+    assert abs(adj - fd) <= TOL * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"
+    return adj, fd
+
+
+@pytest.mark.parametrize("parts", ["P", "X", "Y", "Z", "PXYZ"])
+def test_vowel_tube_map_gradients(parts, cuda_ok):
+    L, A = S.vowel_tube(3)
+    _check(dict(cross_sectional_shape=2, mu3d=0.025), L, A, steps=700, every=128, parts=parts)
+
+
+def test_dirichlet_eigen_gradients(cuda_ok):
+    L, A = S.vowel_tube(6)
+    _check(dict(cross_sectional_shape=2, mouth_radiation_cond=1, engine=V.ENGINE_EIGEN, mu3d=0.025), L, A,
+           steps=600, every=100, parts="PXYZ", seed=1)
+
+
+def test_checkpoint_interval_does_not_change_gradients(cuda_ok):
+    L, A = S.vowel_tube(4)
+    pv, gv = V.params(cross_sectional_shape=2), V.Geometry(L, A)
+    outs = []
+    for every in (600, 97, 1):
+        b = V.Batch([pv], [gv])
+        tr = b.forward_ckpt(600, every)[0]
+        grads, gz = b.adjoint(tr[None])
+        gP, gX, gY = grads[0]
+        outs.append((gP, gX, gY, gz))
+    for o in outs[1:]:
+        for a, ref in zip(o, outs[0]):
+            assert np.array_equal(a, ref)
+
+
+def test_two_mass_source_adjoint_unsupported(cuda_ok):
+    L, A = S.vowel_tube(1)
+    b = V.Batch([V.params(cross_sectional_shape=2, source_type=V.SRC_TMM)], [V.Geometry(L, A)])
+    with pytest.raises(V.VsError) as e:
+        b.forward_ckpt(50, 10)
+    assert e.value.status == 7

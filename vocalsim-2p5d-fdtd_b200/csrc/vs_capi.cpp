@@ -81,6 +81,17 @@ struct vs_batch {
     int device = 0;
     bool wall = false;                     // some tube has the coupled wall oscillator
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
+    // adjoint: checkpoints of the last checkpointed forward, history, adjoint planes
+    int64_t ck_steps = 0;                  // steps of the checkpointed forward (0 = none)
+    int ck_every = 0;
+    int ck_count = 0;
+    char* ckpt = nullptr;                  // [ck_count][sum of state_bytes]
+    size_t ckpt_stride = 0;
+    char* adj_mem = nullptr;               // history + lambda + mu + gradient planes
+    AdjTube* d_adj = nullptr;
+    float* d_gtrace = nullptr;
+    Tile* d_hist_tiles = nullptr;
+    int n_hist_tiles = 0;
 
     ~vs_batch() { release(); }
 
@@ -93,6 +104,12 @@ struct vs_batch {
         if (d_tiles) cudaFree(d_tiles);
         if (d_rs) cudaFree(d_rs);
         if (d_trace) cudaFree(d_trace);
+        if (ckpt) cudaFree(ckpt);
+        if (adj_mem) cudaFree(adj_mem);
+        if (d_adj) cudaFree(d_adj);
+        if (d_gtrace) cudaFree(d_gtrace);
+        if (d_hist_tiles) cudaFree(d_hist_tiles);
+        ckpt = nullptr; adj_mem = nullptr; d_adj = nullptr; d_gtrace = nullptr; d_hist_tiles = nullptr;
         if (own_stream && stream) cudaStreamDestroy(stream);
         arena = nullptr; src_arena = nullptr; d_tubes = nullptr; d_tiles = nullptr;
         d_rs = nullptr; d_trace = nullptr; stream = nullptr;
@@ -373,6 +390,215 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     }
 }
 
+// ---- adjoint -------------------------------------------------------------
+
+void check_adjoint_support(const vs_batch* b) {
+    for (const TubeGrid& g : b->grids) {
+        if (g.tmm) throw VsFailure{VS_ERR_UNSUPPORTED, "adjoint of the two-mass source is not implemented"};
+        if (g.wall_ode) throw VsFailure{VS_ERR_UNSUPPORTED, "adjoint of the coupled wall oscillator is not implemented"};
+    }
+}
+
+// Issue `count` step launches from the device step counter (graph chunks of
+// kChunk plus direct launches), RunState already set.
+void issue_steps(vs_batch* b, int64_t count) {
+    int64_t done = 0;
+    if (count >= kChunk) {
+        ensure_graph(b);
+        for (; done + kChunk <= count; done += kChunk) ck(cudaGraphLaunch(b->graph, b->stream), "graph launch");
+    }
+    const int rem = (int)(count - done);
+    for (int i = 0; i < rem; ++i)
+        ck(launch_step(b->shape, b->wall, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch),
+           "step launch");
+    if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
+}
+
+void copy_state(vs_batch* b, int k, bool save) {
+    size_t off = 0;
+    for (size_t i = 0; i < b->grids.size(); ++i) {
+        char* slot = b->ckpt + (size_t)k * b->ckpt_stride + off;
+        ck(cudaMemcpyAsync(save ? slot : b->state_base[i], save ? b->state_base[i] : slot, b->state_bytes[i],
+                           cudaMemcpyDeviceToDevice, b->stream),
+           save ? "save checkpoint" : "restore checkpoint");
+        off += b->state_bytes[i];
+    }
+}
+
+void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces) {
+    check_adjoint_support(b);
+    const int n = (int)b->grids.size();
+    if (b->shape < 0) b->shape = kDefaultShape;
+    build_tiles(b, b->shape);
+    reset_state(b);
+    upload_sources(b, steps);
+    const int64_t need = (int64_t)n * steps;
+    if (need > b->trace_cap) {
+        if (b->d_trace) cudaFree(b->d_trace);
+        b->d_trace = nullptr;
+        ck(cudaMalloc(&b->d_trace, need * sizeof(float)), "cudaMalloc(trace)");
+        b->trace_cap = need;
+    }
+    const int count = (int)((steps + every - 1) / every);
+    size_t stride = 0;
+    for (size_t bytes : b->state_bytes) stride += bytes;
+    if (b->ckpt) { cudaFree(b->ckpt); b->ckpt = nullptr; }
+    ck(cudaMalloc(&b->ckpt, stride * count), "cudaMalloc(checkpoints)");
+    b->ckpt_stride = stride;
+    RunState rs{};
+    rs.trace = b->d_trace;
+    rs.trace_stride = steps;
+    ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
+    for (int k = 0; k < count; ++k) {
+        copy_state(b, k, true);
+        issue_steps(b, std::min<int64_t>(every, steps - (int64_t)k * every));
+    }
+    b->step = steps;
+    b->ck_steps = steps;
+    b->ck_every = every;
+    b->ck_count = count;
+    if (traces)
+        ck(cudaMemcpyAsync(traces, b->d_trace, need * sizeof(float), cudaMemcpyDeviceToHost, b->stream),
+           "copy traces");
+    ck(cudaStreamSynchronize(b->stream), "forward sync");
+}
+
+void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float* gdY, float* gz) {
+    if (b->ck_steps <= 0) throw VsFailure{VS_ERR_INVALID_ARG, "run vs_batch_forward_ckpt before vs_batch_adjoint"};
+    check_adjoint_support(b);
+    const int n = (int)b->grids.size();
+    const int64_t steps = b->ck_steps;
+    const int K = b->ck_every;
+    // device memory: per tube history (K+1 slots x 3 planes), lambda (2 x 3
+    // planes), mu (1 plane), gradients (4 double planes)
+    std::vector<size_t> off(n);
+    size_t total = 0;
+    int max_cells = 0, max_plane = 0;
+    for (int i = 0; i < n; ++i) {
+        const size_t pe = (size_t)b->h_tubes[i].plane;
+        off[i] = total;
+        total += align_up(pe * sizeof(float) * (3 * (size_t)(K + 1) + 6 + 1)) + align_up(pe * sizeof(double) * 4);
+        const TubeGrid& g = b->grids[i];
+        max_cells = std::max(max_cells, (g.H - 2) * (g.W - 2));
+        max_plane = std::max(max_plane, g.H * g.pitch);
+    }
+    if (b->adj_mem) { cudaFree(b->adj_mem); b->adj_mem = nullptr; }
+    ck(cudaMalloc(&b->adj_mem, total), "cudaMalloc(adjoint)");
+    ck(cudaMemsetAsync(b->adj_mem, 0, total, b->stream), "zero adjoint");
+    std::vector<AdjTube> adj(n);
+    if (b->d_gtrace) { cudaFree(b->d_gtrace); b->d_gtrace = nullptr; }
+    ck(cudaMalloc(&b->d_gtrace, (size_t)n * steps * sizeof(float)), "cudaMalloc(trace gradient)");
+    ck(cudaMemcpyAsync(b->d_gtrace, gtrace, (size_t)n * steps * sizeof(float), cudaMemcpyHostToDevice, b->stream),
+       "upload trace gradient");
+    for (int i = 0; i < n; ++i) {
+        const size_t pe = (size_t)b->h_tubes[i].plane;
+        float* base = reinterpret_cast<float*>(b->adj_mem + off[i]);
+        b->h_tubes[i].hist = base;
+        float* lam = base + 3 * (size_t)(K + 1) * pe;
+        adj[i].lam[0] = lam;
+        adj[i].lam[1] = lam + 3 * pe;
+        adj[i].mu = lam + 6 * pe;
+        double* g = reinterpret_cast<double*>(b->adj_mem + off[i] +
+                                              align_up(pe * sizeof(float) * (3 * (size_t)(K + 1) + 6 + 1)));
+        adj[i].gP = g;
+        adj[i].gX = g + pe;
+        adj[i].gY = g + 2 * pe;
+        adj[i].gZ = g + 3 * pe;
+        adj[i].gtrace = b->d_gtrace + (size_t)i * steps;
+    }
+    if (b->d_adj) { cudaFree(b->d_adj); b->d_adj = nullptr; }
+    ck(cudaMalloc(&b->d_adj, n * sizeof(AdjTube)), "cudaMalloc(adjoint descriptors)");
+    ck(cudaMemcpyAsync(b->d_adj, adj.data(), n * sizeof(AdjTube), cudaMemcpyHostToDevice, b->stream),
+       "upload adjoint descriptors");
+    // strip list of the history-capturing step kernel
+    {
+        const int keep_shape = b->tiles_shape;
+        Tile* keep_tiles = b->d_tiles;
+        const int keep_n = b->ntiles;
+        b->d_tiles = nullptr;
+        b->tiles_shape = -1;
+        cudaGraphExec_t keep_graph = b->graph;
+        const int keep_graph_shape = b->graph_shape;
+        b->graph = nullptr;
+        build_tiles(b, history_shape());
+        if (b->d_hist_tiles) cudaFree(b->d_hist_tiles);
+        b->d_hist_tiles = b->d_tiles;
+        b->n_hist_tiles = b->ntiles;
+        b->d_tiles = keep_tiles;
+        b->ntiles = keep_n;
+        b->tiles_shape = keep_shape;
+        b->graph = keep_graph;
+        b->graph_shape = keep_graph_shape;
+    }
+    int q = 0;                    // lambda parity holding the adjoint of the later state
+    for (int k = b->ck_count - 1; k >= 0; --k) {
+        const int64_t start = (int64_t)k * K;
+        const int64_t len = std::min<int64_t>(K, steps - start);
+        copy_state(b, k, false);
+        for (int i = 0; i < n; ++i) b->h_tubes[i].hist_start = start;
+        ck(cudaMemcpyAsync(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice, b->stream),
+           "upload tube descriptors");
+        RunState rs{};
+        rs.step = start;
+        rs.run_start = start;
+        rs.trace = b->d_trace;
+        rs.trace_stride = len;
+        ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
+        ck(launch_history_seed(b->d_tubes, n, max_plane, (int)(start & 1), b->stream), "history seed");
+        for (int64_t j = 0; j < len; ++j)
+            ck(launch_step_history(b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, (int)j, b->stream),
+               "history step");
+        for (int64_t t = start + len - 1; t >= start; --t) {
+            ck(launch_adjoint_step(b->d_tubes, b->d_adj, n, max_cells, t, t - start, q, b->stream), "adjoint step");
+            q ^= 1;
+        }
+        // the host descriptors reach the device again before the next segment's
+        // launches: wait for this segment before rewriting them
+        ck(cudaStreamSynchronize(b->stream), "adjoint segment sync");
+    }
+    // gradients to the caller, frame by frame (unpadded)
+    size_t cell_off = 0;
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
+        const size_t pe = (size_t)b->h_tubes[i].plane;
+        std::vector<double> host(4 * pe);
+        ck(cudaMemcpy(host.data(), adj[i].gP, 4 * pe * sizeof(double), cudaMemcpyDeviceToHost), "read gradients");
+        double z = 0.0;
+        for (int r = 0; r < g.H; ++r)
+            for (int c = 0; c < g.W; ++c) {
+                const size_t src = (size_t)r * g.pitch + c, dst = cell_off + (size_t)r * g.W + c;
+                if (gdP) gdP[dst] = (float)host[src];
+                if (gdX) gdX[dst] = (float)host[pe + src];
+                if (gdY) gdY[dst] = (float)host[2 * pe + src];
+                z += host[3 * pe + src];
+            }
+        if (gz) gz[i] = (float)z;
+        cell_off += (size_t)g.H * g.W;
+    }
+    for (int i = 0; i < n; ++i) b->h_tubes[i].hist = nullptr;
+    ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice), "restore descriptors");
+    b->step = steps;
+}
+
+void set_maps(vs_batch* b, int i, const float* dP, const float* dX, const float* dY, float zinv) {
+    TubeGrid& g = b->grids[i];
+    const size_t n = (size_t)g.H * g.W;
+    if (dP) std::memcpy(g.dP.data(), dP, n * sizeof(float));
+    if (dX) std::memcpy(g.dX.data(), dX, n * sizeof(float));
+    if (dY) std::memcpy(g.dY.data(), dY, n * sizeof(float));
+    for (size_t k = 0; k < n; ++k)
+        if (!(g.dP[k] > 0.0f) || !(g.dX[k] > 0.0f) || !(g.dY[k] > 0.0f) || !std::isfinite(g.dP[k]) ||
+            !std::isfinite(g.dX[k]) || !std::isfinite(g.dY[k]))
+            throw VsFailure{VS_ERR_INVALID_ARG, "depth maps must be finite and > 0"};
+    if (!(zinv >= 0.0f) || !std::isfinite(zinv)) throw VsFailure{VS_ERR_INVALID_ARG, "z_inv must be finite and >= 0"};
+    g.zinv_val = zinv;
+    b->h_tubes[i].zinv = zinv;
+    upload_static(b);
+    ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev), cudaMemcpyHostToDevice),
+       "upload tube descriptors");
+    b->ck_steps = 0;    // checkpoints no longer match the maps
+}
+
 template <class F>
 int guarded(F&& f) {
     try {
@@ -504,6 +730,23 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {
 }
 
 void vs_batch_destroy(vs_batch* b) { delete b; }
+
+int vs_batch_set_maps(vs_batch* b, int32_t tube, const float* depth_p, const float* depth_x, const float* depth_y,
+                      float z_inv) {
+    if (!b || tube < 0 || tube >= (int)b->grids.size()) return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_maps");
+    return guarded([&] { set_maps(b, tube, depth_p, depth_x, depth_y, z_inv); });
+}
+
+int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces) {
+    if (!b || steps < 1 || ckpt_every < 1) return set_error(VS_ERR_INVALID_ARG, "vs_batch_forward_ckpt arguments");
+    return guarded([&] { forward_checkpointed(b, steps, ckpt_every, traces); });
+}
+
+int vs_batch_adjoint(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, float* grad_depth_x,
+                     float* grad_depth_y, float* grad_z_inv) {
+    if (!b || !dL_dtrace) return set_error(VS_ERR_INVALID_ARG, "vs_batch_adjoint arguments");
+    return guarded([&] { run_adjoint(b, dL_dtrace, grad_depth_p, grad_depth_x, grad_depth_y, grad_z_inv); });
+}
 
 int vs_create(const vs_params* p, const vs_geometry* g, vs_solver** out) {
     if (!out || !p) return set_error(VS_ERR_INVALID_ARG, "vs_create arguments");

@@ -43,6 +43,11 @@ struct TubeDev {
     float dir0, dir1, dir2, dir3;
     float sigma[13];
     TmmConsts tmmc;
+    // state history for the adjoint's recomputation (strip kernel with
+    // history capture only): the state after step n goes to slot
+    // n + 1 - hist_start, slot = [P, Vx, Vy] planes, `plane` apart
+    float* hist;
+    int64_t hist_start;
 };
 
 // Mutable run bookkeeping kept in device memory so that CUDA graphs captured
@@ -145,6 +150,32 @@ cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* 
 // max_pitch (0 for strips), and the one-time kernel attribute set-up for it.
 size_t shape_smem_bytes(int shape, int max_pitch);
 cudaError_t prepare_shape(int shape, int max_pitch);
+
+// One step of the strip kernel that also stores the new state into the tube's
+// history (TubeDev::hist); tubes without a wall oscillator only.
+cudaError_t launch_step_history(const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs, int local,
+                                cudaStream_t stream);
+int history_shape();
+
+// Adjoint buffers of one tube (device memory).
+struct AdjTube {
+    float* lam[2];        // [parity]: lambda P, Vx, Vy planes at +0, +plane, +2*plane
+    float* mu;            // adjoint of P' (one plane; ring kept zero)
+    double* gP;           // per-cell gradient accumulators of dP, dX, dY, z_inv
+    double* gX;
+    double* gY;
+    double* gZ;
+    const float* gtrace;  // dL/d trace[step], this tube's row
+};
+
+// Reverse of forward step n for every tube: the adjoint of the state after
+// step n is in lam[par], the adjoint of the state before it goes to
+// lam[par ^ 1]; slot j of TubeDev::hist holds the state before step n.
+cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_cells, int64_t n,
+                                int64_t slot, int par, cudaStream_t stream);
+
+// Copy each tube's state (parity par) into slot 0 of its history.
+cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_cells, int par, cudaStream_t stream);
 
 // Set the text vs_last_error() returns on this host thread.
 void record_error(const char* msg);

@@ -204,7 +204,7 @@ __device__ __forceinline__ VelocityOut velocity_generic(
 //   V_GENERIC  walls, excitation cells, admittance: the full expression
 // Every shortened path drops only operations whose operands are exact 0 / 1
 // (x*1, x+0, x/1), so values equal the full reference expression.
-template <int TR, int MINB, bool WALL>
+template <int TR, int MINB, bool WALL, bool HIST = false>
 __global__ void __launch_bounds__(256, MINB)
 strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
              RunState* __restrict__ rs, int local) {
@@ -352,6 +352,12 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             if (lane_commit) {
                 Vxout[o] = vx;
                 Vyout[o] = vy;
+                if (HIST) {
+                    float* h = T->hist + (n + 1 - T->hist_start) * 3 * pl;
+                    h[o] = pn;
+                    h[pl + o] = vx;
+                    h[2 * pl + o] = vy;
+                }
             }
         }
         // ---- shift the row pipeline
@@ -646,6 +652,16 @@ cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* 
         const int wpb = e.warps;
         fn<<<(ntiles + wpb - 1) / wpb, wpb * 32, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     }
+    return cudaGetLastError();
+}
+
+int history_shape() { return 2; }
+
+cudaError_t launch_step_history(const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs, int local,
+                                cudaStream_t stream) {
+    // shape 2 of the table: 8-row strips, 4 warps per CTA
+    if (ntiles <= 0) return cudaSuccess;
+    strip_kernel<8, 4, false, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     return cudaGetLastError();
 }
 

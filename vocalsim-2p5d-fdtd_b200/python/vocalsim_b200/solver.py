@@ -157,6 +157,35 @@ class Batch:
     def set_tile(self, index: int) -> None:
         check(self.lib, self.lib.vs_batch_set_tile(self.h, index), "vs_batch_set_tile")
 
+    def set_maps(self, tube: int, depth_p=None, depth_x=None, depth_y=None, z_inv: float = 0.0) -> None:
+        """Replace tube `tube`'s depth maps (frame-shaped float32) and z_inv value."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32) for a in (depth_p, depth_x, depth_y)]
+        ptrs = [None if a is None else _fp(a) for a in arrs]
+        check(self.lib, self.lib.vs_batch_set_maps(self.h, tube, *ptrs, float(z_inv)), "vs_batch_set_maps")
+
+    def forward_ckpt(self, steps: int, ckpt_every: int = 512) -> np.ndarray:
+        """Forward from rest keeping checkpoints for adjoint(); returns (n, steps) traces."""
+        tr = np.zeros((self.n, steps), np.float32)
+        check(self.lib, self.lib.vs_batch_forward_ckpt(self.h, steps, ckpt_every, _fp(tr)), "vs_batch_forward_ckpt")
+        self._ck_steps = steps
+        return tr
+
+    def adjoint(self, dL_dtrace: np.ndarray):
+        """Per-cell gradients (list of (dP, dX, dY) frames per tube) and dL/dz_inv per tube."""
+        g = np.ascontiguousarray(dL_dtrace, dtype=np.float32).reshape(self.n, -1)
+        sizes = [d["frame_h"] * d["frame_w"] for d in self.dims]
+        tot = sum(sizes)
+        gp, gx, gy = (np.zeros(tot, np.float32) for _ in range(3))
+        gz = np.zeros(self.n, np.float32)
+        check(self.lib, self.lib.vs_batch_adjoint(self.h, _fp(g), _fp(gp), _fp(gx), _fp(gy), _fp(gz)),
+              "vs_batch_adjoint")
+        out, off = [], 0
+        for d, sz in zip(self.dims, sizes):
+            shp = (d["frame_h"], d["frame_w"])
+            out.append((gp[off:off + sz].reshape(shp), gx[off:off + sz].reshape(shp), gy[off:off + sz].reshape(shp)))
+            off += sz
+        return out, gz
+
     def autotune(self, steps: int):
         best = C.c_int32(-1)
         ms = C.c_float(0)
