@@ -148,6 +148,16 @@ int vs_build_maps(const vs_params* p, const vs_geometry* g, vs_dims* dims,
                   int32_t* cell_type, float* depth_p, float* depth_x,
                   float* depth_y, float* z_inv);
 
+/* Host-only: the tube rasterisation behind the maps, for tube simulations.
+ * upper_wall / lower_wall / column_segment have tube_length_cells entries
+ * (TubeGeometry::upper_wall_pos / lower_wall_pos, TubeGeometry.cu:197-199,
+ * and the segment id the depth kernel uses per column, TubeDepth.cu:417);
+ * major_axis_m / minor_axis_m have n_sections entries (the section widths and
+ * the elliptical minor axes, TubeGeometry.cu:316-364; minor 0 for circles).
+ * Any pointer may be NULL. */
+int vs_tube_layout(const vs_params* p, const vs_geometry* g, vs_dims* dims, int32_t* upper_wall,
+                   int32_t* lower_wall, int32_t* column_segment, float* major_axis_m, float* minor_axis_m);
+
 /* Host-only: the per-step excitation table of GlottalExcitations::
  * setExcitationVelocity (GlottalExcitations.cu:9-52); zeros for the two-mass
  * source, whose velocity is computed on the device each step. */

@@ -1,0 +1,64 @@
+"""Gradients of the transfer-function loss with respect to the 44 section
+widths, 44 section depths and the wall admittance z_inv, through
+SectionDepthModel (torch) -> TubeTrace (forward_ckpt / adjoint on the GPU) ->
+spectral_loss, against central finite differences (h = 1e-4 relative) of the
+FP64 oracle run on the same relaxed maps.  Widths use the continuous
+relaxation of SectionDepthModel (wall rows fixed at the nominal
+rasterisation), so the finite differences are of that same relaxed model."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import vocalsim_b200 as V
+from vocalsim_b200 import synthetic as S
+from vocalsim_b200.autograd import SectionDepthModel, TubeTrace, spectral_loss
+
+pytestmark = pytest.mark.gpu
+
+FS = 44100.0 * 15
+H_REL = 1e-4
+TOL = 1e-3
+
+
+def _setup(steps):
+    L, A = S.vowel_tube(5)
+    kw = dict(cross_sectional_shape=2, mu3d=0.025, num_steps=steps)
+    p, g = V.params(**kw), V.Geometry(L, A)
+    M = SectionDepthModel(p, g)
+    Lt, At = S.vowel_tube(6)
+    target = torch.from_numpy(V.Solver(V.params(**kw), V.Geometry(Lt, At)).run(steps)).double()
+    return kw, L, A, p, g, M, target
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_section_gradients_match_fd(seed, cuda_ok):
+    steps = 2000
+    kw, L, A, p, g, M, target = _setup(steps)
+    z0 = float(M.nominal["dims"]["z_inv_val"])
+    w = M.width0.clone().requires_grad_(True)
+    d = M.depth0.clone().requires_grad_(True)
+    z = torch.tensor([z0], dtype=torch.float64, requires_grad=True)
+    b = V.Batch([p], [g])
+    dp, dx, dy = M.maps(w, d)
+    tr = TubeTrace.apply(b, steps, 256, z, dp, dx, dy)
+    loss = spectral_loss(tr[0], target, FS)
+    loss.backward()
+    assert torch.count_nonzero(w.grad) > 0 and torch.count_nonzero(d.grad) > 0 and z.grad.item() != 0
+
+    rng = np.random.default_rng(seed)
+    dw = torch.from_numpy(rng.uniform(-1, 1, len(w)))
+    dd = torch.from_numpy(rng.uniform(-1, 1, len(d)))
+    dz = float(rng.uniform(-1, 1))
+    adj = float((w.grad * M.width0 * dw).sum() + (d.grad * M.depth0 * dd).sum() + z.grad[0] * z0 * dz)
+
+    po, go = O.params(**kw), O.Geometry(L, A)
+
+    def loss_at(h):
+        with torch.no_grad():
+            mp, mx, my = M.maps(M.width0 * (1 + h * dw), M.depth0 * (1 + h * dd))
+            t = O.run_maps_f64(po, go, steps, mp.numpy(), mx.numpy(), my.numpy(), z0 * (1 + h * dz))
+            return float(spectral_loss(torch.from_numpy(t), target, FS))
+
+    fd = (loss_at(H_REL) - loss_at(-H_REL)) / (2 * H_REL)
+    assert abs(adj - fd) <= TOL * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"

@@ -205,3 +205,20 @@ def test_tiny_tube_one_cell_wide():
     assert e.value.status == 8
     with pytest.raises(RuntimeError, match="status 8"):
         O.maps(O.params(cross_sectional_shape=1, depth_fma=1), O.Geometry(L, A))
+
+
+def test_section_depth_model_reproduces_builder_maps():
+    """The differentiable section model (vocalsim_b200.autograd) at nominal section
+    widths / depths gives the reference maps up to float rounding."""
+    import torch
+    from vocalsim_b200.autograd import SectionDepthModel
+    for seed in (0, 7):
+        L, A = S.vowel_tube(seed)
+        M = SectionDepthModel(V.params(cross_sectional_shape=2), V.Geometry(L, A))
+        dp, dx, dy = M.maps(M.width0.clone(), M.depth0.clone())
+        for t, ref in ((dp, M.nominal["depth_p"]), (dx, M.nominal["depth_x"]), (dy, M.nominal["depth_y"])):
+            assert np.abs(t.numpy() - ref).max() <= 4e-6 * np.abs(ref).max()
+        # widths move depths continuously (relaxed rasterisation)
+        w = M.width0.clone().requires_grad_(True)
+        M.maps(w, M.depth0)[1].sum().backward()
+        assert torch.count_nonzero(w.grad) > 0

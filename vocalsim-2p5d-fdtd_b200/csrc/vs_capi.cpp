@@ -643,6 +643,20 @@ int vs_build_maps(const vs_params* p, const vs_geometry* g, vs_dims* dims, int32
     });
 }
 
+int vs_tube_layout(const vs_params* p, const vs_geometry* g, vs_dims* dims, int32_t* upper_wall,
+                   int32_t* lower_wall, int32_t* column_segment, float* major_axis_m, float* minor_axis_m) {
+    return guarded([&] {
+        TubeGrid t;
+        build_tube(p, g, t, 1);
+        if (dims) *dims = t.dims;
+        if (upper_wall) std::copy(t.upper.begin(), t.upper.end(), upper_wall);
+        if (lower_wall) std::copy(t.lower.begin(), t.lower.end(), lower_wall);
+        if (column_segment) std::copy(t.colseg.begin(), t.colseg.end(), column_segment);
+        if (major_axis_m) std::copy(t.major_m.begin(), t.major_m.end(), major_axis_m);
+        if (minor_axis_m) std::copy(t.minor_m.begin(), t.minor_m.end(), minor_axis_m);
+    });
+}
+
 int vs_source_table(const vs_params* p, int64_t num_steps, float* out) {
     if (!p || !out || num_steps < 0) return set_error(VS_ERR_INVALID_ARG, "vs_source_table arguments");
     return guarded([&] {

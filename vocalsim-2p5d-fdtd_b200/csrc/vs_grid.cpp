@@ -288,6 +288,13 @@ private:
 
         if (p_.fdtd_solver_type == 1) depth(col, minor, sx, my, ex, column_max_seg);
         (void)W;
+        for (int i = 0; i < L; ++i) {
+            T_.upper.push_back(col[i].up);
+            T_.lower.push_back(col[i].down);
+            T_.colseg.push_back(column_max_seg(sx + i) - 1);
+        }
+        T_.major_m = width;
+        T_.minor_m = minor;
     }
 
     static std::vector<float> scale_2d(const std::vector<float>& d) {

@@ -57,6 +57,9 @@ struct TubeGrid {
     std::vector<float> source;        // per-step excitation (empty for the two-mass source)
     TmmConsts tmmc{};
     vs_params src_params{};           // parameters the source table is rebuilt from
+    // tube rasterisation (empty for the open-space domain)
+    std::vector<int32_t> upper, lower, colseg;   // per tube column: wall rows, 0-based segment
+    std::vector<float> major_m, minor_m;         // per section: width used for walls, minor axis
 };
 
 // Fill p with the reference's defaults.

@@ -136,6 +136,7 @@ def load_library(path: os.PathLike | None = None) -> C.CDLL:
         "vs_params_init": (C.c_int, [vp]),
         "vs_build_maps": (C.c_int, [vp, vg, vd, i32p, fp, fp, fp, fp]),
         "vs_source_table": (C.c_int, [vp, C.c_int64, fp]),
+        "vs_tube_layout": (C.c_int, [vp, vg, vd, i32p, i32p, i32p, fp, fp]),
         "vs_create": (C.c_int, [vp, vg, C.POINTER(C.c_void_p)]),
         "vs_get_dims": (C.c_int, [C.c_void_p, vd]),
         "vs_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int]),

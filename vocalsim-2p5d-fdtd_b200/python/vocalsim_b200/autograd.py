@@ -1,0 +1,180 @@
+"""Gradients through the solver.
+
+* SectionDepthModel -- the tube's depth maps as a differentiable (torch,
+  float64) function of per-section parameters: width (major axis, m) and
+  depth (minor axis, m) of the 3:1 elliptical sections.  It follows the
+  reference's elliptical depth kernel, open-space reset, half-cell smoothing
+  and depthP average (TubeDepth.cu:392-490, 642-762) on the nominal tube's
+  rasterisation: wall rows stay where the nominal widths put them
+  (TubeGeometry.cu:433-484 rounds them to whole cells, which has no useful
+  derivative), and a section's width enters continuously through the
+  semi-major axis a = (air cells x ds / 2) x width / nominal width of the
+  depth formula.  At the nominal parameters the maps equal vs_build_maps'
+  up to float rounding.
+* TubeTrace -- torch.autograd.Function over vs_batch_set_maps /
+  vs_batch_forward_ckpt (forward) and vs_batch_adjoint (backward): listener
+  traces as a function of the depth maps and z_inv of each tube.
+* spectral_loss -- L2 between log power spectra over 0..fmax, the transfer
+  function the reference plots (results/plt_transfer_function.py:20-24).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from .abi import SRC_TMM, VsDims, check, load_library
+from .solver import Batch, Geometry, build_maps
+
+OPEN_SPACE_DEPTH = 0.5     # TubeDepth.cu:91
+MIN_DEPTH = 1e-3           # TubeDepth.cu:90
+
+
+def tube_layout(p, g: Geometry) -> dict:
+    """Wall rows, per-column segment ids and section axes (vs_tube_layout)."""
+    lib = load_library()
+    d = VsDims()
+    check(lib, lib.vs_tube_layout(C.byref(p), C.byref(g.struct), C.byref(d), None, None, None, None, None),
+          "vs_tube_layout")
+    L, n = d.tube_length_cells, len(g.length)
+    up, lo, seg = (np.zeros(L, np.int32) for _ in range(3))
+    major, minor = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    i32 = C.POINTER(C.c_int32)
+    f32 = C.POINTER(C.c_float)
+    check(lib, lib.vs_tube_layout(C.byref(p), C.byref(g.struct), C.byref(d), up.ctypes.data_as(i32),
+                                  lo.ctypes.data_as(i32), seg.ctypes.data_as(i32), major.ctypes.data_as(f32),
+                                  minor.ctypes.data_as(f32)), "vs_tube_layout")
+    return dict(dims=d.as_dict(), upper=up, lower=lo, segment=seg, major=major, minor=minor)
+
+
+class SectionDepthModel:
+    """Depth maps of one elliptical-section tube as a function of section widths and depths."""
+
+    def __init__(self, p, g: Geometry):
+        if p.cross_sectional_shape != 2 or p.fdtd_solver_type != 1:
+            raise ValueError("the section model covers 2.5D elliptical sections")
+        lay = tube_layout(p, g)
+        d = lay["dims"]
+        self.H, self.W = d["frame_h"], d["frame_w"]
+        self.ds = float(d["ds"])
+        self.width0 = torch.tensor(lay["major"], dtype=torch.float64)
+        self.depth0 = torch.tensor(lay["minor"], dtype=torch.float64)
+        self.nominal = build_maps(p, g)
+        # the cells the depth kernel writes, in its order (last write wins):
+        # (flat index, segment, nominal semi-major a0, distance in cells or None for a zero)
+        writes_x, writes_y = {}, {}
+        sx = d["tube_start_x"]
+        for i, (u, lo_, s) in enumerate(zip(lay["upper"], lay["lower"], lay["segment"])):
+            x = sx + i
+            air = int(lo_) - int(u) - 1
+            half = math.ceil(air * 0.5) - 1
+            a0 = (air * self.ds) / 2.0
+            for cc in range(half, -1, -1):
+                pu = int(u) + (half - cc) + 1
+                pl = int(lo_) - (half - cc) - 1
+                writes_x[pu * self.W + x] = (int(s), a0, float(cc))
+                writes_x[pl * self.W + x] = (int(s), a0, float(cc))
+                writes_y[pu * self.W + x] = (int(s), a0, float(cc) + 0.5 if cc != half else None)
+                writes_y[pl * self.W + x] = (int(s), a0, float(cc) - 0.5)
+            for r in (int(u), int(lo_)):
+                writes_x[r * self.W + x] = (int(s), a0, None)
+                writes_y[r * self.W + x] = (int(s), a0, None)
+        self.pivot = d["tube_mid_y"] * self.W + d["tube_end_x"]
+        self._x = self._pack(writes_x)
+        self._y = self._pack(writes_y)
+        self.clamp_p = torch.from_numpy(self.nominal["depth_p"] <= MIN_DEPTH)
+        self.clamp_x = torch.from_numpy(self.nominal["depth_x"] <= MIN_DEPTH)
+        self.clamp_y = torch.from_numpy(self.nominal["depth_y"] <= MIN_DEPTH)
+
+    def _pack(self, writes):
+        idx = np.array(list(writes.keys()), np.int64)
+        vals = list(writes.values())
+        seg = np.array([v[0] for v in vals], np.int64)
+        a0 = np.array([v[1] for v in vals], np.float64)
+        dist = np.array([0.0 if v[2] is None else v[2] for v in vals], np.float64)
+        zero = np.array([v[2] is None for v in vals], bool)
+        written = np.zeros(self.H * self.W, bool)
+        written[idx] = True
+        return dict(idx=torch.from_numpy(idx), seg=torch.from_numpy(seg), a0=torch.from_numpy(a0),
+                    dist=torch.from_numpy(dist), zero=torch.from_numpy(zero), unwritten=torch.from_numpy(~written))
+
+    def _raw(self, w, dep, spec):
+        a = spec["a0"] * (w[spec["seg"]] / self.width0[spec["seg"]])
+        b = dep[spec["seg"]] / 2.0
+        y = spec["dist"] * self.ds
+        v = 2.0 * b * torch.sqrt(torch.clamp(1.0 - (y * y) / (a * a), min=0.0))
+        v = torch.where(spec["zero"], torch.zeros_like(v), v)
+        out = torch.full((self.H * self.W,), OPEN_SPACE_DEPTH, dtype=torch.float64)
+        return out.index_put((spec["idx"],), v)
+
+    def maps(self, width: torch.Tensor, depth: torch.Tensor):
+        """(depth_p, depth_x, depth_y) frames (float64) for section widths / depths (m)."""
+        H, W = self.H, self.W
+        x = self._raw(width, depth, self._x)
+        y = self._raw(width, depth, self._y)
+        # open-space cells take the (mid row, tube end) value (resetOpenSpaceDepth)
+        x = torch.where(self._x["unwritten"], x[self.pivot], x).reshape(H, W)
+        y = torch.where(self._y["unwritten"], y[self.pivot], y).reshape(H, W)
+        px, py = x.reshape(-1)[self.pivot], y.reshape(-1)[self.pivot]
+        # half-cell smoothing (smoothDepthX / smoothDepthY)
+        xr = torch.cat([x[:, 1:], px.expand(H, 1)], dim=1)
+        ya = torch.cat([py.expand(1, W), y[:-1, :]], dim=0)
+        xs = 0.5 * (x + xr)
+        ys = 0.5 * (y + ya)
+        # depthP = mean of the four face depths (updateDepthP)
+        pxs, pys = xs.reshape(-1)[self.pivot], ys.reshape(-1)[self.pivot]
+        xl = torch.cat([pxs.expand(H, 1), xs[:, :-1]], dim=1)
+        yb = torch.cat([ys[1:, :], pys.expand(1, W)], dim=0)
+        dp = 0.25 * (xs + ys + xl + yb)
+        lo = torch.tensor(MIN_DEPTH, dtype=torch.float64)
+        dp = torch.where(self.clamp_p, lo, dp)
+        xs = torch.where(self.clamp_x, lo, xs)
+        ys = torch.where(self.clamp_y, lo, ys)
+        return dp, xs, ys
+
+
+class TubeTrace(torch.autograd.Function):
+    """Listener traces (n, steps) of a Batch as a function of each tube's depth
+    maps and z_inv; backward runs the checkpointed adjoint."""
+
+    @staticmethod
+    def forward(ctx, batch: Batch, steps: int, ckpt_every: int, z_inv: torch.Tensor, *maps: torch.Tensor):
+        n = batch.n
+        for i in range(n):
+            dp, dx, dy = (m.detach().to(torch.float32).cpu().numpy() for m in maps[3 * i:3 * i + 3])
+            batch.set_maps(i, dp, dx, dy, float(z_inv[i]))
+        tr = batch.forward_ckpt(steps, ckpt_every)
+        ctx.batch = batch
+        ctx.n = n
+        return torch.from_numpy(tr).to(torch.float64)
+
+    @staticmethod
+    def backward(ctx, grad_trace: torch.Tensor):
+        grads, gz = ctx.batch.adjoint(grad_trace.detach().to(torch.float32).cpu().numpy())
+        out = [None, None, None, torch.from_numpy(gz.astype(np.float64))]
+        for gp, gx, gy in grads:
+            out += [torch.from_numpy(gp.astype(np.float64)), torch.from_numpy(gx.astype(np.float64)),
+                    torch.from_numpy(gy.astype(np.float64))]
+        return tuple(out)
+
+
+def log_power_spectrum(trace: torch.Tensor, fs: float, fmax: float = 5000.0, floor: float = 1e-30) -> torch.Tensor:
+    """log |FFT|^2 of the trace on the bins 0 < f <= fmax."""
+    X = torch.fft.rfft(trace, dim=-1)
+    f = torch.fft.rfftfreq(trace.shape[-1], d=1.0 / fs)
+    sel = (f > 0) & (f <= fmax)
+    p = (X.real ** 2 + X.imag ** 2)[..., sel]
+    return torch.log(p + floor)
+
+
+def spectral_loss(trace: torch.Tensor, target: torch.Tensor, fs: float, fmax: float = 5000.0) -> torch.Tensor:
+    """Mean squared difference of log power spectra over 0..fmax (per tube, summed over tubes)."""
+    d = log_power_spectrum(trace, fs, fmax) - log_power_spectrum(target, fs, fmax)
+    return (d * d).mean(dim=-1).sum()
+
+
+def check_supported(params) -> None:
+    if params.source_type == SRC_TMM:
+        raise NotImplementedError("gradients through the two-mass source are not implemented")
