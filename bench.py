@@ -209,6 +209,53 @@ def run_reference(args, rank):
 
 
 # --------------------------------------------------------------------------- GPU arm
+GRAD_STEPS = 13230                     # 20 ms at 44.1 kHz x 15
+GRAD_CKPT = 512
+
+
+def gradient_cost(V, stream, reps: int = 3) -> dict:
+    """Cost of one gradient against one forward on the same tube: a seeded
+    vowel tube (44 sections, 3:1 elliptical, two-mass source at 800 Pa in
+    double), 20 ms simulated.  forward = the plain graph-replayed run (device trace);
+    gradient = vs_batch_adjoint after vs_batch_forward_ckpt (checkpoints every
+    512 steps, segment recomputation, reverse-time adjoint).  Both include
+    their host synchronisation; medians of `reps` runs after one warm-up."""
+    import torch
+    from vocalsim_b200 import synthetic as S
+
+    L, A = S.vowel_tube(0)
+    p = V.params(cross_sectional_shape=2, source_type=V.SRC_TMM, tmm_ps_pa=800.0, tmm_f64=1, num_steps=GRAD_STEPS)
+    g = V.Geometry(L, A)
+    b = V.Batch([p], [g])
+    b.set_stream(stream.cuda_stream)
+    b.autotune(128)
+    fwd, ck, adj = [], [], []
+    rng = np.random.default_rng(0)
+    gt = rng.standard_normal((1, GRAD_STEPS)).astype(np.float32) * 1e-3
+    for i in range(reps + 1):
+        b.reset()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run_device(GRAD_STEPS)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        b.forward_ckpt(GRAD_STEPS, GRAD_CKPT)
+        t2 = time.perf_counter()
+        b.adjoint(gt)
+        t3 = time.perf_counter()
+        if i:
+            fwd.append((t1 - t0) * 1e3)
+            ck.append((t2 - t1) * 1e3)
+            adj.append((t3 - t2) * 1e3)
+    cells = b.interior_cells
+    b.close()
+    f, c, a = statistics.median(fwd), statistics.median(ck), statistics.median(adj)
+    return {"workload": f"vowel tube (seed 0), two-mass source 800 Pa, {GRAD_STEPS} steps, checkpoints every "
+                        f"{GRAD_CKPT}, {cells} interior cells",
+            "forward_ms": round(f, 2), "forward_ckpt_ms": round(c, 2), "adjoint_ms": round(a, 2),
+            "ratio": round(a / f, 3), "ratio_with_ckpt_forward": round((c + a) / f, 3)}
+
+
 def run_b200(args, rank, world):
     import torch
     import vocalsim_b200 as V
@@ -303,6 +350,10 @@ def run_b200(args, rank, world):
                   "unit": "Gcell-updates/s", "ms": round(sms, 2)}
         s.close()
 
+    grad = None
+    if not args.no_grad:
+        grad = gradient_cost(V, stream)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         procs = host_cores()
@@ -333,7 +384,8 @@ def run_b200(args, rank, world):
         "cpu_baseline": cpu,
         "single_tube": single,
         "batched_vs_single": round(value / world / single["value"], 2) if single else None,
-        "grad_fwd_ratio": None,
+        "grad_fwd_ratio": grad["ratio"] if grad else None,
+        "gradient": grad,
     }
     return line
 
@@ -351,6 +403,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-single", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -100,7 +100,15 @@ typedef struct vs_params {
     /* listener */
     int32_t listener_mode;         /* VS_LISTENER_*                                      */
     int32_t listener_x, listener_y;/* used when listener_mode == VS_LISTENER_EXPLICIT    */
-    int32_t reserved[8];
+    /* two-mass precision (no counterpart in the reference) */
+    int32_t tmm_f64;               /* 0: the reference's float model (TwoMassModel.h:18-
+                                      60 members), bit-exact with it; 1: the same
+                                      equations in double, fields stay FP32.  The float
+                                      model's displacement update loses digits at
+                                      fs = 661.5 kHz and drifts from its double
+                                      restatement (0.2% rel-L2 of the flow by 2000
+                                      steps); the double model tracks it to ~1e-8.    */
+    int32_t reserved[7];
 } vs_params;
 
 /* Area function: n sections of (length cm, area cm^2), the pairs the reference
@@ -233,8 +241,9 @@ void vs_batch_destroy(vs_batch* b);
 
 /* ---- gradients: checkpointed forward + reverse-time discrete adjoint -----
  * No counterpart in the reference (it has no differentiation).  The adjoint
- * covers table sources (Gaussian, sine) without wall coupling; the two-mass
- * source and the coupled wall return VS_ERR_UNSUPPORTED. */
+ * covers table sources (Gaussian, sine) and the two-mass source (whose flow
+ * depends on the pressure at the excitation point) without wall coupling;
+ * the coupled wall oscillator returns VS_ERR_UNSUPPORTED. */
 
 /* Replace tube i's depth maps (frameH*frameW each, NULL keeps one) and its
  * z_inv value; cell types stay.  Invalidates stored checkpoints. */

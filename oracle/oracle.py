@@ -57,6 +57,7 @@ def lib() -> C.CDLL:
         L.orc_run_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, fp]
         L.orc_run_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, dp]
         L.orc_run_maps_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, C.c_double, dp]
+        L.orc_run_maps_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, C.c_float, fp]
         _orc = L
     return _orc
 
@@ -176,6 +177,15 @@ def run_maps_f64(p: VsParams, g: Geometry | None, steps: int, depth_p, depth_x, 
     tr = np.zeros(steps, np.float64)
     _check(lib().orc_run_maps_f64(C.byref(p), g.ref() if g is not None else None, steps, _dp(mp), _dp(mx), _dp(my),
                                   float(z_inv), _dp(tr)), "run_maps_f64")
+    return tr
+
+
+def run_maps_f32(p: VsParams, g: Geometry | None, steps: int, depth_p, depth_x, depth_y, z_inv: float) -> np.ndarray:
+    """FP32 trace of the engine on the given depth maps (rounded to float) and z_inv value."""
+    mp, mx, my = (np.ascontiguousarray(a, np.float32).reshape(-1) for a in (depth_p, depth_x, depth_y))
+    tr = np.zeros(steps, np.float32)
+    _check(lib().orc_run_maps_f32(C.byref(p), g.ref() if g is not None else None, steps, _fp(mp), _fp(mx), _fp(my),
+                                  float(z_inv), _fp(tr)), "run_maps_f32")
     return tr
 
 

@@ -786,6 +786,8 @@ int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long ste
     source_table<T>(p, steps, (double)G.k.dt, src);
     TwoMass<T> tmm;
     tmm.init(p->tmm_ps_pa);
+    TwoMass<double> tmm64;                /* tmm_f64: the model in double, fields in T */
+    tmm64.init(p->tmm_ps_pa);
     T K1, K2;
     if (sizeof(T) == 4) { K1 = (T)G.K1; K2 = (T)G.K2; }
     else {
@@ -801,7 +803,11 @@ int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long ste
 
     for (long long ts = 0; ts < steps; ts++) {
         T exeV;
-        if (p->source_type == VS_SRC_TMM) {
+        if (p->source_type == VS_SRC_TMM && p->tmm_f64) {
+            tmm64.p1 = (double)PN[exc].Pr;
+            tmm64.step(p->srate_mul);
+            exeV = (T)tmm64.ug_next;
+        } else if (p->source_type == VS_SRC_TMM) {
             tmm.p1 = PN[exc].Pr;
             tmm.step(p->srate_mul);
             exeV = tmm.ug_next;
@@ -1053,6 +1059,22 @@ int orc_run_maps_f64(const vs_params* p, const vs_geometry* g, long long steps, 
         std::vector<double> mP(dP, dP + N), mX(dX, dX + N), mY(dY, dY + N), zin(N, 0.0);
         for (size_t i = 0; i < N; i++) if (G.bst[i] != 0) zin[i] = zinv_val;
         return run_engine_maps(p, G, C, steps, mP, mX, mY, zin, trace);
+    } catch (const OracleError& e) { return fail(e); }
+}
+
+/* The FP32 engine on caller-supplied depth maps and z_inv value, as
+ * orc_run_maps_f64 (the maps are rounded to float as the device copy is). */
+int orc_run_maps_f32(const vs_params* p, const vs_geometry* g, long long steps, const float* dP,
+                     const float* dX, const float* dY, float zinv_val, float* trace) {
+    try {
+        Grid G;
+        build_grid(p, g, G);
+        Coeffs C;
+        build_coeffs(G, C);
+        const size_t N = (size_t)G.H * G.W;
+        std::vector<double> mP(dP, dP + N), mX(dX, dX + N), mY(dY, dY + N), zin(N, 0.0);
+        for (size_t i = 0; i < N; i++) if (G.bst[i] != 0) zin[i] = zinv_val;
+        return run_engine<float>(p, G, C, steps, trace, nullptr, nullptr, nullptr, &mP, &mX, &mY, &zin);
     } catch (const OracleError& e) { return fail(e); }
 }
 

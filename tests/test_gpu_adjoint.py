@@ -83,9 +83,32 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_ok):
             assert np.array_equal(a, ref)
 
 
-def test_two_mass_source_adjoint_unsupported(cuda_ok):
+@pytest.mark.parametrize("parts,tmm_f64", [("P", 0), ("PXYZ", 0), ("PXYZ", 1)])
+def test_two_mass_source_gradients(parts, tmm_f64, cuda_ok):
+    # the glottal flow depends on the pressure at the excitation point, so the
+    # reverse step runs the two-mass model's Jacobian transpose each step
     L, A = S.vowel_tube(1)
-    b = V.Batch([V.params(cross_sectional_shape=2, source_type=V.SRC_TMM)], [V.Geometry(L, A)])
+    _check(dict(cross_sectional_shape=2, source_type=V.SRC_TMM, tmm_ps_pa=800.0, mu3d=0.025, tmm_f64=tmm_f64),
+           L, A, steps=1500, every=256, parts=parts, seed=2)
+
+
+@pytest.mark.parametrize("tmm_f64", [0, 1])
+def test_two_mass_checkpoint_interval_does_not_change_gradients(tmm_f64, cuda_ok):
+    L, A = S.vowel_tube(2)
+    pv, gv = V.params(cross_sectional_shape=2, source_type=V.SRC_TMM, tmm_f64=tmm_f64), V.Geometry(L, A)
+    outs = []
+    for every in (500, 33):
+        b = V.Batch([pv], [gv])
+        tr = b.forward_ckpt(500, every)[0]
+        grads, gz = b.adjoint(tr[None])
+        outs.append((*grads[0], gz))
+    for a, ref in zip(outs[1], outs[0]):
+        assert np.array_equal(a, ref)
+
+
+def test_coupled_wall_adjoint_unsupported(cuda_ok):
+    L, A = S.vowel_tube(1)
+    b = V.Batch([V.params(cross_sectional_shape=2, wall_coupling=0.5)], [V.Geometry(L, A)])
     with pytest.raises(V.VsError) as e:
         b.forward_ckpt(50, 10)
     assert e.value.status == 7

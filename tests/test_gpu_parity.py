@@ -38,6 +38,8 @@ CASES = {
         dict(mu3d=0.005, uniform_depth_m=0.02, source_type=3, gauss_peak_s=5e-4, gauss_width_s=1e-4,
              listener_mode=1, listener_x=244, listener_y=28), S.uniform_tube()),
     "vowel_ellipse_tmm": (dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0), S.vowel_tube(3)),
+    "vowel_ellipse_tmm_f64": (dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0, tmm_f64=1),
+                              S.vowel_tube(3)),
     "vowel_circle_dirichlet": (dict(mouth_radiation_cond=1), S.vowel_tube(5)),
     "vowel_eigen": (dict(cross_sectional_shape=2, engine=2), S.vowel_tube(7)),
     "vowel_2d_sine": (dict(fdtd_solver_type=0, source_type=0), S.vowel_tube(9)),
@@ -115,3 +117,24 @@ def test_config1_full_length_rel_l2_vs_double(cuda_ok):
     tr = V.Solver(pv, gv).run(33075)
     ref64 = O.run(po, go, 33075, "f64")
     assert rel_l2(tr, ref64) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("tmm_f64,bound", [(1, REL_L2_TOL), (0, None)])
+def test_two_mass_vowel_rel_l2_vs_double(tmm_f64, bound, cuda_ok):
+    """A vowel tube with the two-mass source (800 Pa), 5000 steps, against the
+    FP64 restatement.  With the double two-mass model (tmm_f64 = 1) the FP32
+    field trace stays within the bound; the reference's float model drifts
+    from its own double restatement by several per cent over the same span
+    (its displacement update loses digits at fs = 661.5 kHz), which the
+    oracle reproduces bit for bit -- recorded here, not bounded."""
+    kw = dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0, tmm_f64=tmm_f64)
+    L, A = S.vowel_tube(0)
+    po, go, pv, gv = both(kw, L, A)
+    tr = V.Solver(pv, gv).run(5000)
+    ref64 = O.run(po, go, 5000, "f64")
+    assert np.array_equal(tr, O.run(po, go, 5000, "f32"))
+    err = rel_l2(tr, ref64)
+    if bound is not None:
+        assert err <= bound, err
+    else:
+        assert err > 10 * REL_L2_TOL, err

@@ -21,9 +21,9 @@ H_REL = 1e-4
 TOL = 1e-3
 
 
-def _setup(steps):
+def _setup(steps, **extra):
     L, A = S.vowel_tube(5)
-    kw = dict(cross_sectional_shape=2, mu3d=0.025, num_steps=steps)
+    kw = dict(cross_sectional_shape=2, mu3d=0.025, num_steps=steps, **extra)
     p, g = V.params(**kw), V.Geometry(L, A)
     M = SectionDepthModel(p, g)
     Lt, At = S.vowel_tube(6)
@@ -31,17 +31,44 @@ def _setup(steps):
     return kw, L, A, p, g, M, target
 
 
-@pytest.mark.parametrize("seed", [0, 1])
-def test_section_gradients_match_fd(seed, cuda_ok):
-    steps = 2000
-    kw, L, A, p, g, M, target = _setup(steps)
+TWO_MASS = dict(source_type=V.SRC_TMM, tmm_ps_pa=800.0, tmm_f64=1)
+
+
+# The two-mass cases use the double two-mass model: the reference's float
+# model drifts from its FP64 restatement by 0.2% of the trace within 2000
+# steps, more than the 1e-3 gradient tolerance, so central differences of
+# the FP64 oracle only check gradients of a forward that tracks it.
+@pytest.mark.parametrize("seed,source", [(0, "gauss"), (1, "gauss"), (2, "two_mass")])
+def test_section_gradients_match_fd(seed, source, cuda_ok):
+    adj, fd = _directional(seed, 2000, TWO_MASS if source == "two_mass" else {})
+    assert abs(adj - fd) <= TOL * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"
+
+
+# The 20 ms gradient workload (13230 steps, checkpoints every 512).  Over this
+# horizon the FP32 fields' rounding, fed back through the self-oscillating
+# two-mass source, moves the gradient of the FP32 system itself: central
+# differences of the FP32 oracle with h = 1e-2 .. 3e-4 scatter by about 2%
+# around the FP64 value.  The adjoint is checked against the FP64 central
+# difference with that bound.
+TOL_20MS = 2e-2
+
+
+def test_section_gradients_20ms_two_mass(cuda_ok):
+    adj, fd = _directional(3, 13230, TWO_MASS, every=512)
+    assert abs(adj - fd) <= TOL_20MS * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"
+
+
+def _directional(seed, steps, extra, every=256):
+    """(adjoint, FP64 central difference) of the spectral loss along a random
+    relative direction of the 44 widths, 44 depths and z_inv."""
+    kw, L, A, p, g, M, target = _setup(steps, **extra)
     z0 = float(M.nominal["dims"]["z_inv_val"])
     w = M.width0.clone().requires_grad_(True)
     d = M.depth0.clone().requires_grad_(True)
     z = torch.tensor([z0], dtype=torch.float64, requires_grad=True)
     b = V.Batch([p], [g])
     dp, dx, dy = M.maps(w, d)
-    tr = TubeTrace.apply(b, steps, 256, z, dp, dx, dy)
+    tr = TubeTrace.apply(b, steps, every, z, dp, dx, dy)
     loss = spectral_loss(tr[0], target, FS)
     loss.backward()
     assert torch.count_nonzero(w.grad) > 0 and torch.count_nonzero(d.grad) > 0 and z.grad.item() != 0
@@ -61,4 +88,4 @@ def test_section_gradients_match_fd(seed, cuda_ok):
             return float(spectral_loss(torch.from_numpy(t), target, FS))
 
     fd = (loss_at(H_REL) - loss_at(-H_REL)) / (2 * H_REL)
-    assert abs(adj - fd) <= TOL * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"
+    return adj, fd

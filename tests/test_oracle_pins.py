@@ -59,6 +59,21 @@ def test_two_mass_model_free_oscillation(mul):
     assert ug.max() > 1e-4          # the folds oscillate and let air through
 
 
+def test_double_two_mass_model_tracks_the_fp64_restatement():
+    """FP32 fields with the two-mass model in double (tmm_f64) stay within
+    1e-4 relative L2 of the all-double run; the reference's float model
+    drifts from it by more than 1e-3 over the same 3000 steps."""
+    from vocalsim_b200 import synthetic as S
+    L, A = S.vowel_tube(0)
+    g = O.Geometry(L, A)
+    err = {}
+    for f64 in (0, 1):
+        p = O.params(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0, tmm_f64=f64)
+        a, b = O.run(p, g, 3000), O.run(p, g, 3000, precision="f64")
+        err[f64] = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert err[1] <= 1e-4 and err[0] > 1e-3, err
+
+
 def test_survey_known_answers():
     """Constants derived while surveying the reference (float probes of its expressions)."""
     k15, k30 = O.consts(15), O.consts(30)

@@ -154,6 +154,167 @@ __global__ void adjoint_lambda_kernel(const TubeDev* __restrict__ tubes, const A
     }
 }
 
+// ---- two-mass source ------------------------------------------------------
+// With the two-mass source, exeV_n = ug_n = TMM(state_n, p1 = P_n[exc]) feeds
+// the velocity of the excitation cells.  Its reverse step needs the Jacobian
+// of one model step (TwoMassModel.cpp:90-232) with respect to the six state
+// values and p1; it is evaluated by forward-mode dual numbers over the same
+// expressions in double (branches on the primal values).
+constexpr int kTmmIn = 7;
+
+struct Dual {
+    double v;
+    double d[kTmmIn];
+};
+
+__device__ inline Dual dconst(double v) {
+    Dual r;
+    r.v = v;
+    for (int i = 0; i < kTmmIn; ++i) r.d[i] = 0.0;
+    return r;
+}
+__device__ inline Dual operator+(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v + b.v;
+    for (int i = 0; i < kTmmIn; ++i) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+__device__ inline Dual operator-(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v - b.v;
+    for (int i = 0; i < kTmmIn; ++i) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+__device__ inline Dual operator*(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v * b.v;
+    for (int i = 0; i < kTmmIn; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+__device__ inline Dual operator/(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v / b.v;
+    for (int i = 0; i < kTmmIn; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
+    return r;
+}
+__device__ inline Dual operator*(double a, const Dual& b) { return dconst(a) * b; }
+__device__ inline Dual operator+(double a, const Dual& b) { return dconst(a) + b; }
+__device__ inline Dual operator-(double a, const Dual& b) { return dconst(a) - b; }
+__device__ inline Dual operator/(double a, const Dual& b) { return dconst(a) / b; }
+__device__ inline Dual operator/(const Dual& a, double b) { return a / dconst(b); }
+__device__ inline Dual dabs(const Dual& a) { return a.v < 0.0 ? dconst(0.0) - a : a; }
+
+// One model step on st = {x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr}.
+__device__ void tmm_math(const TmmConsts64& k, Dual st[6], const Dual& p1) {
+    const double srate = k.srate, s2 = srate * srate;
+    const double lg = k.lg, two_lg = 2.0 * lg, rho = k.rho, ps = k.ps;
+    const Dual x1o = st[0], x1 = st[1], x2o = st[2], x2 = st[3], ugo = st[4], ug = st[5];
+    const Dual Ag1 = k.Ag01 + two_lg * x1, Ag2 = k.Ag02 + two_lg * x2;
+    const double c12 = 12.0 * k.mu * lg * lg;
+    const Dual Rv1 = (c12 * k.d1) / (Ag1 * Ag1 * Ag1), Lg1 = (rho * k.d1) / Ag1;
+    const Dual Rv2 = (c12 * k.d2) / (Ag2 * Ag2 * Ag2), Lg2 = (rho * k.d2) / Ag2;
+    const double thr1 = -k.Ag01 / two_lg, thr2 = -k.Ag02 / two_lg;
+    Dual pm1 = dconst(ps), pm2;
+    if (x1.v > thr1 && x2.v > thr2) {
+        const Dual q = ug / Ag1;
+        pm1 = ps - 1.37 * (rho / 2.0) * q * q - 0.5 * (Rv1 * ug + srate * (Lg1 * (ug - ugo)));
+    }
+    const Dual fm1 = (k.d1 * lg) * pm1;
+    if (x1.v > thr1) {
+        if (x2.v > thr2)
+            pm2 = pm1 - (0.5 * (Rv1 + Rv2) * ug + srate * ((Lg1 + Lg2) * (ug - ugo))) -
+                  (rho / 2.0) * ug * ug * (1.0 / (Ag2 * Ag2) - 1.0 / (Ag1 * Ag1));
+        else
+            pm2 = dconst(ps);
+    } else {
+        pm2 = dconst(0.0);
+    }
+    const Dual fm2 = (k.d2 * lg) * pm2;
+    const double g1 = k.Ag01 / two_lg, g2 = k.Ag02 / two_lg;
+    const bool c1 = x1.v + g1 < 0.0, c2 = x2.v + g2 < 0.0;
+    const double h1u = c1 ? k.h1 : 0.0, r1u = c1 ? k.r1c : k.r1o;
+    const double h2u = c2 ? k.h2 : 0.0, r2u = c2 ? k.r2c : k.r2o;
+    const double a11 = (k.k1 + h1u + k.kc) / s2 + r1u / srate + k.m1;
+    const double a12 = -k.kc / s2;
+    const double a22 = (k.k2 + h2u + k.kc) / s2 + r2u / srate + k.m2;
+    const Dual e1 = g1 + x1, e2 = g2 + x2;
+    const Dual sp1 = (k.k1 * k.etak1) * x1 * x1 * x1 + h1u * (g1 + k.etah1 * e1 * e1 * e1);
+    const Dual sp2 = (k.k2 * k.etak2) * x2 * x2 * x2 + h2u * (g2 + k.etah2 * e2 * e2 * e2);
+    const Dual b1 = (2.0 * k.m1 + r1u / srate) * x1 - k.m1 * x1o - sp1 / s2 + fm1 / s2;
+    const Dual b2 = (2.0 * k.m2 + r2u / srate) * x2 - k.m2 * x2o - sp2 / s2 + fm2 / s2;
+    double det = a11 * a22 - a12 * a12;
+    if (det == 0.0) det = 1.0;
+    const Dual x1n = (a22 * b1 - a12 * b2) / dconst(det);
+    const Dual x2n = (a11 * b2 - a12 * b1) / dconst(det);
+    const Dual A1n = k.Ag01 + two_lg * x1n, A2n = k.Ag02 + two_lg * x2n;
+    Dual ugn = dconst(0.0);
+    if (!(A1n.v < 0.0 || A2n.v < 0.0)) {
+        const Dual r = A2n / dconst(k.A1);
+        const Dual Rtot = (rho / 2.0) * dabs(ug) * (0.37 / (A1n * A1n) + (1.0 - 2.0 * r * (1.0 - r)) / (A2n * A2n)) +
+                          c12 * (k.d1 / (A1n * A1n * A1n) + k.d2 / (A2n * A2n * A2n));
+        const Dual Ltot = rho * (k.d1 / A1n + k.d2 / A2n);
+        ugn = ((ps - p1) / dconst(srate) + Ltot * ug) / (Rtot / dconst(srate) + Ltot);
+    }
+    st[0] = x1; st[1] = x1n; st[2] = x2; st[3] = x2n; st[4] = ug; st[5] = ugn;
+}
+
+// Reverse of the two-mass step n: one thread per tube.  lam[par] holds the
+// adjoint of the state after step n, lam[par ^ 1] the (already computed)
+// adjoint of the state before it, which receives d/d p1 at the excitation cell.
+__global__ void tmm_adjoint_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj, int ntubes,
+                                   int64_t slot, int par) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntubes) return;
+    const TubeDev& T = tubes[t];
+    const AdjTube& A = adj[t];
+    if (!(T.flags & TUBE_TMM)) return;
+    const int64_t pl = T.plane;
+    const int pitch = T.pitch;
+    const float* __restrict__ lam = A.lam[par];
+    // dL/d exeV: a velocity whose cell (or right / top neighbour) is an
+    // excitation cell carries exeV * ew * mS / (mB + mS); every excitation
+    // cell lies in column exc_x, so columns exc_x - 1 and exc_x cover them
+    const float* sig = T.sigma;
+    double lexe = 0.0;
+    for (int r = 1; r <= T.H - 2; ++r) {
+        for (int c = max(T.exc_x - 1, 1); c <= min(T.exc_x, T.W - 2); ++c) {
+            const int64_t o = (int64_t)r * pitch + c;
+            const int tc = T.code[o] & CODE_TYPE_MASK, tr = T.code[o + 1] & CODE_TYPE_MASK;
+            const int tt = T.code[o - pitch] & CODE_TYPE_MASK;
+            const double ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
+            const double ewx = ec * T.dir2 + er * T.dir0, ewy = ec * T.dir3 + et * T.dir1;
+            if (ewx != 0.0) {
+                const double mb = fmin(a_beta[tc], a_beta[tr]), ms = fmax(sig[tc], sig[tr]);
+                lexe += ewx * ms / (mb + ms) * lam[pl + o];
+            }
+            if (ewy != 0.0) {
+                const double mb = fmin(a_beta[tc], a_beta[tt]), ms = fmax(sig[tc], sig[tt]);
+                lexe += ewy * ms / (mb + ms) * lam[2 * pl + o];
+            }
+        }
+    }
+    const double* sv = T.tmm_hist + 6 * slot;
+    const float p1v = T.hist[slot * 3 * pl + (int64_t)T.exc_y * pitch + T.exc_x];
+    Dual st[6];
+    for (int i = 0; i < 6; ++i) {
+        st[i] = dconst(sv[i]);
+        st[i].d[i] = 1.0;
+    }
+    Dual p1 = dconst(p1v);
+    p1.d[6] = 1.0;
+    tmm_math(T.tmmd, st, p1);
+    double lout[6];
+    for (int i = 0; i < 6; ++i) lout[i] = A.lam_tmm[i];
+    lout[5] += lexe;                       // ug_curr after the step is exeV_n
+    double lin[kTmmIn];
+    for (int j = 0; j < kTmmIn; ++j) {
+        lin[j] = 0.0;
+        for (int i = 0; i < 6; ++i) lin[j] += lout[i] * st[i].d[j];
+    }
+    for (int i = 0; i < 6; ++i) A.lam_tmm[i] = lin[i];
+    A.lam[par ^ 1][(int64_t)T.exc_y * pitch + T.exc_x] += (float)lin[6];
+}
+
 // Slot 0 of every tube's history = the state before the first step of a
 // segment (P, Vx, Vy of parity par).
 __global__ void history_seed_kernel(const TubeDev* __restrict__ tubes, int par) {
@@ -166,6 +327,16 @@ __global__ void history_seed_kernel(const TubeDev* __restrict__ tubes, int par) 
     T.hist[i] = P[i];
     T.hist[pl + i] = P[2 * pl + i];
     T.hist[2 * pl + i] = P[4 * pl + i];
+    if (i == 0 && (T.flags & TUBE_TMM)) {
+        double* h = T.tmm_hist;
+        if (T.flags & TUBE_TMM64) {
+            const TmmState64 s = T.tmm64[par];
+            h[0] = s.x1_old; h[1] = s.x1_curr; h[2] = s.x2_old; h[3] = s.x2_curr; h[4] = s.ug_old; h[5] = s.ug_curr;
+        } else {
+            const TmmState s = T.tmm[par];
+            h[0] = s.x1_old; h[1] = s.x1_curr; h[2] = s.x2_old; h[3] = s.x2_curr; h[4] = s.ug_old; h[5] = s.ug_curr;
+        }
+    }
 }
 
 }  // namespace
@@ -177,10 +348,11 @@ cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_
 }
 
 cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_cells, int64_t n,
-                                int64_t slot, int par, cudaStream_t stream) {
+                                int64_t slot, int par, bool tmm, cudaStream_t stream) {
     const dim3 grid((max_cells + 255) / 256, ntubes);
     adjoint_mu_kernel<<<grid, 256, 0, stream>>>(tubes, adj, n, par);
     adjoint_lambda_kernel<<<grid, 256, 0, stream>>>(tubes, adj, slot, par);
+    if (tmm) tmm_adjoint_kernel<<<(ntubes + 31) / 32, 32, 0, stream>>>(tubes, adj, ntubes, slot, par);
     return cudaGetLastError();
 }
 

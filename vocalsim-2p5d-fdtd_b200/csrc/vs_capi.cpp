@@ -285,7 +285,8 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         const TubeGrid& g = b->grids[i];
         base[i] = total;
         const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
-        total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState));
+        total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState)) +
+                 align_up(2 * sizeof(TmmState64));
     }
     total += kGuard;
     b->arena_bytes = total;
@@ -315,6 +316,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
             for (int k = 0; k < 2; ++k) t.z[k] = (float*)next(pl);
         }
         t.tmm = (TmmState*)next(align_up(2 * sizeof(TmmState)));
+        t.tmm64 = (TmmState64*)next(align_up(2 * sizeof(TmmState64)));
         b->state_bytes[i] = (size_t)(p - b->state_base[i]);
         t.dP = (const float*)next(pl);
         t.dX = (const float*)next(pl);
@@ -323,7 +325,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.H = g.H; t.W = g.W; t.pitch = g.pitch;
         t.plane = (int64_t)(pl / sizeof(float));
         t.flags = (g.dirichlet ? TUBE_DIRICHLET : 0) | (g.eigen ? TUBE_EIGEN : 0) |
-                  (g.tmm ? TUBE_TMM : 0) | (g.wall_ode ? TUBE_WALL_ODE : 0);
+                  (g.tmm ? TUBE_TMM : 0) | (g.wall_ode ? TUBE_WALL_ODE : 0) | (g.tmm64 ? TUBE_TMM64 : 0);
         t.lis_x = g.dims.listener_x; t.lis_y = g.dims.listener_y;
         t.exc_x = g.dims.excitation_x; t.exc_y = g.dims.excitation_y;
         t.K1 = g.K1; t.K2 = g.K2; t.bcoef = g.bcoef; t.zinv = g.zinv_val;
@@ -331,6 +333,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.dir0 = g.dir[0]; t.dir1 = g.dir[1]; t.dir2 = g.dir[2]; t.dir3 = g.dir[3];
         for (int k = 0; k < 13; ++k) t.sigma[k] = g.sigma[k];
         t.tmmc = g.tmmc;
+        t.tmmd = g.tmmd;
     }
     ck(cudaMalloc(&b->d_tubes, n * sizeof(TubeDev)), "cudaMalloc(tubes)");
     ck(cudaMalloc(&b->d_rs, sizeof(RunState)), "cudaMalloc(run state)");
@@ -394,7 +397,6 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
 
 void check_adjoint_support(const vs_batch* b) {
     for (const TubeGrid& g : b->grids) {
-        if (g.tmm) throw VsFailure{VS_ERR_UNSUPPORTED, "adjoint of the two-mass source is not implemented"};
         if (g.wall_ode) throw VsFailure{VS_ERR_UNSUPPORTED, "adjoint of the coupled wall oscillator is not implemented"};
     }
 }
@@ -470,15 +472,20 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     const int64_t steps = b->ck_steps;
     const int K = b->ck_every;
     // device memory: per tube history (K+1 slots x 3 planes), lambda (2 x 3
-    // planes), mu (1 plane), gradients (4 double planes)
+    // planes), mu (1 plane), gradients (4 double planes); with the two-mass
+    // source also its state history (K+1) and adjoint (6 doubles)
     std::vector<size_t> off(n);
     size_t total = 0;
     int max_cells = 0, max_plane = 0;
+    bool any_tmm = false;
+    auto float_bytes = [&](size_t pe) { return align_up(pe * sizeof(float) * (3 * (size_t)(K + 1) + 6 + 1)); };
     for (int i = 0; i < n; ++i) {
         const size_t pe = (size_t)b->h_tubes[i].plane;
-        off[i] = total;
-        total += align_up(pe * sizeof(float) * (3 * (size_t)(K + 1) + 6 + 1)) + align_up(pe * sizeof(double) * 4);
         const TubeGrid& g = b->grids[i];
+        off[i] = total;
+        total += float_bytes(pe) + align_up(pe * sizeof(double) * 4);
+        if (g.tmm) total += align_up((size_t)(K + 1) * 6 * sizeof(double)) + align_up(6 * sizeof(double));
+        any_tmm = any_tmm || g.tmm;
         max_cells = std::max(max_cells, (g.H - 2) * (g.W - 2));
         max_plane = std::max(max_plane, g.H * g.pitch);
     }
@@ -498,13 +505,20 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         adj[i].lam[0] = lam;
         adj[i].lam[1] = lam + 3 * pe;
         adj[i].mu = lam + 6 * pe;
-        double* g = reinterpret_cast<double*>(b->adj_mem + off[i] +
-                                              align_up(pe * sizeof(float) * (3 * (size_t)(K + 1) + 6 + 1)));
+        char* gbase = b->adj_mem + off[i] + float_bytes(pe);
+        double* g = reinterpret_cast<double*>(gbase);
         adj[i].gP = g;
         adj[i].gX = g + pe;
         adj[i].gY = g + 2 * pe;
         adj[i].gZ = g + 3 * pe;
         adj[i].gtrace = b->d_gtrace + (size_t)i * steps;
+        adj[i].lam_tmm = nullptr;
+        b->h_tubes[i].tmm_hist = nullptr;
+        if (b->grids[i].tmm) {
+            char* tbase = gbase + align_up(pe * sizeof(double) * 4);
+            b->h_tubes[i].tmm_hist = reinterpret_cast<double*>(tbase);
+            adj[i].lam_tmm = reinterpret_cast<double*>(tbase + align_up((size_t)(K + 1) * 6 * sizeof(double)));
+        }
     }
     if (b->d_adj) { cudaFree(b->d_adj); b->d_adj = nullptr; }
     ck(cudaMalloc(&b->d_adj, n * sizeof(AdjTube)), "cudaMalloc(adjoint descriptors)");
@@ -549,7 +563,7 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
             ck(launch_step_history(b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, (int)j, b->stream),
                "history step");
         for (int64_t t = start + len - 1; t >= start; --t) {
-            ck(launch_adjoint_step(b->d_tubes, b->d_adj, n, max_cells, t, t - start, q, b->stream), "adjoint step");
+            ck(launch_adjoint_step(b->d_tubes, b->d_adj, n, max_cells, t, t - start, q, any_tmm, b->stream), "adjoint step");
             q ^= 1;
         }
         // the host descriptors reach the device again before the next segment's
@@ -575,7 +589,10 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         if (gz) gz[i] = (float)z;
         cell_off += (size_t)g.H * g.W;
     }
-    for (int i = 0; i < n; ++i) b->h_tubes[i].hist = nullptr;
+    for (int i = 0; i < n; ++i) {
+        b->h_tubes[i].hist = nullptr;
+        b->h_tubes[i].tmm_hist = nullptr;
+    }
     ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice), "restore descriptors");
     b->step = steps;
 }

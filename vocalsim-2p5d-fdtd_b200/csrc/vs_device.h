@@ -16,6 +16,7 @@ enum : int32_t {
     TUBE_EIGEN = 2,       // FDTDEngineEigen pressure denominator sigma*dP + dP
     TUBE_TMM = 4,         // two-mass source computed on the device each step
     TUBE_WALL_ODE = 8,    // 2.5D wall oscillator with nonzero pressure coupling
+    TUBE_TMM64 = 16,      // with TUBE_TMM: the two-mass model in double
 };
 
 // One tube as the step kernel sees it.  All planes share `pitch` and live in
@@ -32,6 +33,7 @@ struct TubeDev {
     const uint8_t* code;  // type | zinv bit
     const float* src;     // per-step excitation table (nullptr for the two-mass source)
     TmmState* tmm;        // [2], ping-ponged by step parity
+    TmmState64* tmm64;    // [2], the double model's state (TUBE_TMM64)
     int64_t src_len;
     int64_t plane;        // elements between consecutive planes: P[k] = P[0] + k*plane,
                           // Vx[k] = P[0] + (2+k)*plane, Vy[k] = P[0] + (4+k)*plane,
@@ -43,11 +45,14 @@ struct TubeDev {
     float dir0, dir1, dir2, dir3;
     float sigma[13];
     TmmConsts tmmc;
+    TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
     // state history for the adjoint's recomputation (strip kernel with
     // history capture only): the state after step n goes to slot
     // n + 1 - hist_start, slot = [P, Vx, Vy] planes, `plane` apart
     float* hist;
     int64_t hist_start;
+    double* tmm_hist;     // two-mass state before each step of the segment: 6 values
+                          // per slot (x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr)
 };
 
 // Mutable run bookkeeping kept in device memory so that CUDA graphs captured
@@ -166,15 +171,19 @@ struct AdjTube {
     double* gY;
     double* gZ;
     const float* gtrace;  // dL/d trace[step], this tube's row
+    double* lam_tmm;      // adjoint of the two-mass state (6 values)
 };
 
 // Reverse of forward step n for every tube: the adjoint of the state after
 // step n is in lam[par], the adjoint of the state before it goes to
-// lam[par ^ 1]; slot j of TubeDev::hist holds the state before step n.
+// lam[par ^ 1]; slot j of TubeDev::hist holds the state before step n.  With
+// `tmm`, tubes with the two-mass source also run its reverse step (after the
+// cell update, adding the pressure term at the excitation point).
 cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_cells, int64_t n,
-                                int64_t slot, int par, cudaStream_t stream);
+                                int64_t slot, int par, bool tmm, cudaStream_t stream);
 
-// Copy each tube's state (parity par) into slot 0 of its history.
+// Copy each tube's state (parity par) into slot 0 of its history (and the
+// two-mass state into slot 0 of tmm_hist).
 cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_cells, int par, cudaStream_t stream);
 
 // Set the text vs_last_error() returns on this host thread.

@@ -107,6 +107,7 @@ private:
         if (p_.simulation_type != 0 && p_.simulation_type != 1) raise(VS_ERR_INVALID_ARG, "simulation_type must be 0 or 1");
         if (p_.engine != VS_ENGINE_CPU && p_.engine != VS_ENGINE_EIGEN) raise(VS_ERR_INVALID_ARG, "engine must be VS_ENGINE_CPU or VS_ENGINE_EIGEN");
         if (p_.source_type < 0 || p_.source_type > 3) raise(VS_ERR_INVALID_ARG, "source_type must be 0..3");
+        if (p_.tmm_f64 != 0 && p_.tmm_f64 != 1) raise(VS_ERR_INVALID_ARG, "tmm_f64 must be 0 or 1");
         if (p_.num_steps <= 0 && !(p_.audio_dur > 0.0f)) raise(VS_ERR_INVALID_ARG, "need num_steps > 0 or audio_dur > 0");
         if ((p_.source_type == VS_SRC_GAUSS || p_.source_type == VS_SRC_GAUSS_STD) && !(p_.gauss_width_s > 0.0f))
             raise(VS_ERR_INVALID_ARG, "gauss_width_s must be > 0");
@@ -493,36 +494,49 @@ void build_source(const vs_params* p, float dt, int64_t n, std::vector<float>& o
     }
 }
 
-TmmConsts tmm_consts(float ps, int srate_mul) {
-    // TwoMassModel::setTwoMassModelParams (TwoMassModel.cpp:4-87), q = gs = 1
-    TmmConsts t;
-    t.mu = (float)(1.86e-4 * (double)(kDyn * kSecond / (kCm * kCm)));
-    t.rho = (float)(1.14 * (double)(kKg / (kMeter * kMeter * kMeter)));
-    const float q = 1.0f, gs = 1.0f;
-    t.m1 = (0.125f * kGram) / q;
-    t.m2 = (0.025f * kGram) / q;
-    t.d1 = (0.25f * kCm) / q;
-    t.d2 = (0.05f * kCm) / q;
-    t.k1 = 80000.0f * (kDyn / kCm) * q;
-    t.k2 = 8000.0f * (kDyn / kCm) * q;
-    t.kc = 25000.0f * (kDyn / kCm) * (q * q);
-    t.etak1 = 100 / (kCm * kCm);
-    t.etak2 = 100 / (kCm * kCm);
+template <class F>
+TmmConstsT<F> tmm_consts(float ps, int srate_mul) {
+    // TwoMassModel::setTwoMassModelParams (TwoMassModel.cpp:4-87), q = gs = 1.
+    // The unit constants and literals are floats; for F = double they are
+    // widened before the products, as a double instantiation of the
+    // reference's expressions would do.
+    TmmConstsT<F> t;
+    const F cm = (F)kCm, gram = (F)kGram, dyn = (F)kDyn;
+    t.mu = (F)(1.86e-4 * (double)(kDyn * kSecond / (kCm * kCm)));
+    t.rho = (F)(1.14 * (double)(kKg / (kMeter * kMeter * kMeter)));
+    const F q = 1.0f, gs = 1.0f;
+    t.m1 = ((F)0.125f * gram) / q;
+    t.m2 = ((F)0.025f * gram) / q;
+    t.d1 = ((F)0.25f * cm) / q;
+    t.d2 = ((F)0.05f * cm) / q;
+    t.k1 = (F)80000.0f * (dyn / cm) * q;
+    t.k2 = (F)8000.0f * (dyn / cm) * q;
+    t.kc = (F)25000.0f * (dyn / cm) * (q * q);
+    t.etak1 = 100 / (cm * cm);
+    t.etak2 = 100 / (cm * cm);
     t.h1 = 3 * t.k1;
     t.h2 = 3 * t.k2;
-    t.etah1 = 500.0f / (kCm * kCm);
-    t.etah2 = 500.0f / (kCm * kCm);
-    t.Ag01 = 0.05f * (kCm * kCm);
+    t.etah1 = (F)500.0f / (cm * cm);
+    t.etah2 = (F)500.0f / (cm * cm);
+    t.Ag01 = (F)0.05f * (cm * cm);
     t.Ag02 = t.Ag01;
-    t.lg = 1.40f * kCm;
-    t.r1o = (2 * 0.2f * sqrtf(t.k1 * t.m1)) / (gs * gs);
-    t.r2o = (2 * 0.6f * sqrtf(t.k2 * t.m2)) / (gs * gs);
-    t.r1c = (2 * 1.1f * sqrtf(t.k1 * t.m1)) / (gs * gs);
-    t.r2c = (2 * 1.9f * sqrtf(t.k2 * t.m2)) / (gs * gs);
-    t.A1 = 3.0f * (kCm * kCm);
-    t.ps = ps;
-    t.srate = 44100 * (float)srate_mul;
+    t.lg = (F)1.40f * cm;
+    t.r1o = (2 * (F)0.2f * std::sqrt(t.k1 * t.m1)) / (gs * gs);
+    t.r2o = (2 * (F)0.6f * std::sqrt(t.k2 * t.m2)) / (gs * gs);
+    t.r1c = (2 * (F)1.1f * std::sqrt(t.k1 * t.m1)) / (gs * gs);
+    t.r2c = (2 * (F)1.9f * std::sqrt(t.k2 * t.m2)) / (gs * gs);
+    t.A1 = (F)3.0f * (cm * cm);
+    t.ps = (F)ps;
+    t.srate = 44100 * (F)srate_mul;
     return t;
+}
+
+template TmmConstsT<float> tmm_consts<float>(float, int);
+template TmmConstsT<double> tmm_consts<double>(float, int);
+
+static TmmConsts64 widen(const TmmConsts& c) {
+    return {c.mu, c.rho, c.m1, c.m2, c.d1, c.d2, c.k1, c.k2, c.kc, c.etak1, c.etak2, c.h1, c.h2, c.etah1,
+            c.etah2, c.Ag01, c.Ag02, c.lg, c.r1o, c.r2o, c.r1c, c.r2c, c.A1, c.ps, c.srate};
 }
 
 void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source) {
@@ -531,7 +545,9 @@ void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t
     const int64_t n = steps_for_source > 0 ? steps_for_source : out.dims.num_steps;
     if (p->source_type == VS_SRC_TMM) out.source.clear();
     else build_source(p, out.dt, n, out.source);
-    out.tmmc = tmm_consts(p->tmm_ps_pa, p->srate_mul);
+    out.tmmc = tmm_consts<float>(p->tmm_ps_pa, p->srate_mul);
+    out.tmm64 = p->source_type == VS_SRC_TMM && p->tmm_f64 != 0;
+    out.tmmd = out.tmm64 ? tmm_consts<double>(p->tmm_ps_pa, p->srate_mul) : widen(out.tmmc);
 }
 
 }  // namespace vsb

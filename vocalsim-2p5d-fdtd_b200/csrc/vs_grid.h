@@ -21,18 +21,25 @@ struct VsFailure {
     std::string what;
 };
 
-// Constants of the two-mass vocal fold model (TwoMassModel.cpp:4-87), as the
-// float values the reference stores in its members.
-struct TmmConsts {
-    float mu, rho, m1, m2, d1, d2, k1, k2, kc, etak1, etak2, h1, h2, etah1, etah2;
-    float Ag01, Ag02, lg, r1o, r2o, r1c, r2c, A1, ps, srate;
+// Constants of the two-mass vocal fold model (TwoMassModel.cpp:4-87): with
+// F = float the values the reference stores in its members, with F = double
+// the same expressions evaluated in double (the double-precision model).
+template <class F>
+struct TmmConstsT {
+    F mu, rho, m1, m2, d1, d2, k1, k2, kc, etak1, etak2, h1, h2, etah1, etah2;
+    F Ag01, Ag02, lg, r1o, r2o, r1c, r2c, A1, ps, srate;
 };
+using TmmConsts = TmmConstsT<float>;
+using TmmConsts64 = TmmConstsT<double>;
 
 // Two-mass model state carried from step to step (the members the reference
 // reads before writing in runTwoMassModel).
-struct TmmState {
-    float x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr;
+template <class F>
+struct TmmStateT {
+    F x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr;
 };
+using TmmState = TmmStateT<float>;
+using TmmState64 = TmmStateT<double>;
 
 // Everything the device needs for one tube, in host memory.
 struct TubeGrid {
@@ -56,6 +63,8 @@ struct TubeGrid {
     std::vector<float> dP, dX, dY;    // H*W
     std::vector<float> source;        // per-step excitation (empty for the two-mass source)
     TmmConsts tmmc{};
+    bool tmm64 = false;               // two-mass model in double (vs_params::tmm_f64)
+    TmmConsts64 tmmd{};               // double constants: the double model's, else tmmc widened
     vs_params src_params{};           // parameters the source table is rebuilt from
     // tube rasterisation (empty for the open-space domain)
     std::vector<int32_t> upper, lower, colseg;   // per tube column: wall rows, 0-based segment
@@ -72,7 +81,9 @@ void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t
 // The per-step excitation table (GlottalExcitations::setExcitationVelocity).
 void build_source(const vs_params* p, float dt, int64_t n, std::vector<float>& out);
 
-// Two-mass model constants (setTwoMassModelParams) for a given subglottal pressure.
-TmmConsts tmm_consts(float ps, int srate_mul);
+// Two-mass model constants (setTwoMassModelParams) for a given subglottal
+// pressure, in float (the reference's) or double.
+template <class F>
+TmmConstsT<F> tmm_consts(float ps, int srate_mul);
 
 }  // namespace vsb

@@ -137,7 +137,7 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     const size_t off_state = off;             off += plane_bytes * nstate;
     const size_t off_depth = off;             off += plane_bytes * 3;
     const size_t off_code = off;              off += up256((size_t)H * pitch);
-    const size_t off_tmm = off;               off += up256(2 * sizeof(TmmState));
+    const size_t off_tmm = off;               off += up256(2 * sizeof(TmmState)) + up256(2 * sizeof(TmmState64));
     const size_t off_tube = off;              off += up256(sizeof(TubeDev));
     const size_t off_rs = off;                off += up256(sizeof(RunState));
     const size_t off_tiles = off;             off += up256((size_t)nitems * sizeof(Tile));
@@ -173,10 +173,12 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     t.src = p->source_type == VS_SRC_TMM ? nullptr : source;
     t.src_len = p->source_type == VS_SRC_TMM ? 0 : steps;
     t.tmm = reinterpret_cast<TmmState*>(base + off_tmm);
+    t.tmm64 = reinterpret_cast<TmmState64*>(base + off_tmm + up256(2 * sizeof(TmmState)));
     t.plane = (int64_t)pe;
     t.H = H; t.W = W; t.pitch = pitch;
     t.flags = (p->mouth_radiation_cond ? TUBE_DIRICHLET : 0) | (p->engine == VS_ENGINE_EIGEN ? TUBE_EIGEN : 0) |
-              (p->source_type == VS_SRC_TMM ? TUBE_TMM : 0) | (wall ? TUBE_WALL_ODE : 0);
+              (p->source_type == VS_SRC_TMM ? TUBE_TMM : 0) | (wall ? TUBE_WALL_ODE : 0) |
+              (p->source_type == VS_SRC_TMM && p->tmm_f64 ? TUBE_TMM64 : 0);
     t.lis_x = dims->listener_x; t.lis_y = dims->listener_y;
     t.exc_x = dims->excitation_x; t.exc_y = dims->excitation_y;
     t.K1 = (kappa * dt) / ds;
@@ -190,7 +192,8 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     const float sig[13] = {dt, 0, dt, 0, 0, 0, 0, 0, 0, 0, 1000000.0f, 0, dt};
     for (int k = 0; k < 13; ++k) t.sigma[k] = sig[k];
     for (int l = 0; l < 6; ++l) t.sigma[VS_CELL_PML0 + l] = ((float)l / (float)5) * 0.5f;
-    t.tmmc = tmm_consts(p->tmm_ps_pa, p->srate_mul);
+    t.tmmc = tmm_consts<float>(p->tmm_ps_pa, p->srate_mul);
+    t.tmmd = tmm_consts<double>(p->tmm_ps_pa, p->srate_mul);
 
     RunState rs;
     std::memset(&rs, 0, sizeof(rs));
@@ -202,7 +205,8 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     Tile* d_tiles = reinterpret_cast<Tile*>(base + off_tiles);
     // fields, wall state and the two-mass state restart at zero on every call
     e = cudaMemsetAsync(base + off_state, 0, plane_bytes * nstate, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(base + off_tmm, 0, up256(2 * sizeof(TmmState)), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(base + off_tmm, 0, up256(2 * sizeof(TmmState)) + up256(2 * sizeof(TmmState64)), st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_tube, &t, sizeof(t), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));

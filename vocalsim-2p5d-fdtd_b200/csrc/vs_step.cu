@@ -142,6 +142,98 @@ __device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1
     return ugn;
 }
 
+// The same model step with every quantity in double (tmm_f64), following
+// TwoMassModel.cpp:90-232 operation by operation; the caller's pressure is
+// widened and the flow rounded to float for the field update.
+__device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, float p1f) {
+    const double srate = k.srate, ss = srate * srate;
+    const double p1 = (double)p1f;
+    const double x1c = s.x1_curr, x2c = s.x2_curr, ug = s.ug_curr, ugo = s.ug_old;
+    double Ag1 = k.Ag01 + 2 * k.lg * x1c;
+    double Ag2 = k.Ag02 + 2 * k.lg * x2c;
+    const double Rv1 = (12 * k.mu * k.lg * k.lg * k.d1) / (Ag1 * Ag1 * Ag1);
+    const double Lg1 = (k.rho * k.d1) / Ag1;
+    const double Rv2 = (12 * k.mu * k.lg * k.lg * k.d2) / (Ag2 * Ag2 * Ag2);
+    const double Lg2 = (k.rho * k.d2) / Ag2;
+    double pm1, pm2;
+    if (x1c > -k.Ag01 / (2 * k.lg) && x2c > -k.Ag02 / (2 * k.lg))
+        pm1 = k.ps - 1.37 * (k.rho / 2) * (ug / Ag1) * (ug / Ag1) - 0.5 * (Rv1 * ug + Lg1 * srate * (ug - ugo));
+    else
+        pm1 = k.ps;
+    const double fm1 = pm1 * k.d1 * k.lg;
+    if (x1c > -k.Ag01 / (2 * k.lg)) {
+        if (x2c > -k.Ag02 / (2 * k.lg))
+            pm2 = pm1 - (0.5 * (Rv1 + Rv2) * ug + (Lg1 + Lg2) * (ug - ugo) * srate) -
+                  (k.rho / 2 * ug * ug) * (1 / (Ag2 * Ag2) - 1 / (Ag1 * Ag1));
+        else
+            pm2 = k.ps;
+    } else {
+        pm2 = 0;
+    }
+    const double fm2 = pm2 * k.d2 * k.lg;
+    double h1u, r1u, h2u, r2u;
+    if (x1c + k.Ag01 / (2 * k.lg) < 0) { h1u = k.h1; r1u = k.r1c; } else { h1u = 0; r1u = k.r1o; }
+    if (x2c + k.Ag02 / (2 * k.lg) < 0) { h2u = k.h2; r2u = k.r2c; } else { h2u = 0; r2u = k.r2o; }
+    const double a11 = (k.k1 + h1u + k.kc) / ss + r1u / srate + k.m1;
+    const double a12 = -k.kc / ss;
+    const double a21 = a12;
+    const double a22 = (k.k2 + h2u + k.kc) / ss + r2u / srate + k.m2;
+    const double g1 = k.Ag01 / (2 * k.lg), g2 = k.Ag02 / (2 * k.lg);
+    const double s1 = k.k1 * k.etak1 * x1c * x1c * x1c + h1u * (g1 + k.etah1 * (g1 + x1c) * (g1 + x1c) * (g1 + x1c));
+    const double s2 = k.k2 * k.etak2 * x2c * x2c * x2c + h2u * (g2 + k.etah2 * (g2 + x2c) * (g2 + x2c) * (g2 + x2c));
+    const double b1 = (2 * k.m1 + r1u / srate) * x1c - k.m1 * s.x1_old - s1 / ss + fm1 / ss;
+    const double b2 = (2 * k.m2 + r2u / srate) * x2c - k.m2 * s.x2_old - s2 / ss + fm2 / ss;
+    double det = a11 * a22 - a21 * a12;
+    if (det == 0) det = 1;
+    const double x1n = (a22 * b1 - a12 * b2) / det;
+    const double x2n = (a11 * b2 - a21 * b1) / det;
+    s.x1_old = x1c; s.x1_curr = x1n;
+    s.x2_old = x2c; s.x2_curr = x2n;
+    Ag1 = k.Ag01 + 2 * k.lg * x1n;
+    Ag2 = k.Ag02 + 2 * k.lg * x2n;
+    double ugn;
+    if (Ag1 < 0 || Ag2 < 0) {
+        ugn = 0;
+    } else {
+        const double Rtot = (k.rho / 2) * fabs(ug) *
+                                ((0.37 / (Ag1 * Ag1)) + (1 - 2 * (Ag2 / k.A1) * (1 - Ag2 / k.A1)) / (Ag2 * Ag2)) +
+                            (12 * k.mu * k.lg * k.lg * (k.d1 / (Ag1 * Ag1 * Ag1) + k.d2 / (Ag2 * Ag2 * Ag2)));
+        const double Ltot = k.rho * (k.d1 / Ag1 + k.d2 / Ag2);
+        ugn = ((k.ps - p1) / srate + Ltot * ug) / (Rtot / srate + Ltot);
+    }
+    s.ug_old = ug;
+    s.ug_curr = ugn;
+    return (float)ugn;
+}
+
+// One two-mass step of tube T from the state of parity par and the pressure
+// p1 at the excitation point; with `store` the new state is written to parity
+// par ^ 1 (and, when hist is given, as 6 doubles to hist).
+__device__ __noinline__ float glottal_step(const TubeDev* T, int par, float p1, bool store, double* hist) {
+    if (T->flags & TUBE_TMM64) {
+        TmmState64 s = T->tmm64[par];
+        const float e = tmm_step64(T->tmmd, s, p1);
+        if (store) {
+            T->tmm64[par ^ 1] = s;
+            if (hist) {
+                hist[0] = s.x1_old; hist[1] = s.x1_curr; hist[2] = s.x2_old;
+                hist[3] = s.x2_curr; hist[4] = s.ug_old; hist[5] = s.ug_curr;
+            }
+        }
+        return e;
+    }
+    TmmState s = T->tmm[par];
+    const float e = tmm_step(T->tmmc, s, p1);
+    if (store) {
+        T->tmm[par ^ 1] = s;
+        if (hist) {
+            hist[0] = s.x1_old; hist[1] = s.x1_curr; hist[2] = s.x2_old;
+            hist[3] = s.x2_curr; hist[4] = s.ug_old; hist[5] = s.ug_curr;
+        }
+    }
+    return e;
+}
+
 // a / b for b > 0 with the signed zero returned directly when a is zero:
 // the same value as the division, without sending the zero fields of a cold
 // start through the slow path of the IEEE divide.
@@ -248,11 +340,11 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             if (lane == 0) {
                 // every strip holding excitation cells advances the same state from
                 // the same input; the strip that commits the excitation cell stores it
-                TmmState s = T->tmm[par];
-                exeV = tmm_step(T->tmmc, s, Pin[(size_t)T->exc_y * pitch + T->exc_x]);
                 const int ex = T->exc_x - it.c0;
-                if (T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= kStripLead && ex < kStripLead + kStripCommit)
-                    T->tmm[par ^ 1] = s;
+                const bool owner =
+                    T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= kStripLead && ex < kStripLead + kStripCommit;
+                exeV = glottal_step(T, par, Pin[(size_t)T->exc_y * pitch + T->exc_x], owner,
+                                    HIST ? T->tmm_hist + 6 * (n + 1 - T->hist_start) : nullptr);
             }
             exeV = __shfl_sync(kFull, exeV, 0);
         } else {
@@ -490,9 +582,8 @@ band_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ bands, i
         float e = 0.0f;
         if (bd.has_exc) {
             if (flags & TUBE_TMM) {
-                TmmState s = T->tmm[par];
-                e = tmm_step(T->tmmc, s, Pin[(size_t)T->exc_y * pitch + T->exc_x]);
-                if (T->exc_y >= r0 && T->exc_y <= rcommit) T->tmm[par ^ 1] = s;
+                e = glottal_step(T, par, Pin[(size_t)T->exc_y * pitch + T->exc_x],
+                                 T->exc_y >= r0 && T->exc_y <= rcommit, nullptr);
             } else {
                 e = n < T->src_len ? T->src[n] : 0.0f;
             }

@@ -68,7 +68,8 @@ class VsParams(C.Structure):
         ("listener_mode", C.c_int32),
         ("listener_x", C.c_int32),
         ("listener_y", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("tmm_f64", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
     def copy(self) -> "VsParams":

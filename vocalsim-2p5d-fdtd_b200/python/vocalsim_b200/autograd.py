@@ -25,7 +25,7 @@ import math
 import numpy as np
 import torch
 
-from .abi import SRC_TMM, VsDims, check, load_library
+from .abi import VsDims, check, load_library
 from .solver import Batch, Geometry, build_maps
 
 OPEN_SPACE_DEPTH = 0.5     # TubeDepth.cu:91
@@ -174,7 +174,3 @@ def spectral_loss(trace: torch.Tensor, target: torch.Tensor, fs: float, fmax: fl
     d = log_power_spectrum(trace, fs, fmax) - log_power_spectrum(target, fs, fmax)
     return (d * d).mean(dim=-1).sum()
 
-
-def check_supported(params) -> None:
-    if params.source_type == SRC_TMM:
-        raise NotImplementedError("gradients through the two-mass source are not implemented")
