@@ -61,7 +61,7 @@ __device__ inline VCoef vcoef(bool dirx, int kc, int kr, int kt, float zval, flo
     const float nn = (float)((1 - ec) * (1 - en));
     const float xout = bc * (1.0f - bn), xin = bn * (1.0f - bc);
     const float z = (kc & CODE_ZINV_BIT) ? zval : 0.0f;
-    const float g = 1.0f / (mB + mS);
+    const float g = __frcp_rn(mB + mS);
     VCoef v;
     v.al = mB * g;
     v.a = g * (bxy + mS * z * nn * xout * Nout);
@@ -72,24 +72,16 @@ __device__ inline VCoef vcoef(bool dirx, int kc, int kr, int kt, float zval, flo
     return v;
 }
 
-__global__ void adjoint_mu_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj, int64_t n,
-                                  int par) {
-    const TubeDev& T = tubes[blockIdx.y];
-    const AdjTube& A = adj[blockIdx.y];
-    const int W = T.W, H = T.H, pitch = T.pitch;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (H - 2) * (W - 2)) return;
-    const int r = 1 + i / (W - 2), c = 1 + i % (W - 2);
+// mu of interior cell (r, c): the adjoint of P' (see the file comment).
+__device__ float mu_at(const TubeDev& T, const AdjTube& A, int par, int r, int c, int64_t n) {
+    const float* __restrict__ lam = A.lam[par];
+    const int pitch = T.pitch;
     const int64_t pl = T.plane;
     const int64_t o = (int64_t)r * pitch + c;
     const uint8_t* __restrict__ code = T.code;
-    const float* __restrict__ lam = A.lam[par];
     const float* __restrict__ sig = T.sigma;
     const int kc = code[o];
-    if ((T.flags & TUBE_DIRICHLET) && (kc & CODE_TYPE_MASK) == VS_CELL_NOPRESSURE) {
-        A.mu[o] = 0.0f;
-        return;
-    }
+    if ((T.flags & TUBE_DIRICHLET) && (kc & CODE_TYPE_MASK) == VS_CELL_NOPRESSURE) return 0.0f;
     const int kr = code[o + 1], kt = code[o - pitch];
     const VCoef cx = vcoef(true, kc, kr, kt, T.zinv, T.bcoef, sig);
     const VCoef cy = vcoef(false, kc, kr, kt, T.zinv, T.bcoef, sig);
@@ -98,221 +90,213 @@ __global__ void adjoint_mu_kernel(const TubeDev* __restrict__ tubes, const AdjTu
         const VCoef cl = vcoef(true, code[o - 1], kc, code[o - 1 - pitch], T.zinv, T.bcoef, sig);
         mu -= cl.b * lam[pl + o - 1];
     }
-    if (r + 1 <= H - 2) {   // the cell below's Vy' depends on this P' as its top neighbour
+    if (r + 1 <= T.H - 2) {   // the cell below's Vy' depends on this P' as its top neighbour
         const VCoef cd = vcoef(false, code[o + pitch], code[o + pitch + 1], kc, T.zinv, T.bcoef, sig);
         mu -= cd.b * lam[2 * pl + o + pitch];
     }
     if (r == T.lis_y && c == T.lis_x) mu += A.gtrace[n];
-    A.mu[o] = mu;
-}
-
-__global__ void adjoint_lambda_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
-                                      int64_t slot, int par) {
-    const TubeDev& T = tubes[blockIdx.y];
-    const AdjTube& A = adj[blockIdx.y];
-    const int W = T.W, H = T.H, pitch = T.pitch;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (H - 2) * (W - 2)) return;
-    const int r = 1 + i / (W - 2), c = 1 + i % (W - 2);
-    const int64_t pl = T.plane;
-    const int64_t o = (int64_t)r * pitch + c;
-    const uint8_t* __restrict__ code = T.code;
-    const float* __restrict__ sig = T.sigma;
-    const float* __restrict__ lam = A.lam[par];
-    float* __restrict__ lout = A.lam[par ^ 1];
-    const float* __restrict__ mu = A.mu;
-    const float* __restrict__ dP = T.dP;
-    const float* __restrict__ dX = T.dP + pl;
-    const float* __restrict__ dY = T.dP + 2 * pl;
-    const float K1 = T.K1;
-    auto D = [&](int64_t q) { return (1.0f + sig[code[q] & CODE_TYPE_MASK]) * dP[q]; };
-    const int kc = code[o], kr = code[o + 1], kt = code[o - pitch];
-    const float muc = mu[o], Dc = D(o);
-    // ring cells keep mu = 0, so the neighbours' terms vanish there
-    const float lamU = K1 * (mu[o + 1] / D(o + 1) - muc / Dc);
-    const float lamW = K1 * (mu[o - pitch] / D(o - pitch) - muc / Dc);
-    const VCoef cx = vcoef(true, kc, kr, kt, T.zinv, T.bcoef, sig);
-    const VCoef cy = vcoef(false, kc, kr, kt, T.zinv, T.bcoef, sig);
-    const float lvx1 = lam[pl + o], lvy1 = lam[2 * pl + o];
-    lout[o] = muc * dP[o] / Dc;
-    lout[pl + o] = cx.al * lvx1 + dX[o] * lamU;
-    lout[2 * pl + o] = cy.al * lvy1 + dY[o] * lamW;
-    // state before the step (slot) and P' after it (slot + 1)
-    const float* __restrict__ s0 = T.hist + slot * 3 * pl;
-    const float* __restrict__ s1 = s0 + 3 * pl;
-    const float vx = s0[pl + o], vy = s0[2 * pl + o];
-    const float S = (vx * dX[o] - s0[pl + o - 1] * dX[o - 1]) + (vy * dY[o] - s0[2 * pl + o + pitch] * dY[o + pitch]);
-    const float sc = sig[kc & CODE_TYPE_MASK];
-    if (!((T.flags & TUBE_DIRICHLET) && (kc & CODE_TYPE_MASK) == VS_CELL_NOPRESSURE))
-        A.gP[o] += (double)muc * (double)K1 * (double)S / ((1.0 + (double)sc) * (double)dP[o] * (double)dP[o]);
-    A.gX[o] += (double)vx * (double)lamU;
-    A.gY[o] += (double)vy * (double)lamW;
-    if (kc & CODE_ZINV_BIT) {
-        const float pc = s1[o], pr = s1[o + 1], pt = s1[o - pitch];
-        A.gZ[o] += (double)(cx.zc_out * pc - cx.zc_in * pr) * (double)lvx1 +
-                   (double)(cy.zc_out * pc - cy.zc_in * pt) * (double)lvy1;
-    }
+    // the two-mass flow of the step after this one read P' here
+    if ((T.flags & TUBE_TMM) && r == T.exc_y && c == T.exc_x) mu += (float)A.lam_tmm[6 + par];
+    return mu;
 }
 
 // ---- two-mass source ------------------------------------------------------
 // With the two-mass source, exeV_n = ug_n = TMM(state_n, p1 = P_n[exc]) feeds
 // the velocity of the excitation cells.  Its reverse step needs the Jacobian
 // of one model step (TwoMassModel.cpp:90-232) with respect to the six state
-// values and p1; it is evaluated by forward-mode dual numbers over the same
-// expressions in double (branches on the primal values).
-constexpr int kTmmIn = 7;
-
+// values and p1.  Lane j of a warp evaluates the step's expressions in
+// double on a dual number carrying the derivative along input j (forward
+// mode; branches follow the primal values), so lanes 0..6 hold the seven
+// columns of the Jacobian.
 struct Dual {
-    double v;
-    double d[kTmmIn];
+    double v, d;
 };
 
-__device__ inline Dual dconst(double v) {
-    Dual r;
-    r.v = v;
-    for (int i = 0; i < kTmmIn; ++i) r.d[i] = 0.0;
-    return r;
+__device__ inline Dual dc(double v) { return {v, 0.0}; }
+__device__ inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ inline Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__device__ inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__device__ inline Dual dabs(Dual a) { return a.v < 0.0 ? Dual{-a.v, -a.d} : a; }
+
+__device__ inline Dual dinv(Dual b) {
+    const double r = 1.0 / b.v;
+    return {r, -b.d * r * r};
 }
-__device__ inline Dual operator+(const Dual& a, const Dual& b) {
-    Dual r;
-    r.v = a.v + b.v;
-    for (int i = 0; i < kTmmIn; ++i) r.d[i] = a.d[i] + b.d[i];
-    return r;
-}
-__device__ inline Dual operator-(const Dual& a, const Dual& b) {
-    Dual r;
-    r.v = a.v - b.v;
-    for (int i = 0; i < kTmmIn; ++i) r.d[i] = a.d[i] - b.d[i];
-    return r;
-}
-__device__ inline Dual operator*(const Dual& a, const Dual& b) {
-    Dual r;
-    r.v = a.v * b.v;
-    for (int i = 0; i < kTmmIn; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
-    return r;
-}
-__device__ inline Dual operator/(const Dual& a, const Dual& b) {
-    Dual r;
-    r.v = a.v / b.v;
-    for (int i = 0; i < kTmmIn; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
-    return r;
-}
-__device__ inline Dual operator*(double a, const Dual& b) { return dconst(a) * b; }
-__device__ inline Dual operator+(double a, const Dual& b) { return dconst(a) + b; }
-__device__ inline Dual operator-(double a, const Dual& b) { return dconst(a) - b; }
-__device__ inline Dual operator/(double a, const Dual& b) { return dconst(a) / b; }
-__device__ inline Dual operator/(const Dual& a, double b) { return a / dconst(b); }
-__device__ inline Dual dabs(const Dual& a) { return a.v < 0.0 ? dconst(0.0) - a : a; }
 
 // One model step on st = {x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr}.
-__device__ void tmm_math(const TmmConsts64& k, Dual st[6], const Dual& p1) {
-    const double srate = k.srate, s2 = srate * srate;
+// The divisions by state-dependent quantities go through one reciprocal
+// each (Ag1, Ag2 before and after the update, the flow denominator), so the
+// chain holds three dependent double divisions; the values agree with the
+// forward model to rounding, which is all its derivative needs.
+__device__ void tmm_math(const TmmConsts64& k, Dual st[6], Dual p1) {
+    const double srate = k.srate, isr = 1.0 / srate, is2 = isr * isr;
     const double lg = k.lg, two_lg = 2.0 * lg, rho = k.rho, ps = k.ps;
-    const Dual x1o = st[0], x1 = st[1], x2o = st[2], x2 = st[3], ugo = st[4], ug = st[5];
-    const Dual Ag1 = k.Ag01 + two_lg * x1, Ag2 = k.Ag02 + two_lg * x2;
-    const double c12 = 12.0 * k.mu * lg * lg;
-    const Dual Rv1 = (c12 * k.d1) / (Ag1 * Ag1 * Ag1), Lg1 = (rho * k.d1) / Ag1;
-    const Dual Rv2 = (c12 * k.d2) / (Ag2 * Ag2 * Ag2), Lg2 = (rho * k.d2) / Ag2;
     const double thr1 = -k.Ag01 / two_lg, thr2 = -k.Ag02 / two_lg;
-    Dual pm1 = dconst(ps), pm2;
+    const double g1 = k.Ag01 / two_lg, g2 = k.Ag02 / two_lg;
+    const double iA1 = 1.0 / k.A1;
+    const Dual x1o = st[0], x1 = st[1], x2o = st[2], x2 = st[3], ugo = st[4], ug = st[5];
+    const Dual ia1 = dinv(k.Ag01 + two_lg * x1), ia2 = dinv(k.Ag02 + two_lg * x2);
+    const Dual ia1s = ia1 * ia1, ia2s = ia2 * ia2;
+    const double c12 = 12.0 * k.mu * lg * lg;
+    const Dual Rv1 = (c12 * k.d1) * (ia1s * ia1), Lg1 = (rho * k.d1) * ia1;
+    const Dual Rv2 = (c12 * k.d2) * (ia2s * ia2), Lg2 = (rho * k.d2) * ia2;
+    Dual pm1 = dc(ps), pm2;
     if (x1.v > thr1 && x2.v > thr2) {
-        const Dual q = ug / Ag1;
+        const Dual q = ug * ia1;
         pm1 = ps - 1.37 * (rho / 2.0) * q * q - 0.5 * (Rv1 * ug + srate * (Lg1 * (ug - ugo)));
     }
     const Dual fm1 = (k.d1 * lg) * pm1;
     if (x1.v > thr1) {
         if (x2.v > thr2)
             pm2 = pm1 - (0.5 * (Rv1 + Rv2) * ug + srate * ((Lg1 + Lg2) * (ug - ugo))) -
-                  (rho / 2.0) * ug * ug * (1.0 / (Ag2 * Ag2) - 1.0 / (Ag1 * Ag1));
+                  (rho / 2.0) * ug * ug * (ia2s - ia1s);
         else
-            pm2 = dconst(ps);
+            pm2 = dc(ps);
     } else {
-        pm2 = dconst(0.0);
+        pm2 = dc(0.0);
     }
     const Dual fm2 = (k.d2 * lg) * pm2;
-    const double g1 = k.Ag01 / two_lg, g2 = k.Ag02 / two_lg;
     const bool c1 = x1.v + g1 < 0.0, c2 = x2.v + g2 < 0.0;
     const double h1u = c1 ? k.h1 : 0.0, r1u = c1 ? k.r1c : k.r1o;
     const double h2u = c2 ? k.h2 : 0.0, r2u = c2 ? k.r2c : k.r2o;
-    const double a11 = (k.k1 + h1u + k.kc) / s2 + r1u / srate + k.m1;
-    const double a12 = -k.kc / s2;
-    const double a22 = (k.k2 + h2u + k.kc) / s2 + r2u / srate + k.m2;
+    const double a11 = (k.k1 + h1u + k.kc) * is2 + r1u * isr + k.m1;
+    const double a12 = -k.kc * is2;
+    const double a22 = (k.k2 + h2u + k.kc) * is2 + r2u * isr + k.m2;
     const Dual e1 = g1 + x1, e2 = g2 + x2;
     const Dual sp1 = (k.k1 * k.etak1) * x1 * x1 * x1 + h1u * (g1 + k.etah1 * e1 * e1 * e1);
     const Dual sp2 = (k.k2 * k.etak2) * x2 * x2 * x2 + h2u * (g2 + k.etah2 * e2 * e2 * e2);
-    const Dual b1 = (2.0 * k.m1 + r1u / srate) * x1 - k.m1 * x1o - sp1 / s2 + fm1 / s2;
-    const Dual b2 = (2.0 * k.m2 + r2u / srate) * x2 - k.m2 * x2o - sp2 / s2 + fm2 / s2;
+    const Dual b1 = (2.0 * k.m1 + r1u * isr) * x1 - k.m1 * x1o + is2 * (fm1 - sp1);
+    const Dual b2 = (2.0 * k.m2 + r2u * isr) * x2 - k.m2 * x2o + is2 * (fm2 - sp2);
     double det = a11 * a22 - a12 * a12;
     if (det == 0.0) det = 1.0;
-    const Dual x1n = (a22 * b1 - a12 * b2) / dconst(det);
-    const Dual x2n = (a11 * b2 - a12 * b1) / dconst(det);
+    const double idet = 1.0 / det;
+    const Dual x1n = idet * (a22 * b1 - a12 * b2);
+    const Dual x2n = idet * (a11 * b2 - a12 * b1);
     const Dual A1n = k.Ag01 + two_lg * x1n, A2n = k.Ag02 + two_lg * x2n;
-    Dual ugn = dconst(0.0);
+    Dual ugn = dc(0.0);
     if (!(A1n.v < 0.0 || A2n.v < 0.0)) {
-        const Dual r = A2n / dconst(k.A1);
-        const Dual Rtot = (rho / 2.0) * dabs(ug) * (0.37 / (A1n * A1n) + (1.0 - 2.0 * r * (1.0 - r)) / (A2n * A2n)) +
-                          c12 * (k.d1 / (A1n * A1n * A1n) + k.d2 / (A2n * A2n * A2n));
-        const Dual Ltot = rho * (k.d1 / A1n + k.d2 / A2n);
-        ugn = ((ps - p1) / dconst(srate) + Ltot * ug) / (Rtot / dconst(srate) + Ltot);
+        const Dual ib1 = dinv(A1n), ib2 = dinv(A2n);
+        const Dual ib1s = ib1 * ib1, ib2s = ib2 * ib2;
+        const Dual r = iA1 * A2n;
+        const Dual Rtot = (rho / 2.0) * dabs(ug) * (0.37 * ib1s + (1.0 - 2.0 * r * (1.0 - r)) * ib2s) +
+                          c12 * (k.d1 * (ib1s * ib1) + k.d2 * (ib2s * ib2));
+        const Dual Ltot = rho * (k.d1 * ib1 + k.d2 * ib2);
+        ugn = (isr * (ps - p1) + Ltot * ug) * dinv(isr * Rtot + Ltot);
     }
     st[0] = x1; st[1] = x1n; st[2] = x2; st[3] = x2n; st[4] = ug; st[5] = ugn;
 }
 
-// Reverse of the two-mass step n: one thread per tube.  lam[par] holds the
-// adjoint of the state after step n, lam[par ^ 1] the (already computed)
-// adjoint of the state before it, which receives d/d p1 at the excitation cell.
-__global__ void tmm_adjoint_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj, int ntubes,
-                                   int64_t slot, int par) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntubes) return;
-    const TubeDev& T = tubes[t];
-    const AdjTube& A = adj[t];
-    if (!(T.flags & TUBE_TMM)) return;
-    const int64_t pl = T.plane;
-    const int pitch = T.pitch;
-    const float* __restrict__ lam = A.lam[par];
-    // dL/d exeV: a velocity whose cell (or right / top neighbour) is an
-    // excitation cell carries exeV * ew * mS / (mB + mS); every excitation
-    // cell lies in column exc_x, so columns exc_x - 1 and exc_x cover them
-    const float* sig = T.sigma;
+// Reverse of the two-mass step n, by one warp: lam holds the adjoint of the
+// state after step n.  d/d p1 belongs to the adjoint of the state before the
+// step at the excitation point; it is left in lam_tmm[6 + (par ^ 1)] for the
+// next reverse step's mu there, so this warp runs beside the cell blocks.
+__device__ void tmm_reverse(const TubeDev& T, const AdjTube& A, const float* __restrict__ lam, int par,
+                            int64_t slot) {
+    const int lane = threadIdx.x & 31;
+    // dL/d exeV = sum over the velocities it enters of lambda' * dV'/d exeV
     double lexe = 0.0;
-    for (int r = 1; r <= T.H - 2; ++r) {
-        for (int c = max(T.exc_x - 1, 1); c <= min(T.exc_x, T.W - 2); ++c) {
-            const int64_t o = (int64_t)r * pitch + c;
-            const int tc = T.code[o] & CODE_TYPE_MASK, tr = T.code[o + 1] & CODE_TYPE_MASK;
-            const int tt = T.code[o - pitch] & CODE_TYPE_MASK;
-            const double ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
-            const double ewx = ec * T.dir2 + er * T.dir0, ewy = ec * T.dir3 + et * T.dir1;
-            if (ewx != 0.0) {
-                const double mb = fmin(a_beta[tc], a_beta[tr]), ms = fmax(sig[tc], sig[tr]);
-                lexe += ewx * ms / (mb + ms) * lam[pl + o];
-            }
-            if (ewy != 0.0) {
-                const double mb = fmin(a_beta[tc], a_beta[tt]), ms = fmax(sig[tc], sig[tt]);
-                lexe += ewy * ms / (mb + ms) * lam[2 * pl + o];
-            }
+    for (int i = lane; i < A.n_exc; i += 32) lexe += (double)A.exc_coef[i] * (double)lam[A.exc_off[i]];
+    for (int m = 16; m > 0; m >>= 1) lexe += __shfl_xor_sync(0xffffffffu, lexe, m);
+    const int64_t pl = T.plane;
+    const int64_t oexc = (int64_t)T.exc_y * T.pitch + T.exc_x;
+    const double* sv = T.tmm_hist + 6 * slot;
+    double lo[6];
+    for (int i = 0; i < 6; ++i) lo[i] = A.lam_tmm[i];
+    lo[5] += lexe;                          // ug_curr after the step is exeV_n
+    __syncwarp();
+    if (lane < 7) {
+        Dual st[6];
+        for (int i = 0; i < 6; ++i) st[i] = Dual{sv[i], i == lane ? 1.0 : 0.0};
+        const Dual p1{(double)T.hist[slot * 3 * pl + oexc], lane == 6 ? 1.0 : 0.0};
+        tmm_math(T.tmmd, st, p1);
+        double lin = 0.0;
+        for (int i = 0; i < 6; ++i) lin += lo[i] * st[i].d;
+        if (lane < 6) A.lam_tmm[lane] = lin;
+        else A.lam_tmm[6 + (par ^ 1)] = lin;
+    }
+}
+
+// One reverse step: block (tile, tube) computes mu over its 32 x 8 cells
+// plus the row above and the column to the right into shared memory, then
+// lambda of the state before the step and the gradient terms of its cells;
+// the block holding the excitation point also runs the two-mass reverse step.
+__global__ void __launch_bounds__(kAdjTileW * kAdjTileH)
+adjoint_step_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
+                    const AdjRun* __restrict__ run, int local) {
+    const TubeDev& T = tubes[blockIdx.y];
+    const AdjTube& A = adj[blockIdx.y];
+    const AdjRun ar = *run;
+    const int64_t n = ar.start + ar.len - 1 - local;
+    const int64_t slot = n - ar.start;
+    const int par = ar.q0 ^ (local & 1);
+    if ((int)blockIdx.x >= A.tiles) {
+        // the block after the last tile reverses the two-mass step
+        if ((int)blockIdx.x == A.tiles && (T.flags & TUBE_TMM) && threadIdx.x < 32)
+            tmm_reverse(T, A, A.lam[par], par, slot);
+        return;
+    }
+    const int W = T.W, H = T.H, pitch = T.pitch;
+    const int tiles_x = (W - 2 + kAdjTileW - 1) / kAdjTileW;
+    const int c0 = 1 + (int)(blockIdx.x % tiles_x) * kAdjTileW, r0 = 1 + (int)(blockIdx.x / tiles_x) * kAdjTileH;
+    const int tx = threadIdx.x % kAdjTileW, ty = threadIdx.x / kAdjTileW;
+    const float* __restrict__ lam = A.lam[par];
+    float* __restrict__ lout = A.lam[par ^ 1];
+    __shared__ float smu[kAdjTileH + 1][kAdjTileW + 1];   // row 0: row r0 - 1; column 32: column c0 + 32
+    const int r = r0 + ty, c = c0 + tx;
+    const bool in = r <= H - 2 && c <= W - 2;
+    smu[ty + 1][tx] = in ? mu_at(T, A, par, r, c, n) : 0.0f;
+    if (threadIdx.x < kAdjTileW) {
+        const int rr = r0 - 1, cc = c0 + (int)threadIdx.x;
+        smu[0][threadIdx.x] = (rr >= 1 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n) : 0.0f;
+    } else if (threadIdx.x < kAdjTileW + kAdjTileH) {
+        const int k = threadIdx.x - kAdjTileW, rr = r0 + k, cc = c0 + kAdjTileW;
+        smu[k + 1][kAdjTileW] = (rr <= H - 2 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n) : 0.0f;
+    }
+    __syncthreads();
+    if (in) {
+        const int64_t pl = T.plane;
+        const int64_t o = (int64_t)r * pitch + c;
+        const uint8_t* __restrict__ code = T.code;
+        const float* __restrict__ sig = T.sigma;
+        const float* __restrict__ dP = T.dP;
+        const float* __restrict__ dX = T.dP + pl;
+        const float* __restrict__ dY = T.dP + 2 * pl;
+        const float K1 = T.K1;
+        const int kc = code[o], kr = code[o + 1], kt = code[o - pitch];
+        const float muc = smu[ty + 1][tx], mur = smu[ty + 1][tx + 1], mut = smu[ty][tx];
+        const float Dc = (1.0f + sig[kc & CODE_TYPE_MASK]) * dP[o];
+        const float qc = muc / Dc;
+        // ring cells and no-pressure cells of a Dirichlet mouth have mu = 0
+        const float qr = mur != 0.0f ? mur / ((1.0f + sig[kr & CODE_TYPE_MASK]) * dP[o + 1]) : 0.0f;
+        const float qt = mut != 0.0f ? mut / ((1.0f + sig[kt & CODE_TYPE_MASK]) * dP[o - pitch]) : 0.0f;
+        const float lamU = K1 * (qr - qc);
+        const float lamW = K1 * (qt - qc);
+        const VCoef cx = vcoef(true, kc, kr, kt, T.zinv, T.bcoef, sig);
+        const VCoef cy = vcoef(false, kc, kr, kt, T.zinv, T.bcoef, sig);
+        const float lvx1 = lam[pl + o], lvy1 = lam[2 * pl + o];
+        lout[o] = qc * dP[o];
+        lout[pl + o] = cx.al * lvx1 + dX[o] * lamU;
+        lout[2 * pl + o] = cy.al * lvy1 + dY[o] * lamW;
+        // state before the step (slot) and P' after it (slot + 1)
+        const float* __restrict__ s0 = T.hist + slot * 3 * pl;
+        const float* __restrict__ s1 = s0 + 3 * pl;
+        const float vx = s0[pl + o], vy = s0[2 * pl + o];
+        const float S =
+            (vx * dX[o] - s0[pl + o - 1] * dX[o - 1]) + (vy * dY[o] - s0[2 * pl + o + pitch] * dY[o + pitch]);
+        const float sc = sig[kc & CODE_TYPE_MASK];
+        if (muc != 0.0f)
+            A.gP[o] += (double)muc * (double)K1 * (double)S / ((1.0 + (double)sc) * (double)dP[o] * (double)dP[o]);
+        A.gX[o] += (double)vx * (double)lamU;
+        A.gY[o] += (double)vy * (double)lamW;
+        if (kc & CODE_ZINV_BIT) {
+            const float pc = s1[o], pr = s1[o + 1], pt = s1[o - pitch];
+            A.gZ[o] += (double)(cx.zc_out * pc - cx.zc_in * pr) * (double)lvx1 +
+                       (double)(cy.zc_out * pc - cy.zc_in * pt) * (double)lvy1;
         }
     }
-    const double* sv = T.tmm_hist + 6 * slot;
-    const float p1v = T.hist[slot * 3 * pl + (int64_t)T.exc_y * pitch + T.exc_x];
-    Dual st[6];
-    for (int i = 0; i < 6; ++i) {
-        st[i] = dconst(sv[i]);
-        st[i].d[i] = 1.0;
-    }
-    Dual p1 = dconst(p1v);
-    p1.d[6] = 1.0;
-    tmm_math(T.tmmd, st, p1);
-    double lout[6];
-    for (int i = 0; i < 6; ++i) lout[i] = A.lam_tmm[i];
-    lout[5] += lexe;                       // ug_curr after the step is exeV_n
-    double lin[kTmmIn];
-    for (int j = 0; j < kTmmIn; ++j) {
-        lin[j] = 0.0;
-        for (int i = 0; i < 6; ++i) lin[j] += lout[i] * st[i].d[j];
-    }
-    for (int i = 0; i < 6; ++i) A.lam_tmm[i] = lin[i];
-    A.lam[par ^ 1][(int64_t)T.exc_y * pitch + T.exc_x] += (float)lin[6];
 }
 
 // Slot 0 of every tube's history = the state before the first step of a
@@ -347,12 +331,10 @@ cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_
     return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_cells, int64_t n,
-                                int64_t slot, int par, bool tmm, cudaStream_t stream) {
-    const dim3 grid((max_cells + 255) / 256, ntubes);
-    adjoint_mu_kernel<<<grid, 256, 0, stream>>>(tubes, adj, n, par);
-    adjoint_lambda_kernel<<<grid, 256, 0, stream>>>(tubes, adj, slot, par);
-    if (tmm) tmm_adjoint_kernel<<<(ntubes + 31) / 32, 32, 0, stream>>>(tubes, adj, ntubes, slot, par);
+cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_tiles,
+                                const AdjRun* run, int local, cudaStream_t stream) {
+    const dim3 grid(max_tiles, ntubes);
+    adjoint_step_kernel<<<grid, kAdjTileW * kAdjTileH, 0, stream>>>(tubes, adj, run, local);
     return cudaGetLastError();
 }
 

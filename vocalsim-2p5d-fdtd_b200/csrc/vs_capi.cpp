@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -87,11 +88,20 @@ struct vs_batch {
     int ck_count = 0;
     char* ckpt = nullptr;                  // [ck_count][sum of state_bytes]
     size_t ckpt_stride = 0;
-    char* adj_mem = nullptr;               // history + lambda + mu + gradient planes
+    char* adj_mem = nullptr;               // history + lambda + gradient planes
+    size_t adj_bytes = 0;
+    std::vector<size_t> adj_off;           // per tube: offset of its block in adj_mem
     AdjTube* d_adj = nullptr;
+    AdjRun* d_adjrun = nullptr;
     float* d_gtrace = nullptr;
+    int64_t gtrace_cap = 0;
+    char* d_exc = nullptr;                 // excitation velocity lists (offsets, coefficients)
+    size_t exc_bytes = 0;
     Tile* d_hist_tiles = nullptr;
     int n_hist_tiles = 0;
+    cudaGraphExec_t hist_graph = nullptr;  // ck_every history steps
+    cudaGraphExec_t adj_graph = nullptr;   // ck_every reverse steps
+    int adj_graph_len = 0;
 
     ~vs_batch() { release(); }
 
@@ -107,9 +117,14 @@ struct vs_batch {
         if (ckpt) cudaFree(ckpt);
         if (adj_mem) cudaFree(adj_mem);
         if (d_adj) cudaFree(d_adj);
+        if (d_adjrun) cudaFree(d_adjrun);
         if (d_gtrace) cudaFree(d_gtrace);
+        if (d_exc) cudaFree(d_exc);
         if (d_hist_tiles) cudaFree(d_hist_tiles);
-        ckpt = nullptr; adj_mem = nullptr; d_adj = nullptr; d_gtrace = nullptr; d_hist_tiles = nullptr;
+        if (hist_graph) cudaGraphExecDestroy(hist_graph);
+        if (adj_graph) cudaGraphExecDestroy(adj_graph);
+        ckpt = nullptr; adj_mem = nullptr; d_adj = nullptr; d_adjrun = nullptr; d_gtrace = nullptr;
+        d_exc = nullptr; d_hist_tiles = nullptr; hist_graph = nullptr; adj_graph = nullptr;
         if (own_stream && stream) cudaStreamDestroy(stream);
         arena = nullptr; src_arena = nullptr; d_tubes = nullptr; d_tiles = nullptr;
         d_rs = nullptr; d_trace = nullptr; stream = nullptr;
@@ -465,67 +480,152 @@ void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces) 
     ck(cudaStreamSynchronize(b->stream), "forward sync");
 }
 
+// Velocities the excitation flow enters, per tube with the two-mass source:
+// lambda-plane offset and dV'/d exeV = ew mS / (mB + mS) (the source term of
+// FDTDEngineCPU.cpp:364-410 divided by the velocity denominator).
+void excitation_list(const TubeGrid& g, int64_t plane, std::vector<int32_t>& off, std::vector<float>& coef) {
+    off.clear();
+    coef.clear();
+    if (!g.tmm) return;
+    const int ex = g.dims.excitation_x;
+    auto type = [&](int r, int c) { return g.code[(size_t)r * g.pitch + c] & CODE_TYPE_MASK; };
+    for (int r = 1; r <= g.H - 2; ++r)
+        for (int c = std::max(ex - 1, 1); c <= std::min(ex, g.W - 2); ++c) {
+            const int tc = type(r, c), tr = type(r, c + 1), tt = type(r - 1, c);
+            const float ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
+            const float ewx = ec * g.dir[2] + er * g.dir[0], ewy = ec * g.dir[3] + et * g.dir[1];
+            const int64_t o = (int64_t)r * g.pitch + c;
+            if (ewx != 0.0f) {
+                const float mb = std::min(g.beta[tc], g.beta[tr]), ms = std::max(g.sigma[tc], g.sigma[tr]);
+                off.push_back((int32_t)(plane + o));
+                coef.push_back(ewx * ms / (mb + ms));
+            }
+            if (ewy != 0.0f) {
+                const float mb = std::min(g.beta[tc], g.beta[tt]), ms = std::max(g.sigma[tc], g.sigma[tt]);
+                off.push_back((int32_t)(2 * plane + o));
+                coef.push_back(ewy * ms / (mb + ms));
+            }
+        }
+}
+
+void capture(vs_batch* b, cudaGraphExec_t* out, const char* what, const std::function<cudaError_t(int)>& launch,
+             int count) {
+    if (*out) { cudaGraphExecDestroy(*out); *out = nullptr; }
+    cudaGraph_t g = nullptr;
+    ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaSuccess;
+    for (int i = 0; i < count && err == cudaSuccess; ++i) err = launch(i);
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    ck(err, what);
+    ck(e2, "end capture");
+    cudaError_t e3 = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    ck(e3, "instantiate graph");
+}
+
 void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float* gdY, float* gz) {
     if (b->ck_steps <= 0) throw VsFailure{VS_ERR_INVALID_ARG, "run vs_batch_forward_ckpt before vs_batch_adjoint"};
     check_adjoint_support(b);
     const int n = (int)b->grids.size();
     const int64_t steps = b->ck_steps;
     const int K = b->ck_every;
-    // device memory: per tube history (K+1 slots x 3 planes), lambda (2 x 3
-    // planes), mu (1 plane), gradients (4 double planes); with the two-mass
-    // source also its state history (K+1) and adjoint (6 doubles)
-    std::vector<size_t> off(n);
+    // device memory per tube: history (K+1 slots x 3 planes), then the part
+    // zeroed per call: lambda (2 x 3 planes), gradients (4 double planes) and,
+    // with the two-mass source, its state history (K+1) and adjoint (6)
+    std::vector<size_t> off(n), zero_off(n), zero_len(n);
     size_t total = 0;
-    int max_cells = 0, max_plane = 0;
-    bool any_tmm = false;
-    auto float_bytes = [&](size_t pe) { return align_up(pe * sizeof(float) * (3 * (size_t)(K + 1) + 6 + 1)); };
+    int max_tiles = 0, max_plane = 0;
     for (int i = 0; i < n; ++i) {
         const size_t pe = (size_t)b->h_tubes[i].plane;
         const TubeGrid& g = b->grids[i];
         off[i] = total;
-        total += float_bytes(pe) + align_up(pe * sizeof(double) * 4);
-        if (g.tmm) total += align_up((size_t)(K + 1) * 6 * sizeof(double)) + align_up(6 * sizeof(double));
-        any_tmm = any_tmm || g.tmm;
-        max_cells = std::max(max_cells, (g.H - 2) * (g.W - 2));
+        total += align_up(pe * sizeof(float) * 3 * (size_t)(K + 1));
+        zero_off[i] = total;
+        total += align_up(pe * sizeof(float) * 6) + align_up(pe * sizeof(double) * 4);
+        if (g.tmm) total += align_up((size_t)(K + 1) * 6 * sizeof(double)) + align_up(8 * sizeof(double));
+        zero_len[i] = total - zero_off[i];
+        const int tiles = ((g.W - 2 + kAdjTileW - 1) / kAdjTileW) * ((g.H - 2 + kAdjTileH - 1) / kAdjTileH);
+        max_tiles = std::max(max_tiles, tiles);
         max_plane = std::max(max_plane, g.H * g.pitch);
     }
-    if (b->adj_mem) { cudaFree(b->adj_mem); b->adj_mem = nullptr; }
-    ck(cudaMalloc(&b->adj_mem, total), "cudaMalloc(adjoint)");
-    ck(cudaMemsetAsync(b->adj_mem, 0, total, b->stream), "zero adjoint");
-    std::vector<AdjTube> adj(n);
-    if (b->d_gtrace) { cudaFree(b->d_gtrace); b->d_gtrace = nullptr; }
-    ck(cudaMalloc(&b->d_gtrace, (size_t)n * steps * sizeof(float)), "cudaMalloc(trace gradient)");
+    if (total != b->adj_bytes) {
+        if (b->adj_mem) { cudaFree(b->adj_mem); b->adj_mem = nullptr; b->adj_bytes = 0; }
+        ck(cudaMalloc(&b->adj_mem, total), "cudaMalloc(adjoint)");
+        b->adj_bytes = total;
+    }
+    for (int i = 0; i < n; ++i)
+        ck(cudaMemsetAsync(b->adj_mem + zero_off[i], 0, zero_len[i], b->stream), "zero adjoint");
+    if ((int64_t)n * steps > b->gtrace_cap) {
+        if (b->d_gtrace) { cudaFree(b->d_gtrace); b->d_gtrace = nullptr; }
+        ck(cudaMalloc(&b->d_gtrace, (size_t)n * steps * sizeof(float)), "cudaMalloc(trace gradient)");
+        b->gtrace_cap = (int64_t)n * steps;
+    }
     ck(cudaMemcpyAsync(b->d_gtrace, gtrace, (size_t)n * steps * sizeof(float), cudaMemcpyHostToDevice, b->stream),
        "upload trace gradient");
+    // excitation lists
+    std::vector<std::vector<int32_t>> eoff(n);
+    std::vector<std::vector<float>> ecoef(n);
+    size_t exc_total = 0;
     for (int i = 0; i < n; ++i) {
+        excitation_list(b->grids[i], b->h_tubes[i].plane, eoff[i], ecoef[i]);
+        exc_total += align_up(eoff[i].size() * sizeof(int32_t)) + align_up(ecoef[i].size() * sizeof(float));
+    }
+    if (exc_total > b->exc_bytes) {
+        if (b->d_exc) { cudaFree(b->d_exc); b->d_exc = nullptr; b->exc_bytes = 0; }
+        ck(cudaMalloc(&b->d_exc, exc_total), "cudaMalloc(excitation lists)");
+        b->exc_bytes = exc_total;
+    }
+    std::vector<AdjTube> adj(n);
+    size_t eo = 0;
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
         const size_t pe = (size_t)b->h_tubes[i].plane;
-        float* base = reinterpret_cast<float*>(b->adj_mem + off[i]);
-        b->h_tubes[i].hist = base;
-        float* lam = base + 3 * (size_t)(K + 1) * pe;
+        b->h_tubes[i].hist = reinterpret_cast<float*>(b->adj_mem + off[i]);
+        float* lam = reinterpret_cast<float*>(b->adj_mem + zero_off[i]);
         adj[i].lam[0] = lam;
         adj[i].lam[1] = lam + 3 * pe;
-        adj[i].mu = lam + 6 * pe;
-        char* gbase = b->adj_mem + off[i] + float_bytes(pe);
-        double* g = reinterpret_cast<double*>(gbase);
-        adj[i].gP = g;
-        adj[i].gX = g + pe;
-        adj[i].gY = g + 2 * pe;
-        adj[i].gZ = g + 3 * pe;
+        char* gbase = b->adj_mem + zero_off[i] + align_up(pe * sizeof(float) * 6);
+        double* gp = reinterpret_cast<double*>(gbase);
+        adj[i].gP = gp;
+        adj[i].gX = gp + pe;
+        adj[i].gY = gp + 2 * pe;
+        adj[i].gZ = gp + 3 * pe;
         adj[i].gtrace = b->d_gtrace + (size_t)i * steps;
         adj[i].lam_tmm = nullptr;
         b->h_tubes[i].tmm_hist = nullptr;
-        if (b->grids[i].tmm) {
+        if (g.tmm) {
             char* tbase = gbase + align_up(pe * sizeof(double) * 4);
             b->h_tubes[i].tmm_hist = reinterpret_cast<double*>(tbase);
             adj[i].lam_tmm = reinterpret_cast<double*>(tbase + align_up((size_t)(K + 1) * 6 * sizeof(double)));
         }
+        const size_t nb = eoff[i].size();
+        int32_t* d_off = reinterpret_cast<int32_t*>(b->d_exc + eo);
+        eo += align_up(nb * sizeof(int32_t));
+        float* d_coef = reinterpret_cast<float*>(b->d_exc + eo);
+        eo += align_up(nb * sizeof(float));
+        if (nb) {
+            ck(cudaMemcpyAsync(d_off, eoff[i].data(), nb * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream),
+               "upload excitation offsets");
+            ck(cudaMemcpyAsync(d_coef, ecoef[i].data(), nb * sizeof(float), cudaMemcpyHostToDevice, b->stream),
+               "upload excitation coefficients");
+        }
+        adj[i].exc_off = d_off;
+        adj[i].exc_coef = d_coef;
+        adj[i].n_exc = (int32_t)nb;
+        adj[i].tiles = ((g.W - 2 + kAdjTileW - 1) / kAdjTileW) * ((g.H - 2 + kAdjTileH - 1) / kAdjTileH);
+        if (g.tmm) max_tiles = std::max(max_tiles, adj[i].tiles + 1);
     }
-    if (b->d_adj) { cudaFree(b->d_adj); b->d_adj = nullptr; }
-    ck(cudaMalloc(&b->d_adj, n * sizeof(AdjTube)), "cudaMalloc(adjoint descriptors)");
+    if (!b->d_adj) ck(cudaMalloc(&b->d_adj, n * sizeof(AdjTube)), "cudaMalloc(adjoint descriptors)");
+    if (!b->d_adjrun) ck(cudaMalloc(&b->d_adjrun, sizeof(AdjRun)), "cudaMalloc(adjoint run state)");
     ck(cudaMemcpyAsync(b->d_adj, adj.data(), n * sizeof(AdjTube), cudaMemcpyHostToDevice, b->stream),
        "upload adjoint descriptors");
-    // strip list of the history-capturing step kernel
-    {
+    ck(cudaMemcpyAsync(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice, b->stream),
+       "upload tube descriptors");
+    // strip list of the history-capturing step kernel (static per batch)
+    int64_t cells = 0;
+    for (const TubeGrid& g : b->grids) cells += (int64_t)(g.H - 2) * (g.W - 2);
+    const int hshape = history_shape(cells);
+    if (!b->d_hist_tiles) {
         const int keep_shape = b->tiles_shape;
         Tile* keep_tiles = b->d_tiles;
         const int keep_n = b->ntiles;
@@ -534,8 +634,7 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         cudaGraphExec_t keep_graph = b->graph;
         const int keep_graph_shape = b->graph_shape;
         b->graph = nullptr;
-        build_tiles(b, history_shape());
-        if (b->d_hist_tiles) cudaFree(b->d_hist_tiles);
+        build_tiles(b, hshape);
         b->d_hist_tiles = b->d_tiles;
         b->n_hist_tiles = b->ntiles;
         b->d_tiles = keep_tiles;
@@ -544,32 +643,40 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         b->graph = keep_graph;
         b->graph_shape = keep_graph_shape;
     }
+    auto hist_step = [&](int j) {
+        return launch_step_history(hshape, b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, j, b->stream);
+    };
+    auto adj_step = [&](int j) { return launch_adjoint_step(b->d_tubes, b->d_adj, n, max_tiles, b->d_adjrun, j,
+                                                            b->stream); };
+    if (b->adj_graph_len != K || !b->hist_graph || !b->adj_graph) {
+        capture(b, &b->hist_graph, "capture history steps", hist_step, K);
+        capture(b, &b->adj_graph, "capture reverse steps", adj_step, K);
+        b->adj_graph_len = K;
+    }
     int q = 0;                    // lambda parity holding the adjoint of the later state
     for (int k = b->ck_count - 1; k >= 0; --k) {
         const int64_t start = (int64_t)k * K;
-        const int64_t len = std::min<int64_t>(K, steps - start);
+        const int len = (int)std::min<int64_t>(K, steps - start);
         copy_state(b, k, false);
-        for (int i = 0; i < n; ++i) b->h_tubes[i].hist_start = start;
-        ck(cudaMemcpyAsync(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice, b->stream),
-           "upload tube descriptors");
         RunState rs{};
         rs.step = start;
         rs.run_start = start;
         rs.trace = b->d_trace;
         rs.trace_stride = len;
         ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
+        const AdjRun ar{start, len, q};
+        ck(cudaMemcpyAsync(b->d_adjrun, &ar, sizeof(ar), cudaMemcpyHostToDevice, b->stream), "set adjoint run");
         ck(launch_history_seed(b->d_tubes, n, max_plane, (int)(start & 1), b->stream), "history seed");
-        for (int64_t j = 0; j < len; ++j)
-            ck(launch_step_history(b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, (int)j, b->stream),
-               "history step");
-        for (int64_t t = start + len - 1; t >= start; --t) {
-            ck(launch_adjoint_step(b->d_tubes, b->d_adj, n, max_cells, t, t - start, q, any_tmm, b->stream), "adjoint step");
-            q ^= 1;
+        if (len == K) {
+            ck(cudaGraphLaunch(b->hist_graph, b->stream), "history graph");
+            ck(cudaGraphLaunch(b->adj_graph, b->stream), "reverse graph");
+        } else {
+            for (int j = 0; j < len; ++j) ck(hist_step(j), "history step");
+            for (int j = 0; j < len; ++j) ck(adj_step(j), "adjoint step");
         }
-        // the host descriptors reach the device again before the next segment's
-        // launches: wait for this segment before rewriting them
-        ck(cudaStreamSynchronize(b->stream), "adjoint segment sync");
+        q ^= len & 1;
     }
+    ck(cudaStreamSynchronize(b->stream), "adjoint sync");
     // gradients to the caller, frame by frame (unpadded)
     size_t cell_off = 0;
     for (int i = 0; i < n; ++i) {

@@ -48,9 +48,8 @@ struct TubeDev {
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
     // state history for the adjoint's recomputation (strip kernel with
     // history capture only): the state after step n goes to slot
-    // n + 1 - hist_start, slot = [P, Vx, Vy] planes, `plane` apart
+    // n + 1 - RunState::run_start, slot = [P, Vx, Vy] planes, `plane` apart
     float* hist;
-    int64_t hist_start;
     double* tmm_hist;     // two-mass state before each step of the segment: 6 values
                           // per slot (x1_old, x1_curr, x2_old, x2_curr, ug_old, ug_curr)
 };
@@ -157,30 +156,51 @@ size_t shape_smem_bytes(int shape, int max_pitch);
 cudaError_t prepare_shape(int shape, int max_pitch);
 
 // One step of the strip kernel that also stores the new state into the tube's
-// history (TubeDev::hist); tubes without a wall oscillator only.
-cudaError_t launch_step_history(const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs, int local,
-                                cudaStream_t stream);
-int history_shape();
+// history (TubeDev::hist); tubes without a wall oscillator only.  `shape` is
+// history_shape() of the batch's interior cell count (the strips in `tiles`
+// must be built for it).
+cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
+                                int local, cudaStream_t stream);
+int history_shape(int64_t cells);
 
 // Adjoint buffers of one tube (device memory).
 struct AdjTube {
     float* lam[2];        // [parity]: lambda P, Vx, Vy planes at +0, +plane, +2*plane
-    float* mu;            // adjoint of P' (one plane; ring kept zero)
     double* gP;           // per-cell gradient accumulators of dP, dX, dY, z_inv
     double* gX;
     double* gY;
     double* gZ;
     const float* gtrace;  // dL/d trace[step], this tube's row
-    double* lam_tmm;      // adjoint of the two-mass state (6 values)
+    double* lam_tmm;      // adjoint of the two-mass state (6 values), then [6 + parity]:
+                          // d/d p1 pending for lambda P of that parity at the excitation point
+    // the velocities the excitation flow enters: lambda-plane offsets (Vx at
+    // plane + o, Vy at 2 plane + o) and dV'/d exeV of each
+    const int32_t* exc_off;
+    const float* exc_coef;
+    int32_t n_exc;
+    int32_t tiles;        // 32 x 8 cell tiles of the interior
 };
 
-// Reverse of forward step n for every tube: the adjoint of the state after
-// step n is in lam[par], the adjoint of the state before it goes to
-// lam[par ^ 1]; slot j of TubeDev::hist holds the state before step n.  With
-// `tmm`, tubes with the two-mass source also run its reverse step (after the
-// cell update, adding the pressure term at the excitation point).
-cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_cells, int64_t n,
-                                int64_t slot, int par, bool tmm, cudaStream_t stream);
+// Segment of the reverse sweep, in device memory so that one captured graph
+// serves every segment: launch `local` reverses forward step
+// n = start + len - 1 - local, whose state-before is history slot n - start;
+// the adjoint of the state after it is in lambda parity q0 ^ (local & 1).
+struct AdjRun {
+    int64_t start;
+    int32_t len;
+    int32_t q0;
+};
+
+// Tile of the reverse step kernel.
+constexpr int kAdjTileW = 32, kAdjTileH = 8;
+
+// One reverse step (launch index `local` of the segment in `run`) for every
+// tube: lambda of the state before the step, the map / z_inv gradient terms
+// and, for the two-mass source, its reverse step.  max_tiles = the largest
+// AdjTube::tiles of the batch, plus one when a tube has the two-mass source
+// (its reverse step runs in the block after the tiles).
+cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_tiles,
+                                const AdjRun* run, int local, cudaStream_t stream);
 
 // Copy each tube's state (parity par) into slot 0 of its history (and the
 // two-mass state into slot 0 of tmm_hist).

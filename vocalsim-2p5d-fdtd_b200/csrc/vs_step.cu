@@ -344,7 +344,7 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                 const bool owner =
                     T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= kStripLead && ex < kStripLead + kStripCommit;
                 exeV = glottal_step(T, par, Pin[(size_t)T->exc_y * pitch + T->exc_x], owner,
-                                    HIST ? T->tmm_hist + 6 * (n + 1 - T->hist_start) : nullptr);
+                                    HIST ? T->tmm_hist + 6 * (n + 1 - rs->run_start) : nullptr);
             }
             exeV = __shfl_sync(kFull, exeV, 0);
         } else {
@@ -445,7 +445,7 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                 Vxout[o] = vx;
                 Vyout[o] = vy;
                 if (HIST) {
-                    float* h = T->hist + (n + 1 - T->hist_start) * 3 * pl;
+                    float* h = T->hist + (n + 1 - rs->run_start) * 3 * pl;
                     h[o] = pn;
                     h[pl + o] = vx;
                     h[2 * pl + o] = vy;
@@ -746,13 +746,20 @@ cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* 
     return cudaGetLastError();
 }
 
-int history_shape() { return 2; }
+int history_shape(int64_t cells) { return cells < 200000 ? 7 : 2; }
 
-cudaError_t launch_step_history(const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs, int local,
-                                cudaStream_t stream) {
-    // shape 2 of the table: 8-row strips, 4 warps per CTA
+cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
+                                int local, cudaStream_t stream) {
+    // shape 7 of the table (2-row strips, 2 warps per CTA) for small grids,
+    // whose step time is the latency of a strip; shape 2 (8-row strips, 4
+    // warps per CTA) otherwise
     if (ntiles <= 0) return cudaSuccess;
-    strip_kernel<8, 4, false, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    if (shape == 7)
+        strip_kernel<2, 4, false, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else if (shape == 2)
+        strip_kernel<8, 4, false, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else
+        return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
