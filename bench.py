@@ -56,13 +56,13 @@ def max_over_ranks(ms: float, world: int, device=None) -> float:
     return float(t.item())
 
 
-def workload_params(rank: int, n_tubes: int):
+def workload_params(rank: int, n_tubes: int, fast_math: int = 1):
     from vocalsim_b200 import synthetic as S
     import vocalsim_b200 as V
     ps, gs = [], []
     for seed in rank_tube_seeds(rank, n_tubes):
         L, A, _, _ = S.batch_tube(seed)
-        ps.append(V.params(cross_sectional_shape=2, num_steps=SIM_STEPS))
+        ps.append(V.params(cross_sectional_shape=2, num_steps=SIM_STEPS, fast_math=fast_math))
         gs.append(V.Geometry(L, A))
     return ps, gs
 
@@ -263,7 +263,8 @@ def run_b200(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream(dev)
-    ps, gs = workload_params(rank, args.tubes)
+    fast = 1 if args.arith == "fast" else 0
+    ps, gs = workload_params(rank, args.tubes, fast)
     batch = V.Batch(ps, gs)
     batch.set_stream(stream.cuda_stream)
     cells = batch.interior_cells
@@ -333,7 +334,8 @@ def run_b200(args, rank, world):
     if not args.no_single:
         from vocalsim_b200 import synthetic as S
         L, A = S.uniform_tube()
-        s = V.Solver(V.params(mu3d=0.005, uniform_depth_m=0.02, num_steps=SIM_STEPS), V.Geometry(L, A))
+        s = V.Solver(V.params(mu3d=0.005, uniform_depth_m=0.02, num_steps=SIM_STEPS, fast_math=fast),
+                     V.Geometry(L, A))
         s.set_stream(stream.cuda_stream)
         dtr = torch.empty(SIM_STEPS, dtype=torch.float32, device=dev)
         s.run_device(SIM_STEPS, dtr.data_ptr())
@@ -373,6 +375,7 @@ def run_b200(args, rank, world):
                                "50 ms (33075 steps) at fs 661.5 kHz; one step = one full forward",
                    "tubes_per_gpu": args.tubes, "interior_cells_per_gpu": cells, "sim_steps": sim_steps,
                    "tile": list(V.tile_shapes()[tile]), "parallelism": f"tube sharding x{world} (no collective)",
+                   "arithmetic": "reciprocal form (fast_math=1)" if fast else "reference rounding (fast_math=0)",
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells),
@@ -404,6 +407,8 @@ def main():
     ap.add_argument("--no-single", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--arith", choices=["fast", "exact"], default="fast",
+                    help="fast: reciprocal-form arithmetic (fast_math = 1); exact: the reference's rounding")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -108,7 +108,15 @@ typedef struct vs_params {
                                       fs = 661.5 kHz and drifts from its double
                                       restatement (0.2% rel-L2 of the flow by 2000
                                       steps); the double model tracks it to ~1e-8.    */
-    int32_t reserved[7];
+    /* arithmetic (no counterpart in the reference) */
+    int32_t fast_math;             /* 0: the reference's expressions and rounding (traces
+                                      equal the FP32 engine's); 1: reciprocal form --
+                                      (P - K1 S / dP) / (1 + sigma) with a 1-ulp
+                                      reciprocal, and the velocity denominators as
+                                      correctly rounded table reciprocals -- for the
+                                      quad-strip kernels (no coupled wall).  Every tube
+                                      of a batch must use the same value.            */
+    int32_t reserved[6];
 } vs_params;
 
 /* Area function: n sections of (length cm, area cm^2), the pairs the reference

@@ -172,12 +172,20 @@ def test_invalid_geometry_rejected(bad):
 @pytest.mark.parametrize("field,value,status", [
     ("srate_mul", 0, 1), ("fdtd_solver_type", 3, 1), ("pml_flag", 2, 1), ("engine", 0, 1),
     ("source_type", 9, 1), ("cross_sectional_shape", 3, 7), ("listener_mode", 5, 1), ("tmm_f64", 2, 1),
+    ("fast_math", 2, 1),
 ])
 def test_invalid_params_rejected(field, value, status):
     L, A = S.vowel_tube(0)
     with pytest.raises(VsError) as e:
         V.build_maps(V.params(**{field: value}), V.Geometry(L, A))
     assert e.value.status == status
+
+
+def test_fast_math_with_coupled_wall_rejected():
+    L, A = S.vowel_tube(0)
+    with pytest.raises(VsError) as e:
+        V.build_maps(V.params(fast_math=1, cross_sectional_shape=2, wall_coupling=0.5), V.Geometry(L, A))
+    assert e.value.status == 7
 
 
 def test_listener_outside_frame_rejected():

@@ -81,6 +81,7 @@ struct vs_batch {
     int64_t step = 0;                      // host mirror of RunState::step
     int device = 0;
     bool wall = false;                     // some tube has the coupled wall oscillator
+    bool fast = false;                     // reciprocal-form arithmetic (vs_params::fast_math)
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
     // adjoint: checkpoints of the last checkpointed forward, history, adjoint planes
     int64_t ck_steps = 0;                  // steps of the checkpointed forward (0 = none)
@@ -139,9 +140,13 @@ namespace vsb {
 namespace {
 
 // Default launch shapes when no autotune ran: 16-row strips with 4 warps per
-// CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells.
+// CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells;
+// with fast_math the quad strips of the same heights (16 rows x 4 warps,
+// 2 rows x 2 warps).
 constexpr int kDefaultShape = 1;
 constexpr int kSmallShape = 8;
+constexpr int kFastShape = 17;
+constexpr int kFastSmallShape = 21;
 constexpr int64_t kSmallGridCells = 200000;
 
 int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
@@ -191,13 +196,23 @@ size_t smem_optin_limit(int device) {
 }
 
 bool shape_fits(const vs_batch* b, int shape) {
+    if (b->wall && tile_shape(shape).kind == SHAPE_QUAD) return false;   // no wall-oscillator variant
+    if (b->fast && !shape_has_fast(shape)) return false;
     return shape_smem_bytes(shape, b->max_pitch) <= smem_optin_limit(b->device);
+}
+
+int default_shape(const vs_batch* b) {
+    int64_t cells = 0;
+    for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
+    const bool small = cells < kSmallGridCells;
+    if (b->fast) return small ? kFastSmallShape : kFastShape;
+    return small ? kSmallShape : kDefaultShape;
 }
 
 void build_tiles(vs_batch* b, int shape) {
     if (b->tiles_shape == shape && b->d_tiles) return;
     const TileShape ts = tile_shape(shape);
-    if (!shape_fits(b, shape)) throw VsFailure{VS_ERR_UNSUPPORTED, "launch shape needs more shared memory than the device has"};
+    if (!shape_fits(b, shape)) throw VsFailure{VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)"};
     ck(prepare_shape(shape, b->max_pitch), "kernel attributes");
     std::vector<Tile> tiles;
     for (size_t i = 0; i < b->grids.size(); ++i) {
@@ -215,14 +230,16 @@ void build_tiles(vs_batch* b, int shape) {
                 tiles.push_back(t);
                 continue;
             }
-            // strips start at c0 = kStripCommit*k - kStripLead and commit columns
-            // c0+kStripLead .. c0+kStripLead+kStripCommit-1; rows r0 .. r0+rows-1
-            for (int c0 = -kStripLead; c0 + kStripLead <= g.W - 2; c0 += kStripCommit) {
+            // strips start at c0 = commit*k - lead and commit columns
+            // c0+lead .. c0+lead+commit-1; rows r0 .. r0+rows-1
+            const bool quad = ts.kind == SHAPE_QUAD;
+            const int lead = quad ? kQuadLead : kStripLead, commit = quad ? kQuadCommit : kStripCommit;
+            for (int c0 = -lead; c0 + lead <= g.W - 2; c0 += commit) {
                 Tile t{};
                 t.tube = (int32_t)i;
                 t.r0 = r0;
                 t.c0 = c0;
-                classify_strip(code_at, g.H, g.W, r0, ts.rows, c0, t);
+                classify_strip(code_at, g.H, g.W, r0, ts.rows, c0, t, lead, commit);
                 tiles.push_back(t);
             }
         }
@@ -243,7 +260,7 @@ void ensure_graph(vs_batch* b) {
     ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
     for (int i = 0; i < kChunk && err == cudaSuccess; ++i)
-        err = launch_step(b->shape, b->wall, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch);
+        err = launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch);
     if (err == cudaSuccess) err = launch_advance(b->d_rs, kChunk, b->stream);
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     ck(err, "capture step launches");
@@ -309,6 +326,10 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         b->wall = b->wall || g.wall_ode;
         b->max_pitch = std::max(b->max_pitch, g.pitch);
     }
+    b->fast = params[0].fast_math != 0;
+    for (int i = 1; i < n; ++i)
+        if ((params[i].fast_math != 0) != b->fast)
+            throw VsFailure{VS_ERR_INVALID_ARG, "every tube of a batch needs the same fast_math"};
     ck(cudaMalloc(&b->arena, total), "cudaMalloc(arena)");
     b->h_tubes.resize(n);
     b->src_len.assign(n, 0);
@@ -346,7 +367,11 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.K1 = g.K1; t.K2 = g.K2; t.bcoef = g.bcoef; t.zinv = g.zinv_val;
         t.dt = g.dt; t.Mw = g.Mw; t.Bw = g.Bw; t.Kw = g.Kw; t.cpl = g.cpl;
         t.dir0 = g.dir[0]; t.dir1 = g.dir[1]; t.dir2 = g.dir[2]; t.dir3 = g.dir[3];
-        for (int k = 0; k < 13; ++k) t.sigma[k] = g.sigma[k];
+        for (int k = 0; k < 13; ++k) {
+            t.sigma[k] = g.sigma[k];
+            t.ginv[k] = (float)(1.0 / (1.0 + (double)g.sigma[k]));
+            t.hinv[k] = g.sigma[k] > 0.0f ? (float)(1.0 / (double)g.sigma[k]) : INFINITY;
+        }
         t.tmmc = g.tmmc;
         t.tmmd = g.tmmd;
     }
@@ -360,14 +385,12 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
     upload_static(b);
     reset_state(b);
     // small grids (a single tube) need short strips to spread over the SMs
-    int64_t cells = 0;
-    for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
-    b->shape = cells < kSmallGridCells ? kSmallShape : kDefaultShape;
+    b->shape = default_shape(b);
 }
 
 void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     const int n = (int)b->grids.size();
-    if (b->shape < 0) b->shape = kDefaultShape;
+    if (b->shape < 0) b->shape = default_shape(b);
     build_tiles(b, b->shape);
     upload_sources(b, b->step + steps);
     const int64_t need = (int64_t)n * steps;
@@ -390,7 +413,7 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     }
     const int rem = (int)(steps - done);
     for (int i = 0; i < rem; ++i)
-        ck(launch_step(b->shape, b->wall, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch), "step launch");
+        ck(launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch), "step launch");
     if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
     b->step += steps;
     if (traces) {
@@ -426,7 +449,7 @@ void issue_steps(vs_batch* b, int64_t count) {
     }
     const int rem = (int)(count - done);
     for (int i = 0; i < rem; ++i)
-        ck(launch_step(b->shape, b->wall, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch),
+        ck(launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch),
            "step launch");
     if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
 }
@@ -445,7 +468,7 @@ void copy_state(vs_batch* b, int k, bool save) {
 void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces) {
     check_adjoint_support(b);
     const int n = (int)b->grids.size();
-    if (b->shape < 0) b->shape = kDefaultShape;
+    if (b->shape < 0) b->shape = default_shape(b);
     build_tiles(b, b->shape);
     reset_state(b);
     upload_sources(b, steps);
@@ -821,8 +844,8 @@ int vs_batch_reset(vs_batch* b) {
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index) {
     if (!b || tile_index < -1 || tile_index >= tile_shape_count())
         return set_error(VS_ERR_INVALID_ARG, "tile index out of range");
-    const int s = tile_index < 0 ? kDefaultShape : tile_index;
-    if (!shape_fits(b, s)) return set_error(VS_ERR_UNSUPPORTED, "launch shape needs more shared memory than the device has");
+    const int s = tile_index < 0 ? default_shape(b) : tile_index;
+    if (!shape_fits(b, s)) return set_error(VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)");
     b->shape = s;
     return VS_OK;
 }
@@ -834,7 +857,7 @@ int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* be
         ck(cudaEventCreate(&e0), "event");
         ck(cudaEventCreate(&e1), "event");
         float best = 1e30f;
-        int best_i = kDefaultShape;
+        int best_i = default_shape(b);
         for (int s = 0; s < tile_shape_count(); ++s) {
             if (!shape_fits(b, s)) continue;
             b->shape = s;

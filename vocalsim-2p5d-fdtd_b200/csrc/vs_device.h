@@ -44,6 +44,8 @@ struct TubeDev {
     float dt, Mw, Bw, Kw, cpl;
     float dir0, dir1, dir2, dir3;
     float sigma[13];
+    float ginv[13];       // 1 / (1 + sigma[t]) and 1 / sigma[t] (infinity for 0), correctly
+    float hinv[13];       // rounded: the reciprocal-form arithmetic (fast_math)
     TmmConsts tmmc;
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
     // state history for the adjoint's recomputation (strip kernel with
@@ -71,6 +73,12 @@ struct RunState {
 constexpr int kStripCommit = 30;
 constexpr int kStripLead = 1;
 constexpr int kMaxStripRows = 62;
+
+// Quad strips: lane i holds the four columns c0 + 4i .. c0 + 4i + 3 (c0 a
+// multiple of 4); lanes 1..30 commit the 120 columns c0 + 4 .. c0 + 123, and
+// strip k of a tube starts at c0 = 120 k - 4.
+constexpr int kQuadCommit = 120;
+constexpr int kQuadLead = 4;
 
 // A strip of one tube processed by one warp: rows [r0, r0+rows), starting
 // column c0.  The masks classify its rows once, from the static cell types,
@@ -100,18 +108,20 @@ __host__ __device__ inline int velocity_class(int kc, int kr, int kt) {
     return (beta_one(tc) && beta_one(tr) && beta_one(tt)) ? V_BETA1 : V_GENERIC;
 }
 
-// Masks and excitation flag of the strip (r0, rows, c0) of an H x W frame;
-// code(r, c) returns the code byte of a frame cell.
+// Masks and excitation flag of the strip (r0, rows, c0) of an H x W frame
+// that commits columns c0 + lead .. c0 + lead + commit - 1 (and computes P'
+// one column further); code(r, c) returns the code byte of a frame cell.
 template <class CodeAt>
-__host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0, int rows, int c0, Tile& t) {
+__host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0, int rows, int c0, Tile& t,
+                                               int lead = kStripLead, int commit = kStripCommit) {
     t.p_rows = 0;
     t.v_beta1 = 0;
     t.v_generic = 0;
     t.has_exc = 0;
     const int rlast = (r0 + rows - 1 < H - 2) ? r0 + rows - 1 : H - 2;
-    const int cfirst = c0 + 1 > 1 ? c0 + 1 : 1;
-    const int plast = c0 + 31 < W - 2 ? c0 + 31 : W - 2;
-    const int vlast = c0 + kStripCommit < W - 2 ? c0 + kStripCommit : W - 2;
+    const int cfirst = c0 + lead > 1 ? c0 + lead : 1;
+    const int plast = c0 + lead + commit < W - 2 ? c0 + lead + commit : W - 2;
+    const int vlast = c0 + lead + commit - 1 < W - 2 ? c0 + lead + commit - 1 : W - 2;
     for (int r = r0 - 1; r <= rlast; ++r) {
         if (r >= 1) {
             for (int c = cfirst; c <= plast; ++c)
@@ -131,10 +141,11 @@ __host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0
     }
 }
 
-// Host-side description of a compiled launch shape.  Strips: rows per strip,
-// committed columns per strip, warps per CTA.  Bands: rows per band (a band
-// spans the full frame width; cols = 0), warps per CTA.
-enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1 };
+// Host-side description of a compiled launch shape.  Strips and quad strips:
+// rows per strip, committed columns per strip, warps per CTA.  Bands: rows
+// per band (a band spans the full frame width; cols = 0), warps per CTA.
+// Quad strips have no wall-oscillator variant.
+enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1, SHAPE_QUAD = 2 };
 
 struct TileShape {
     int rows, cols, warps, kind;
@@ -146,9 +157,11 @@ TileShape tile_shape(int i);
 // Launch one time step (local index `local` after RunState::step) of every
 // strip or band in `tiles` with the compiled shape `shape`; `wall` selects
 // the kernel variant with the coupled wall oscillator (needed when any tube
-// has it); max_pitch sizes a band kernel's shared memory.
-cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* tiles, int ntiles,
+// has it), `fast` the reciprocal-form arithmetic (fast_math; quad strips
+// only, never with `wall`); max_pitch sizes a band kernel's shared memory.
+cudaError_t launch_step(int shape, bool wall, bool fast, const TubeDev* tubes, const Tile* tiles, int ntiles,
                         RunState* rs, int local, cudaStream_t stream, int max_pitch);
+bool shape_has_fast(int shape);
 
 // Dynamic shared memory a shape needs for frames of row pitch up to
 // max_pitch (0 for strips), and the one-time kernel attribute set-up for it.

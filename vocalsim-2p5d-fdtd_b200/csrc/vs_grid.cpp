@@ -108,6 +108,9 @@ private:
         if (p_.engine != VS_ENGINE_CPU && p_.engine != VS_ENGINE_EIGEN) raise(VS_ERR_INVALID_ARG, "engine must be VS_ENGINE_CPU or VS_ENGINE_EIGEN");
         if (p_.source_type < 0 || p_.source_type > 3) raise(VS_ERR_INVALID_ARG, "source_type must be 0..3");
         if (p_.tmm_f64 != 0 && p_.tmm_f64 != 1) raise(VS_ERR_INVALID_ARG, "tmm_f64 must be 0 or 1");
+        if (p_.fast_math != 0 && p_.fast_math != 1) raise(VS_ERR_INVALID_ARG, "fast_math must be 0 or 1");
+        if (p_.fast_math && p_.fdtd_solver_type == 1 && p_.wall_coupling != 0.0f)
+            raise(VS_ERR_UNSUPPORTED, "fast_math does not cover the coupled wall oscillator");
         if (p_.num_steps <= 0 && !(p_.audio_dur > 0.0f)) raise(VS_ERR_INVALID_ARG, "need num_steps > 0 or audio_dur > 0");
         if ((p_.source_type == VS_SRC_GAUSS || p_.source_type == VS_SRC_GAUSS_STD) && !(p_.gauss_width_s > 0.0f))
             raise(VS_ERR_INVALID_ARG, "gauss_width_s must be > 0");

@@ -124,6 +124,7 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
         return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: this source type needs the excitation table");
     if (p->srate_mul < 1 || p->srate_mul > 64 || (p->engine != VS_ENGINE_CPU && p->engine != VS_ENGINE_EIGEN))
         return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: invalid vs_params");
+    if (p->fast_math) return fail(VS_ERR_UNSUPPORTED, "vs_run_noalloc runs the reference arithmetic only (fast_math = 0)");
     const int H = dims->frame_h, W = dims->frame_w;
     if (H < 3 || W < 3) return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: frame smaller than 3 x 3");
     const int pitch = (W + 31) / 32 * 32;
@@ -215,7 +216,7 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     make_strips<<<(nitems + 127) / 128, 128, 0, st>>>(d_tiles, cell_type, z_inv, H, W, rows, nstrips, nitems);
     e = cudaGetLastError();
     for (int64_t i = 0; i < steps && e == cudaSuccess; ++i)
-        e = launch_step(kShape, wall, d_tube, d_tiles, nitems, d_rs, (int)i, st, pitch);
+        e = launch_step(kShape, wall, false, d_tube, d_tiles, nitems, d_rs, (int)i, st, pitch);
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));
     return VS_OK;
 }

@@ -40,19 +40,7 @@ __device__ __forceinline__ double dsub(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double dd(float a) { return (double)a; }
 __device__ __forceinline__ float tof(double a) { return __double2float_rn(a); }
 
-// SolverParams::setBeta (SolverParams.cu:5-27) for 6 PML layers; the normal
-// component tables of DeviceSymbols.cu:20-21.
-__constant__ float c_beta[16] = {0, 1, 0, 1, 1, 1, 1, 1, 1, 0, 0, 1, 0, 0, 0, 0};
-__constant__ float c_airN[4] = {0.0f, 1.0f, 1.0f, 0.707106f};
-__constant__ float c_wallN[4] = {1.0f, 1.0f, 1.0f, 0.0f};
-
 constexpr unsigned kFull = 0xffffffffu;
-
-// betaLookUpTable (FDTDSolver.cu:1047-1056) for beta in {0, 1}:
-// (air, air) -> 0, (air, wall) -> 1, (wall, air) -> 2, (wall, wall) -> 3.
-__device__ __forceinline__ int beta_lut(float br, float bt) {
-    return (br == 0.0f ? 2 : 0) + (bt == 0.0f ? 1 : 0);
-}
 
 // One step of the Ishizaka-Flanagan two-mass model, TwoMassModel.cpp:90-232,
 // in the reference's mixed float/double precision and operand order.  The
@@ -242,42 +230,79 @@ __device__ __forceinline__ float fdiv_z(float a, float b) { return a == 0.0f ? a
 // Velocity update of one cell, FDTDEngineCPU.cpp:364-410, with the 17
 // coefficient arrays of calculateSolverCoefficients (FDTDSolver.cu:652-801)
 // derived from the cell codes of the cell, its right and its top neighbour.
+//
+// Every beta is 0 or 1, so minBeta, x1..x4, the no-excitation factors and
+// the excitation weights multiply by exact 0 / 1 and the normal components
+// are 1 or 0.707106 chosen by the neighbours' betas (betaLookUpTable,
+// FDTDSolver.cu:1047-1056, with the tables of DeviceSymbols.cu:20-21).  The reference expression
+//   V' = ((mB V - bX dP) + exeV ew mS + mS zinv n (x2 Pc Nout - x1 Pn Nin)) / (mB + mS)
+// is evaluated here with those exact factors resolved by selects: the
+// remaining products, sums and the division are the reference's, in its
+// order, so the values are equal (a dropped term only ever adds an exact 0).
 struct VelocityOut { float vx, vy; };
+
+// beta per cell type (SolverParams::setBeta, SolverParams.cu:5-27): 1 for
+// air, PML 0..5 and no-pressure cells, 0 otherwise
+constexpr uint32_t kBetaMask = 0x9FAu;
+
+__device__ __forceinline__ bool beta_bit(int t) { return (kBetaMask >> t) & 1u; }
+
+template <bool FAST = false>
+__device__ __forceinline__ float velocity_dir(bool bc, bool bn, bool bo, bool ec, bool en, float dirc, float dirn,
+                                              float v0, float pc, float pn, float exeV, float mS, float zinv,
+                                              float bco, float rden = 0.0f) {
+    const bool mB = bc && bn;
+    float v = mB ? fsub(v0, fmul(bco, fsub(pn, pc))) : 0.0f;
+    if (ec || en) v = fadd(v, fmul(fmul(exeV, fadd(fmul((float)ec, dirc), fmul((float)en, dirn))), mS));
+    if (zinv != 0.0f && !(ec || en) && bc != bn) {
+        // x2 = bc (1 - bn): Pc * Nout, Nout = 1/sqrt(2) when the other neighbour is
+        // a wall (beta 0), else 1; x1 = bn (1 - bc): -Pn * Nin with Nin = 1
+        const float vb = bc ? fmul(pc, bo ? 1.0f : 0.707106f) : -pn;
+        v = fadd(v, fmul(mS, fmul(vb, zinv)));
+    }
+    if constexpr (FAST) return fmul(v, rden);     // rden = 1 / (mB + mS), correctly rounded
+    return fdiv_z(v, fadd(mB ? 1.0f : 0.0f, mS));
+}
 
 __device__ __forceinline__ VelocityOut velocity_generic(
         int kc, int kr, int kt, float pc, float pr, float pt, float vx0, float vy0, float exeV,
         const float* __restrict__ sig, float zval, float bco, float dir0, float dir1, float dir2, float dir3) {
     const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
-    const float bc = c_beta[tc], br = c_beta[tr], bt = c_beta[tt];
-    const int lut = beta_lut(br, bt);
-    const float Nout = fmul(c_airN[lut], bc);
-    const float Nin = fmul(c_wallN[lut], fsub(1.0f, bc));
-    const float sc = sig[tc], sr = sig[tr], st = sig[tt];
-    const int ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
-    const float mBx = fminf(bc, br), mBy = fminf(bc, bt);
-    const float mSx = fmaxf(sc, sr), mSy = fmaxf(sc, st);
-    // (minBeta^2 * dt) / (rho * ds) with minBeta in {0, 1}
-    const float bX = mBx != 0.0f ? bco : 0.0f;
-    const float bY = mBy != 0.0f ? bco : 0.0f;
-    const float nX = (float)((1 - ec) * (1 - er));
-    const float nY = (float)((1 - ec) * (1 - et));
-    const float ewX = fadd(fmul((float)ec, dir2), fmul((float)er, dir0));
-    const float ewY = fadd(fmul((float)ec, dir3), fmul((float)et, dir1));
-    const float x1 = fmul(br, fsub(1.0f, bc)), x2 = fmul(bc, fsub(1.0f, br));
-    const float x3 = fmul(bt, fsub(1.0f, bc)), x4 = fmul(bc, fsub(1.0f, bt));
+    const bool bc = beta_bit(tc), br = beta_bit(tr), bt = beta_bit(tt);
+    const bool ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
+    const float sc = sig[tc];
     const float zinv = (kc & CODE_ZINV_BIT) ? zval : 0.0f;
-    const float CxP = fsub(pr, pc), CyP = fsub(pt, pc);
-    float vx = fsub(fmul(mBx, vx0), fmul(bX, CxP));
-    float vy = fsub(fmul(mBy, vy0), fmul(bY, CyP));
-    vx = fadd(vx, fmul(fmul(exeV, ewX), mSx));
-    vy = fadd(vy, fmul(fmul(exeV, ewY), mSy));
-    float vbx = fsub(fmul(fmul(x2, pc), Nout), fmul(fmul(x1, pr), Nin));
-    float vby = fsub(fmul(fmul(x4, pc), Nout), fmul(fmul(x3, pt), Nin));
-    vbx = fmul(fmul(vbx, nX), zinv);
-    vby = fmul(fmul(vby, nY), zinv);
-    vx = fadd(vx, fmul(mSx, vbx));
-    vy = fadd(vy, fmul(mSy, vby));
-    return {fdiv_z(vx, fadd(mBx, mSx)), fdiv_z(vy, fadd(mBy, mSy))};
+    return {velocity_dir(bc, br, bt, ec, er, dir2, dir0, vx0, pc, pr, exeV, fmaxf(sc, sig[tr]), zinv, bco),
+            velocity_dir(bc, bt, br, ec, et, dir3, dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco)};
+}
+
+// The same update in the reciprocal form (fast_math): the denominators
+// mB + mS come from the tube's tables of 1 / (1 + sigma) (ginv) and
+// 1 / sigma (hinv): 1 / (1 + max(s1, s2)) = min(ginv), 1 / max(s1, s2) = min(hinv).
+__device__ __forceinline__ VelocityOut velocity_generic_fast(
+        int kc, int kr, int kt, float pc, float pr, float pt, float vx0, float vy0, float exeV,
+        const TubeDev* __restrict__ T, float bco) {
+    const float* __restrict__ sig = T->sigma;
+    const float* __restrict__ gi = T->ginv;
+    const float* __restrict__ hi = T->hinv;
+    const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
+    const bool bc = beta_bit(tc), br = beta_bit(tr), bt = beta_bit(tt);
+    const bool ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
+    const float sc = sig[tc];
+    const float zinv = (kc & CODE_ZINV_BIT) ? T->zinv : 0.0f;
+    const float rx = (bc && br) ? fminf(gi[tc], gi[tr]) : fminf(hi[tc], hi[tr]);
+    const float ry = (bc && bt) ? fminf(gi[tc], gi[tt]) : fminf(hi[tc], hi[tt]);
+    return {velocity_dir<true>(bc, br, bt, ec, er, T->dir2, T->dir0, vx0, pc, pr, exeV, fmaxf(sc, sig[tr]), zinv, bco,
+                               rx),
+            velocity_dir<true>(bc, bt, br, ec, et, T->dir3, T->dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco,
+                               ry)};
+}
+
+// Approximate reciprocal (PTX rcp.approx.f32, at most 1 ulp from 1/x).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 // Row-marching strip kernel.  One warp owns a strip of 32 columns x TR rows:
@@ -461,16 +486,7 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     }
 }
 
-// ---------------------------------------------------------------------------
-// Band kernel: one CTA per band of R rows of a tube.  A band's rows are
-// contiguous in every plane (rows are `pitch` apart), so the rows r0-1 ..
-// r0+R of P, Vx, Vy, dP, dX, dY and the codes arrive with one bulk copy per
-// plane (cp.async.bulk, completion on an mbarrier) and no registers held in
-// flight.  The CTA then computes P' for rows r0-1 .. r0+R-1 into shared
-// memory and V' for rows r0 .. r0+R-1, with the same arithmetic as the
-// strip kernel (value-identical to the reference expressions), and stores
-// both to global memory.
-// ---------------------------------------------------------------------------
+// ---- mbarrier and bulk-copy helpers (strip pipelines and bands) ----------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -516,6 +532,378 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit)
 }
 
 constexpr uint32_t kWaitPolls = 1u << 22;
+
+// Bounded wait on the phase with the given parity.
+__device__ __forceinline__ bool mbar_wait_parity_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Quad-strip kernel: the strip kernel's row pipeline with four consecutive
+// columns per lane.  A warp covers the 128 columns c0 .. c0 + 127, lane i
+// holding x0 = c0 + 4i .. x0 + 3; c0 is a multiple of 4, so each lane's
+// share of a plane row is one aligned 16-byte piece.  Lane 0 only supplies
+// the left depth flux of column c0 + 4 and lane 31 only the P' right of
+// column c0 + 123; lanes 1..30 commit the 120 columns between.  Per row and
+// lane: seven 16-byte reads, three shuffles and four cells.  Same arithmetic
+// as the strip kernel, cell by cell; no wall oscillator and no history
+// capture (those batches use the strip kernel).
+//
+// Row supply.  STAGES = 0: each row's loads are issued into registers one
+// row ahead.  STAGES > 0: lane 0 streams the strip's rows into a per-warp
+// ring of STAGES shared-memory stages with bulk copies (cp.async.bulk, one
+// per plane row, completion on the stage's mbarrier), keeping up to STAGES
+// rows in flight without holding registers; a stage is refilled as soon as
+// the warp has read it.  Waits are bounded: a stage that does not arrive
+// sets RunState::error, and the warp waits (bounded) for its remaining
+// copies before it leaves.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ld4(float (&d)[4], const float* p) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+
+__device__ __forceinline__ void lds4(float (&d)[4], const unsigned char* p) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+
+__device__ __forceinline__ void st4(float* p, const float (&v)[4], unsigned mask) {
+    if (mask == 0xfu) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if ((mask >> q) & 1u) p[q] = v[q];
+    }
+}
+
+__device__ __forceinline__ int code_byte(uint32_t k, int q) { return (int)((k >> (8 * q)) & 0xffu); }
+
+// Stage layout: Vx, dX, P, dP, Vy, dY row pieces (512 B each), then 144 code
+// bytes from the 16-byte boundary at or below column c0.
+constexpr uint32_t kQSeg = 512;
+constexpr uint32_t kQCode = 144;
+constexpr uint32_t kQStage = 6 * kQSeg + 160;
+constexpr uint32_t kQBars = 128;                 // per-warp mbarrier area (up to 16 stages)
+
+__host__ __device__ constexpr uint32_t quad_warp_smem(int stages) {
+    return stages > 0 ? kQBars + (uint32_t)stages * kQStage : 0;
+}
+
+template <int TR, int WARPS, int MINB, int STAGES, bool FAST>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
+            RunState* __restrict__ rs, int local) {
+    extern __shared__ __align__(128) unsigned char q_smem[];
+    const int lane = threadIdx.x & 31;
+    const int wi = blockIdx.x * WARPS + (threadIdx.x >> 5);
+    if (wi >= nitems) return;
+    const Tile it = items[wi];
+    const TubeDev* __restrict__ T = tubes + it.tube;
+    const int64_t n = rs->step + local;
+    const int par = (int)(n & 1);
+    const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
+    const int r0 = it.r0, c0 = it.c0, x0 = c0 + 4 * lane;
+    // columns of this lane that compute P' / commit
+    unsigned calc_m = 0, commit_m = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool c = lane >= 1 && x0 + q >= 1 && x0 + q <= W - 2;
+        calc_m |= (unsigned)c << q;
+        commit_m |= (unsigned)(c && lane <= 30) << q;
+    }
+    // planes P0 P1 Vx0 Vx1 Vy0 Vy1 and dP dX dY, `plane` apart.  Rows
+    // r0-1 .. r0+TR of columns c0-12 .. c0+127 are read without predicates:
+    // the arena keeps guard bytes around every tube, and values read outside
+    // the frame only reach columns that neither compute nor commit them.
+    const int64_t pl = T->plane;
+    const float* __restrict__ Pin = T->P[0] + par * pl;
+    float* __restrict__ Pout = T->P[0] + (par ^ 1) * pl;
+    const float* __restrict__ Vxin = Pin + 2 * pl;
+    const float* __restrict__ Vyin = Pin + 4 * pl;
+    float* __restrict__ Vxout = Pout + 2 * pl;
+    float* __restrict__ Vyout = Pout + 4 * pl;
+    const float* __restrict__ dPp = T->dP;
+    const float* __restrict__ dXp = dPp + pl;
+    const float* __restrict__ dYp = dPp + 2 * pl;
+    const uint8_t* __restrict__ code = T->code;
+    const float* __restrict__ sig = T->sigma;
+    const float K1 = T->K1, bco = T->bcoef;
+    const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
+    const int lis_y = T->lis_y, lis_q = T->lis_x - x0;
+    const uint64_t pmask = it.p_rows, vb1 = it.v_beta1, vgen = it.v_generic;
+    const int rlast = min(r0 + TR - 1, H - 2);
+
+    // ---- row supply
+    constexpr int kS = STAGES > 0 ? STAGES : 1;
+    uint64_t* bars = nullptr;
+    unsigned char* stages = nullptr;
+    const int nrows = rlast - r0 + 3;                 // rows r0-1 .. rlast+1
+    const int cshift = c0 & 15;                        // code bytes ahead of column c0 in a stage
+    if constexpr (STAGES > 0) {
+        unsigned char* wbase = q_smem + (threadIdx.x >> 5) * quad_warp_smem(STAGES);
+        bars = reinterpret_cast<uint64_t*>(wbase);
+        stages = wbase + kQBars;
+        if (lane == 0) {
+            for (int s2 = 0; s2 < STAGES; ++s2) mbar_init(bars + s2, 1);
+            mbar_fence_init();
+        }
+        __syncwarp();
+    }
+    auto issue = [&](int i) {                           // lane 0: stage row r0 - 1 + i
+        const int s2 = i % kS;
+        uint64_t* bar = bars + s2;
+        unsigned char* st = stages + s2 * kQStage;
+        const int64_t off = (int64_t)(r0 - 1 + i) * pitch + c0;
+        mbar_expect_tx(bar, 6 * kQSeg + kQCode);
+        bulk_g2s(st + 0 * kQSeg, Vxin + off, kQSeg, bar);
+        bulk_g2s(st + 1 * kQSeg, dXp + off, kQSeg, bar);
+        bulk_g2s(st + 2 * kQSeg, Pin + off, kQSeg, bar);
+        bulk_g2s(st + 3 * kQSeg, dPp + off, kQSeg, bar);
+        bulk_g2s(st + 4 * kQSeg, Vyin + off, kQSeg, bar);
+        bulk_g2s(st + 5 * kQSeg, dYp + off, kQSeg, bar);
+        bulk_g2s(st + 6 * kQSeg, code + (off & ~(int64_t)15), kQCode, bar);
+    };
+    auto wait_row = [&](int i) -> bool {
+        const bool ok = mbar_wait_parity_bounded(bars + i % kS, (uint32_t)(i / kS) & 1u, kWaitPolls);
+        return __all_sync(kFull, ok);
+    };
+    auto drain = [&](int from, int issued) {            // after a timeout: bounded wait for copies in flight
+        if (lane == 0) {
+            atomicExch(&rs->error, VS_ERR_TIMEOUT);
+            for (int i = from; i < issued; ++i)
+                mbar_wait_parity_bounded(bars + i % kS, (uint32_t)(i / kS) & 1u, kWaitPolls);
+        }
+        __syncwarp();
+    };
+    int issued = 0;
+    if constexpr (STAGES > 0) {
+        if (lane == 0)
+            for (int i = 0; i < STAGES && i < nrows; ++i) issue(i);
+        issued = min(STAGES, nrows);
+    }
+
+    float exeV = 0.0f;
+    if (it.has_exc) {
+        if (flags & TUBE_TMM) {
+            if (lane == 0) {
+                const int ex = T->exc_x - c0;
+                const bool owner =
+                    T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= kQuadLead && ex < kQuadLead + kQuadCommit;
+                exeV = glottal_step(T, par, Pin[(size_t)T->exc_y * pitch + T->exc_x], owner, nullptr);
+            }
+            exeV = __shfl_sync(kFull, exeV, 0);
+        } else {
+            exeV = n < T->src_len ? T->src[n] : 0.0f;
+        }
+    }
+
+    int r = r0 - 1;
+    int o = r * pitch + x0;
+    float vx_c[4], ux_c[4], p_c[4], dp_c[4], vy_c[4], uy_c[4], vy_n[4], uy_n[4], p_above[4], t4[4];
+    uint32_t k_c;
+    if constexpr (STAGES > 0) {
+        if (!wait_row(0)) { drain(0, issued); return; }
+        const unsigned char* st = stages;
+        lds4(vy_c, st + 4 * kQSeg + 16 * lane);
+        lds4(t4, st + 5 * kQSeg + 16 * lane);
+    } else {
+        ld4(vx_c, Vxin + o);
+        ld4(t4, dXp + o);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ux_c[q] = fmul(vx_c[q], t4[q]);
+        ld4(p_c, Pin + o);
+        ld4(dp_c, dPp + o);
+        k_c = __ldg(reinterpret_cast<const unsigned int*>(code + o));
+        ld4(vy_c, Vyin + o);
+        ld4(t4, dYp + o);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uy_c[q] = fmul(vy_c[q], t4[q]);
+        p_above[q] = 0.0f;
+    }
+    if constexpr (STAGES == 0) {
+        ld4(vy_n, Vyin + o + pitch);
+        ld4(t4, dYp + o + pitch);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) uy_n[q] = fmul(vy_n[q], t4[q]);
+    }
+    uint32_t k_above = 0;
+
+    for (int j = 0; r <= rlast; ++j, ++r) {
+        const int o1 = o + pitch;
+        float vx_1[4], dx_1[4], p_1[4], dp_1[4], vy_2[4], dy_2[4];
+        uint32_t k_1 = 0;
+        if constexpr (STAGES > 0) {
+            // row r from stage j (waited last iteration), Vy dY of row r+1 from stage j+1
+            if (!wait_row(j + 1)) { drain(j + 1, issued); return; }
+            const unsigned char* st = stages + (j % kS) * kQStage;
+            const unsigned char* sn = stages + ((j + 1) % kS) * kQStage;
+            lds4(vx_c, st + 0 * kQSeg + 16 * lane);
+            lds4(t4, st + 1 * kQSeg + 16 * lane);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ux_c[q] = fmul(vx_c[q], t4[q]);
+            lds4(p_c, st + 2 * kQSeg + 16 * lane);
+            lds4(dp_c, st + 3 * kQSeg + 16 * lane);
+            k_c = *reinterpret_cast<const uint32_t*>(st + 6 * kQSeg + cshift + 4 * lane);
+            lds4(vy_n, sn + 4 * kQSeg + 16 * lane);
+            lds4(t4, sn + 5 * kQSeg + 16 * lane);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) uy_n[q] = fmul(vy_n[q], t4[q]);
+            __syncwarp();
+            if (lane == 0 && issued < nrows) {
+                // the warp has read stage j: refill it
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue(issued);
+            }
+            issued = min(issued + 1, nrows);
+        } else {
+            // loads for the next iterations (input planes are read-only this step)
+            ld4(vx_1, Vxin + o1);
+            ld4(dx_1, dXp + o1);
+            ld4(p_1, Pin + o1);
+            ld4(dp_1, dPp + o1);
+            k_1 = __ldg(reinterpret_cast<const unsigned int*>(code + o1));
+            if (r + 2 <= H - 1) {
+                ld4(vy_2, Vyin + o1 + pitch);
+                ld4(dy_2, dYp + o1 + pitch);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) { vy_2[q] = 0.0f; dy_2[q] = 0.0f; }
+            }
+        }
+
+        // ---- pressure of row r (FDTDEngineCPU.cpp:316-339)
+        const float ux_l = __shfl_up_sync(kFull, ux_c[3], 1);
+        const bool pgen = (pmask >> j) & 1;
+        const unsigned cm = r >= 1 ? calc_m : 0u;
+        float pn[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float uxl = q == 0 ? ux_l : ux_c[q - 1];
+            const int tc = code_byte(k_c, q) & CODE_TYPE_MASK;
+            if constexpr (FAST) {
+                // (P dP - K1 S) / ((1 + s) dP) = (P - K1 S / dP) / (1 + s)
+                const float ks = fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(uy_c[q], uy_n[q])));
+                float v = __fmaf_rn(-ks, rcp_approx(dp_c[q]), p_c[q]);
+                if (pgen && tc != VS_CELL_AIR) v = fmul(v, T->ginv[tc]);
+                pn[q] = ((cm >> q) & 1u) ? v : 0.0f;
+                if (pgen && dirichlet && tc == VS_CELL_NOPRESSURE) pn[q] = 0.0f;
+            } else {
+                const float num =
+                    fsub(fmul(p_c[q], dp_c[q]), fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(uy_c[q], uy_n[q]))));
+                float den = dp_c[q];
+                if (pgen && tc != VS_CELL_AIR) {
+                    const float s = sig[tc];
+                    den = eigen ? fadd(fmul(s, dp_c[q]), dp_c[q]) : fmul(fadd(1.0f, s), dp_c[q]);
+                }
+                pn[q] = 0.0f;
+                if ((cm >> q) & 1u) {
+                    pn[q] = fdiv_z(num, den);
+                    if (pgen && dirichlet && tc == VS_CELL_NOPRESSURE) pn[q] = 0.0f;
+                }
+            }
+        }
+        // ---- commit row r and its velocity (FDTDEngineCPU.cpp:364-410)
+        const float p_r3 = __shfl_down_sync(kFull, pn[0], 1);
+        const int k_r3 = code_byte(__shfl_down_sync(kFull, k_c, 1), 0);
+        if (j >= 1) {
+            const int jv = j - 1;
+            st4(Pout + o, pn, commit_m);
+            if (r == lis_y && lis_q >= 0 && lis_q < 4 && ((commit_m >> lis_q) & 1u)) {
+                float pv = pn[0];
+#pragma unroll
+                for (int q = 1; q < 4; ++q) if (lis_q == q) pv = pn[q];
+                rs->trace[(int64_t)it.tube * rs->trace_stride + (n - rs->run_start)] = pv;
+            }
+            float vx[4], vy[4];
+            if ((vgen >> jv) & 1) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    vx[q] = 0.0f;
+                    vy[q] = 0.0f;
+                    if ((commit_m >> q) & 1u) {
+                        const int kr = q < 3 ? code_byte(k_c, q + 1) : k_r3;
+                        const float pr = q < 3 ? pn[q + 1] : p_r3;
+                        VelocityOut v;
+                        if constexpr (FAST)
+                            v = velocity_generic_fast(code_byte(k_c, q), kr, code_byte(k_above, q), pn[q], pr,
+                                                      p_above[q], vx_c[q], vy_c[q], exeV, T, bco);
+                        else
+                            v = velocity_generic(code_byte(k_c, q), kr, code_byte(k_above, q), pn[q], pr, p_above[q],
+                                                 vx_c[q], vy_c[q], exeV, sig, T->zinv, bco, T->dir0, T->dir1,
+                                                 T->dir2, T->dir3);
+                        vx[q] = v.vx;
+                        vy[q] = v.vy;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float pr = q < 3 ? pn[q + 1] : p_r3;
+                    vx[q] = fsub(vx_c[q], fmul(bco, fsub(pr, pn[q])));
+                    vy[q] = fsub(vy_c[q], fmul(bco, fsub(p_above[q], pn[q])));
+                }
+                if ((vb1 >> jv) & 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int kr = q < 3 ? code_byte(k_c, q + 1) : k_r3;
+                        const int tcq = code_byte(k_c, q) & CODE_TYPE_MASK;
+                        const int trq = kr & CODE_TYPE_MASK, taq = code_byte(k_above, q) & CODE_TYPE_MASK;
+                        if constexpr (FAST) {
+                            const float* __restrict__ gi = T->ginv;
+                            const float gc = gi[tcq];
+                            vx[q] = fmul(vx[q], fminf(gc, gi[trq]));
+                            vy[q] = fmul(vy[q], fminf(gc, gi[taq]));
+                        } else {
+                            const float sc = sig[tcq];
+                            vx[q] = fdiv_z(vx[q], fadd(1.0f, fmaxf(sc, sig[trq])));
+                            vy[q] = fdiv_z(vy[q], fadd(1.0f, fmaxf(sc, sig[taq])));
+                        }
+                    }
+                }
+            }
+            st4(Vxout + o, vx, commit_m);
+            st4(Vyout + o, vy, commit_m);
+        }
+        // ---- shift the row pipeline
+        k_above = k_c;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            p_above[q] = pn[q];
+            vy_c[q] = vy_n[q];
+            uy_c[q] = uy_n[q];
+        }
+        if constexpr (STAGES == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                vy_n[q] = vy_2[q];
+                uy_n[q] = fmul(vy_2[q], dy_2[q]);
+                vx_c[q] = vx_1[q];
+                ux_c[q] = fmul(vx_1[q], dx_1[q]);
+                p_c[q] = p_1[q];
+                dp_c[q] = dp_1[q];
+            }
+            k_c = k_1;
+        }
+        o = o1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Band kernel: one CTA per band of R rows of a tube.  A band's rows are
+// contiguous in every plane (rows are `pitch` apart), so the rows r0-1 ..
+// r0+R of P, Vx, Vy, dP, dX, dY and the codes arrive with one bulk copy per
+// plane (cp.async.bulk, completion on an mbarrier) and no registers held in
+// flight.  The CTA then computes P' for rows r0-1 .. r0+R-1 into shared
+// memory and V' for rows r0 .. r0+R-1, with the same arithmetic as the
+// strip kernel (value-identical to the reference expressions), and stores
+// both to global memory.
+// ---------------------------------------------------------------------------
 constexpr int kBandThreads = 256;
 
 // Shared-memory bytes of a band kernel with R rows for a row pitch.
@@ -689,12 +1077,19 @@ using StepFn = void (*)(const TubeDev*, const Tile*, int, RunState*, int);
 
 struct ShapeEntry {
     int kind, rows, warps;
-    StepFn plain, wall;
+    StepFn plain, wall;   // wall = nullptr: no wall-oscillator variant
+    int stages;           // quad strips: shared-memory row stages per warp (0 = register prefetch)
+    StepFn fast;          // reciprocal-form arithmetic (fast_math); nullptr: none
 };
 
 #define VS_STRIP(R, WARPS, MINB) \
-    {SHAPE_STRIP, R, WARPS, strip_kernel<R, MINB, false>, strip_kernel<R, MINB, true>}
-#define VS_BAND(R) {SHAPE_BAND, R, kBandThreads / 32, band_kernel<R, false>, band_kernel<R, true>}
+    {SHAPE_STRIP, R, WARPS, strip_kernel<R, MINB, false>, strip_kernel<R, MINB, true>, 0, nullptr}
+#define VS_BAND(R) {SHAPE_BAND, R, kBandThreads / 32, band_kernel<R, false>, band_kernel<R, true>, 0, nullptr}
+#define VS_QUAD(R, WARPS, MINB)                                                                          \
+    {SHAPE_QUAD, R, WARPS, quad_kernel<R, WARPS, MINB, 0, false>, nullptr, 0, quad_kernel<R, WARPS, MINB, 0, true>}
+#define VS_QPIPE(R, WARPS, MINB, ST)                                                                     \
+    {SHAPE_QUAD, R, WARPS, quad_kernel<R, WARPS, MINB, ST, false>, nullptr, ST,                          \
+     quad_kernel<R, WARPS, MINB, ST, true>}
 
 // strips: (rows per strip, warps per CTA, CTAs per SM the register budget
 // targets); bands: rows per band (one CTA of 256 threads each)
@@ -703,9 +1098,15 @@ const ShapeEntry kShapes[] = {
     VS_STRIP(8, 8, 4),  VS_STRIP(16, 8, 4), VS_STRIP(32, 8, 4), VS_STRIP(2, 2, 4),
     VS_STRIP(4, 2, 4),  VS_STRIP(8, 2, 4),  VS_STRIP(16, 4, 3), VS_STRIP(8, 4, 3),
     VS_BAND(4),         VS_BAND(8),         VS_BAND(12),        VS_BAND(16),
+    VS_QUAD(8, 4, 4),   VS_QUAD(16, 4, 4),  VS_QUAD(4, 4, 4),   VS_QUAD(8, 2, 8),
+    VS_QUAD(16, 2, 8),  VS_QUAD(2, 2, 8),   VS_QUAD(8, 8, 2),   VS_QUAD(32, 4, 4),
+    VS_QPIPE(16, 4, 4, 4), VS_QPIPE(32, 4, 4, 4), VS_QPIPE(16, 2, 8, 4), VS_QPIPE(32, 2, 8, 4),
+    VS_QPIPE(16, 4, 2, 6), VS_QPIPE(32, 4, 2, 6), VS_QPIPE(8, 4, 4, 4), VS_QPIPE(48, 4, 4, 4),
 };
 #undef VS_STRIP
 #undef VS_BAND
+#undef VS_QUAD
+#undef VS_QPIPE
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 }  // namespace
@@ -714,34 +1115,45 @@ int tile_shape_count() { return kNumShapes; }
 
 TileShape tile_shape(int i) {
     const ShapeEntry& e = kShapes[i];
-    return {e.rows, e.kind == SHAPE_STRIP ? kStripCommit : 0, e.warps, e.kind};
+    return {e.rows, e.kind == SHAPE_STRIP ? kStripCommit : (e.kind == SHAPE_QUAD ? kQuadCommit : 0), e.warps,
+            e.kind};
 }
 
 size_t shape_smem_bytes(int shape, int max_pitch) {
-    if (shape < 0 || shape >= kNumShapes || kShapes[shape].kind != SHAPE_BAND) return 0;
-    return band_smem_bytes(kShapes[shape].rows, max_pitch);
+    if (shape < 0 || shape >= kNumShapes) return 0;
+    const ShapeEntry& e = kShapes[shape];
+    if (e.kind == SHAPE_QUAD) return (size_t)e.warps * quad_warp_smem(e.stages);
+    if (e.kind != SHAPE_BAND) return 0;
+    return band_smem_bytes(e.rows, max_pitch);
 }
 
 cudaError_t prepare_shape(int shape, int max_pitch) {
     const size_t bytes = shape_smem_bytes(shape, max_pitch);
     if (bytes == 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(kShapes[shape].plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && kShapes[shape].wall)
         e = cudaFuncSetAttribute(kShapes[shape].wall, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess && kShapes[shape].fast)
+        e = cudaFuncSetAttribute(kShapes[shape].fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return e;
 }
 
-cudaError_t launch_step(int shape, bool wall, const TubeDev* tubes, const Tile* tiles, int ntiles,
+bool shape_has_fast(int shape) { return shape >= 0 && shape < kNumShapes && kShapes[shape].fast != nullptr; }
+
+cudaError_t launch_step(int shape, bool wall, bool fast, const TubeDev* tubes, const Tile* tiles, int ntiles,
                         RunState* rs, int local, cudaStream_t stream, int max_pitch) {
     if (shape < 0 || shape >= kNumShapes) return cudaErrorInvalidValue;
     if (ntiles <= 0) return cudaSuccess;
     const ShapeEntry& e = kShapes[shape];
-    const StepFn fn = wall ? e.wall : e.plain;
+    if (fast && wall) return cudaErrorInvalidValue;
+    const StepFn fn = fast ? e.fast : (wall ? e.wall : e.plain);
+    if (!fn) return cudaErrorInvalidValue;
     if (e.kind == SHAPE_BAND) {
         fn<<<ntiles, kBandThreads, band_smem_bytes(e.rows, max_pitch), stream>>>(tubes, tiles, ntiles, rs, local);
     } else {
         const int wpb = e.warps;
-        fn<<<(ntiles + wpb - 1) / wpb, wpb * 32, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+        const size_t smem = e.kind == SHAPE_QUAD ? (size_t)wpb * quad_warp_smem(e.stages) : 0;
+        fn<<<(ntiles + wpb - 1) / wpb, wpb * 32, smem, stream>>>(tubes, tiles, ntiles, rs, local);
     }
     return cudaGetLastError();
 }

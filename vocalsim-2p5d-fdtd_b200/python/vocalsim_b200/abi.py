@@ -69,7 +69,8 @@ class VsParams(C.Structure):
         ("listener_x", C.c_int32),
         ("listener_y", C.c_int32),
         ("tmm_f64", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("fast_math", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
     def copy(self) -> "VsParams":
