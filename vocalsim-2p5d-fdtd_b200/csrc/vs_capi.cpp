@@ -271,6 +271,74 @@ void ensure_graph(vs_batch* b) {
     b->graph_shape = b->shape;
 }
 
+// fast_math descriptors of one tube: every interior cell gets the index of its
+// (code, right type, top type) neighbourhood, and the two tables hold the
+// velocity and pressure factors of each neighbourhood (FDTDSolver.cu:652-801
+// with every beta 0 or 1), computed in double and rounded once:
+//   rden = 1 / (mB + mS); al = mB rden; zo = mS zinv n x_out Nout rden;
+//   zi = mS zinv n x_in Nin rden; ce = ew mS rden; g = 1 / (1 + sigma_c)
+// (g = 0 on the no-pressure cells of a Dirichlet mouth).  Index 0 is plain
+// air.  Ring cells keep index 0 (they are never computed).
+constexpr int kMaxDescriptors = 256;
+constexpr size_t kDescTableBytes = 2 * kMaxDescriptors * 4 * sizeof(float);
+
+void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vector<float>& ta,
+                       std::vector<float>& tb) {
+    desc.assign((size_t)g.H * g.pitch, 0);
+    ta.assign(4 * kMaxDescriptors, 0.0f);
+    tb.assign(4 * kMaxDescriptors, 0.0f);
+    std::vector<int> key_of_id;
+    std::vector<int> id_of_key(32 * 16 * 16, -1);
+    auto key = [](int kc, int tr, int tt) { return (kc * 16 + tr) * 16 + tt; };
+    id_of_key[key(VS_CELL_AIR, VS_CELL_AIR, VS_CELL_AIR)] = 0;
+    key_of_id.push_back(key(VS_CELL_AIR, VS_CELL_AIR, VS_CELL_AIR));
+    auto code_at = [&](int r, int c) { return (int)g.code[(size_t)r * g.pitch + c]; };
+    for (int r = 1; r <= g.H - 2; ++r)
+        for (int c = 1; c <= g.W - 2; ++c) {
+            const int k = key(code_at(r, c) & 0x1f, code_at(r, c + 1) & CODE_TYPE_MASK,
+                              code_at(r - 1, c) & CODE_TYPE_MASK);
+            if (id_of_key[k] < 0) {
+                if ((int)key_of_id.size() >= kMaxDescriptors)
+                    throw VsFailure{VS_ERR_UNSUPPORTED, "fast_math: more than 256 distinct cell neighbourhoods"};
+                id_of_key[k] = (int)key_of_id.size();
+                key_of_id.push_back(k);
+            }
+            desc[(size_t)r * g.pitch + c] = (uint8_t)id_of_key[k];
+        }
+    for (size_t id = 0; id < key_of_id.size(); ++id) {
+        const int k = key_of_id[id];
+        const int kc = k / 256, tr = (k / 16) % 16, tt = k % 16;
+        const int tc = kc & CODE_TYPE_MASK;
+        const bool zbit = (kc & CODE_ZINV_BIT) != 0;
+        const double zinv = zbit ? (double)g.zinv_val : 0.0;
+        const bool bc = g.beta[tc] != 0.0f, br = g.beta[tr] != 0.0f, bt = g.beta[tt] != 0.0f;
+        const bool ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
+        // one direction: neighbour type tn (beta bn, excitation en), other neighbour's beta bo
+        auto dir = [&](int tn, bool bn, bool en, bool bo, double dc, double dn, double* al, double* zo, double* zi,
+                       double* ce) {
+            const bool mB = bc && bn;
+            const double mS = std::max((double)g.sigma[tc], (double)g.sigma[tn]);
+            const double rden = 1.0 / ((mB ? 1.0 : 0.0) + mS);
+            const double n = (ec || en) ? 0.0 : 1.0;
+            const double nout = bo ? 1.0 : (double)0.707106f;
+            *al = mB ? rden : 0.0;
+            *zo = (bc && !bn) ? mS * zinv * n * nout * rden : 0.0;
+            *zi = (bn && !bc) ? mS * zinv * n * rden : 0.0;
+            *ce = ((ec ? dc : 0.0) + (en ? dn : 0.0)) * mS * rden;
+        };
+        double alx, zox, zix, cex, aly, zoy, ziy, cey;
+        dir(tr, br, er, bt, g.dir[2], g.dir[0], &alx, &zox, &zix, &cex);
+        dir(tt, bt, et, br, g.dir[3], g.dir[1], &aly, &zoy, &ziy, &cey);
+        if (cey != 0.0) throw VsFailure{VS_ERR_UNSUPPORTED, "fast_math: source weight on the y velocity"};
+        double gp = 1.0 / (1.0 + (double)g.sigma[tc]);
+        if (g.dirichlet && tc == VS_CELL_NOPRESSURE) gp = 0.0;
+        float* a = &ta[4 * id];
+        float* bq = &tb[4 * id];
+        a[0] = (float)alx; a[1] = (float)aly; a[2] = (float)gp; a[3] = (float)cex;
+        bq[0] = (float)zox; bq[1] = (float)zix; bq[2] = (float)zoy; bq[3] = (float)ziy;
+    }
+}
+
 void upload_static(vs_batch* b) {
     // depth planes and code bytes, padded to the row pitch; written once
     for (size_t i = 0; i < b->grids.size(); ++i) {
@@ -288,6 +356,16 @@ void upload_static(vs_batch* b) {
         up(g.dX, t.dX);
         up(g.dY, t.dY);
         ck(cudaMemcpy((void*)t.code, g.code.data(), g.code.size(), cudaMemcpyHostToDevice), "upload codes");
+        if (b->fast) {
+            std::vector<uint8_t> desc;
+            std::vector<float> ta, tb;
+            build_descriptors(g, desc, ta, tb);
+            ck(cudaMemcpy((void*)t.desc, desc.data(), desc.size(), cudaMemcpyHostToDevice), "upload descriptors");
+            ck(cudaMemcpy((void*)t.desc_a, ta.data(), ta.size() * sizeof(float), cudaMemcpyHostToDevice),
+               "upload descriptor table");
+            ck(cudaMemcpy((void*)t.desc_b, tb.data(), tb.size() * sizeof(float), cudaMemcpyHostToDevice),
+               "upload descriptor table");
+        }
     }
 }
 
@@ -319,6 +397,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
         total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState)) +
                  align_up(2 * sizeof(TmmState64));
+        if (params[0].fast_math) total += align_up((size_t)g.H * g.pitch) + kDescTableBytes;
     }
     total += kGuard;
     b->arena_bytes = total;
@@ -358,6 +437,11 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.dX = (const float*)next(pl);
         t.dY = (const float*)next(pl);
         t.code = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
+        if (b->fast) {
+            t.desc = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
+            t.desc_a = (const float4*)next(kDescTableBytes / 2);
+            t.desc_b = (const float4*)next(kDescTableBytes / 2);
+        }
         t.H = g.H; t.W = g.W; t.pitch = g.pitch;
         t.plane = (int64_t)(pl / sizeof(float));
         t.flags = (g.dirichlet ? TUBE_DIRICHLET : 0) | (g.eigen ? TUBE_EIGEN : 0) |
@@ -367,11 +451,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.K1 = g.K1; t.K2 = g.K2; t.bcoef = g.bcoef; t.zinv = g.zinv_val;
         t.dt = g.dt; t.Mw = g.Mw; t.Bw = g.Bw; t.Kw = g.Kw; t.cpl = g.cpl;
         t.dir0 = g.dir[0]; t.dir1 = g.dir[1]; t.dir2 = g.dir[2]; t.dir3 = g.dir[3];
-        for (int k = 0; k < 13; ++k) {
-            t.sigma[k] = g.sigma[k];
-            t.ginv[k] = (float)(1.0 / (1.0 + (double)g.sigma[k]));
-            t.hinv[k] = g.sigma[k] > 0.0f ? (float)(1.0 / (double)g.sigma[k]) : INFINITY;
-        }
+        for (int k = 0; k < 13; ++k) t.sigma[k] = g.sigma[k];
         t.tmmc = g.tmmc;
         t.tmmd = g.tmmd;
     }

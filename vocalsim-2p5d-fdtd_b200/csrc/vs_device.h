@@ -44,8 +44,13 @@ struct TubeDev {
     float dt, Mw, Bw, Kw, cpl;
     float dir0, dir1, dir2, dir3;
     float sigma[13];
-    float ginv[13];       // 1 / (1 + sigma[t]) and 1 / sigma[t] (infinity for 0), correctly
-    float hinv[13];       // rounded: the reciprocal-form arithmetic (fast_math)
+    // fast_math: per-cell descriptor bytes (same layout as `code`) into two
+    // coefficient tables, desc_a = (alx, aly, g, cex), desc_b = (zox, zix, zoy,
+    // ziy): P' = (P - K1 S / dP) g and
+    // V' = al (V - bcoef (P'n - P'c)) + zo P'c - zi P'n + ce exeV (x and y)
+    const uint8_t* desc;
+    const float4* desc_a;
+    const float4* desc_b;
     TmmConsts tmmc;
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
     // state history for the adjoint's recomputation (strip kernel with

@@ -247,10 +247,9 @@ constexpr uint32_t kBetaMask = 0x9FAu;
 
 __device__ __forceinline__ bool beta_bit(int t) { return (kBetaMask >> t) & 1u; }
 
-template <bool FAST = false>
 __device__ __forceinline__ float velocity_dir(bool bc, bool bn, bool bo, bool ec, bool en, float dirc, float dirn,
                                               float v0, float pc, float pn, float exeV, float mS, float zinv,
-                                              float bco, float rden = 0.0f) {
+                                              float bco) {
     const bool mB = bc && bn;
     float v = mB ? fsub(v0, fmul(bco, fsub(pn, pc))) : 0.0f;
     if (ec || en) v = fadd(v, fmul(fmul(exeV, fadd(fmul((float)ec, dirc), fmul((float)en, dirn))), mS));
@@ -260,7 +259,6 @@ __device__ __forceinline__ float velocity_dir(bool bc, bool bn, bool bo, bool ec
         const float vb = bc ? fmul(pc, bo ? 1.0f : 0.707106f) : -pn;
         v = fadd(v, fmul(mS, fmul(vb, zinv)));
     }
-    if constexpr (FAST) return fmul(v, rden);     // rden = 1 / (mB + mS), correctly rounded
     return fdiv_z(v, fadd(mB ? 1.0f : 0.0f, mS));
 }
 
@@ -274,28 +272,6 @@ __device__ __forceinline__ VelocityOut velocity_generic(
     const float zinv = (kc & CODE_ZINV_BIT) ? zval : 0.0f;
     return {velocity_dir(bc, br, bt, ec, er, dir2, dir0, vx0, pc, pr, exeV, fmaxf(sc, sig[tr]), zinv, bco),
             velocity_dir(bc, bt, br, ec, et, dir3, dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco)};
-}
-
-// The same update in the reciprocal form (fast_math): the denominators
-// mB + mS come from the tube's tables of 1 / (1 + sigma) (ginv) and
-// 1 / sigma (hinv): 1 / (1 + max(s1, s2)) = min(ginv), 1 / max(s1, s2) = min(hinv).
-__device__ __forceinline__ VelocityOut velocity_generic_fast(
-        int kc, int kr, int kt, float pc, float pr, float pt, float vx0, float vy0, float exeV,
-        const TubeDev* __restrict__ T, float bco) {
-    const float* __restrict__ sig = T->sigma;
-    const float* __restrict__ gi = T->ginv;
-    const float* __restrict__ hi = T->hinv;
-    const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
-    const bool bc = beta_bit(tc), br = beta_bit(tr), bt = beta_bit(tt);
-    const bool ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
-    const float sc = sig[tc];
-    const float zinv = (kc & CODE_ZINV_BIT) ? T->zinv : 0.0f;
-    const float rx = (bc && br) ? fminf(gi[tc], gi[tr]) : fminf(hi[tc], hi[tr]);
-    const float ry = (bc && bt) ? fminf(gi[tc], gi[tt]) : fminf(hi[tc], hi[tt]);
-    return {velocity_dir<true>(bc, br, bt, ec, er, T->dir2, T->dir0, vx0, pc, pr, exeV, fmaxf(sc, sig[tr]), zinv, bco,
-                               rx),
-            velocity_dir<true>(bc, bt, br, ec, et, T->dir3, T->dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco,
-                               ry)};
 }
 
 // Approximate reciprocal (PTX rcp.approx.f32, at most 1 ulp from 1/x).
@@ -629,7 +605,8 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
     const float* __restrict__ dPp = T->dP;
     const float* __restrict__ dXp = dPp + pl;
     const float* __restrict__ dYp = dPp + 2 * pl;
-    const uint8_t* __restrict__ code = T->code;
+    // reference arithmetic: cell codes; fast_math: per-cell descriptors
+    const uint8_t* __restrict__ code = FAST ? T->desc : T->code;
     const float* __restrict__ sig = T->sigma;
     const float K1 = T->K1, bco = T->bcoef;
     const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
@@ -782,17 +759,23 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
         const bool pgen = (pmask >> j) & 1;
         const unsigned cm = r >= 1 ? calc_m : 0u;
         float pn[4];
+        // fast_math: rows with any non-air cell read the descriptors' coefficients
+        const bool rowd = FAST && (pgen || (j >= 1 && (((vb1 | vgen) >> (j - 1)) & 1)));
+        float4 da[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float uxl = q == 0 ? ux_l : ux_c[q - 1];
             const int tc = code_byte(k_c, q) & CODE_TYPE_MASK;
             if constexpr (FAST) {
-                // (P dP - K1 S) / ((1 + s) dP) = (P - K1 S / dP) / (1 + s)
+                // (P dP - K1 S) / ((1 + s) dP) = (P - K1 S / dP) g,  g = 1 / (1 + s)
+                // (0 on the no-pressure cells of a Dirichlet mouth)
                 const float ks = fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(uy_c[q], uy_n[q])));
                 float v = __fmaf_rn(-ks, rcp_approx(dp_c[q]), p_c[q]);
-                if (pgen && tc != VS_CELL_AIR) v = fmul(v, T->ginv[tc]);
+                if (rowd) {
+                    da[q] = __ldg(T->desc_a + code_byte(k_c, q));
+                    v = fmul(v, da[q].z);
+                }
                 pn[q] = ((cm >> q) & 1u) ? v : 0.0f;
-                if (pgen && dirichlet && tc == VS_CELL_NOPRESSURE) pn[q] = 0.0f;
             } else {
                 const float num =
                     fsub(fmul(p_c[q], dp_c[q]), fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(uy_c[q], uy_n[q]))));
@@ -821,7 +804,28 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
                 rs->trace[(int64_t)it.tube * rs->trace_stride + (n - rs->run_start)] = pv;
             }
             float vx[4], vy[4];
-            if ((vgen >> jv) & 1) {
+            if constexpr (FAST) {
+                // V' = al (V - bco (P'n - P'c)) + zo P'c - zi P'n + ce exeV
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float pr = q < 3 ? pn[q + 1] : p_r3;
+                    vx[q] = fsub(vx_c[q], fmul(bco, fsub(pr, pn[q])));
+                    vy[q] = fsub(vy_c[q], fmul(bco, fsub(p_above[q], pn[q])));
+                    if (rowd) {
+                        vx[q] = fmul(vx[q], da[q].x);
+                        vy[q] = fmul(vy[q], da[q].y);
+                    }
+                }
+                if ((vgen >> jv) & 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float pr = q < 3 ? pn[q + 1] : p_r3;
+                        const float4 db = __ldg(T->desc_b + code_byte(k_c, q));
+                        vx[q] = __fmaf_rn(da[q].w, exeV, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn[q], vx[q])));
+                        vy[q] = __fmaf_rn(-db.w, p_above[q], __fmaf_rn(db.z, pn[q], vy[q]));
+                    }
+                }
+            } else if ((vgen >> jv) & 1) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     vx[q] = 0.0f;
@@ -829,14 +833,10 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
                     if ((commit_m >> q) & 1u) {
                         const int kr = q < 3 ? code_byte(k_c, q + 1) : k_r3;
                         const float pr = q < 3 ? pn[q + 1] : p_r3;
-                        VelocityOut v;
-                        if constexpr (FAST)
-                            v = velocity_generic_fast(code_byte(k_c, q), kr, code_byte(k_above, q), pn[q], pr,
-                                                      p_above[q], vx_c[q], vy_c[q], exeV, T, bco);
-                        else
-                            v = velocity_generic(code_byte(k_c, q), kr, code_byte(k_above, q), pn[q], pr, p_above[q],
-                                                 vx_c[q], vy_c[q], exeV, sig, T->zinv, bco, T->dir0, T->dir1,
-                                                 T->dir2, T->dir3);
+                        const VelocityOut v =
+                            velocity_generic(code_byte(k_c, q), kr, code_byte(k_above, q), pn[q], pr, p_above[q],
+                                             vx_c[q], vy_c[q], exeV, sig, T->zinv, bco, T->dir0, T->dir1, T->dir2,
+                                             T->dir3);
                         vx[q] = v.vx;
                         vy[q] = v.vy;
                     }
@@ -852,18 +852,9 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int kr = q < 3 ? code_byte(k_c, q + 1) : k_r3;
-                        const int tcq = code_byte(k_c, q) & CODE_TYPE_MASK;
-                        const int trq = kr & CODE_TYPE_MASK, taq = code_byte(k_above, q) & CODE_TYPE_MASK;
-                        if constexpr (FAST) {
-                            const float* __restrict__ gi = T->ginv;
-                            const float gc = gi[tcq];
-                            vx[q] = fmul(vx[q], fminf(gc, gi[trq]));
-                            vy[q] = fmul(vy[q], fminf(gc, gi[taq]));
-                        } else {
-                            const float sc = sig[tcq];
-                            vx[q] = fdiv_z(vx[q], fadd(1.0f, fmaxf(sc, sig[trq])));
-                            vy[q] = fdiv_z(vy[q], fadd(1.0f, fmaxf(sc, sig[taq])));
-                        }
+                        const float sc = sig[code_byte(k_c, q) & CODE_TYPE_MASK];
+                        vx[q] = fdiv_z(vx[q], fadd(1.0f, fmaxf(sc, sig[kr & CODE_TYPE_MASK])));
+                        vy[q] = fdiv_z(vy[q], fadd(1.0f, fmaxf(sc, sig[code_byte(k_above, q) & CODE_TYPE_MASK])));
                     }
                 }
             }
