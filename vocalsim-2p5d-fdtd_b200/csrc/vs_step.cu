@@ -546,10 +546,12 @@ __device__ __forceinline__ void lds4(float (&d)[4], const unsigned char* p) {
     d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
 }
 
+// Store the masked columns of a lane's four; partial masks only occur at a
+// frame's left and right edges, so interior warps issue the vector store only.
 __device__ __forceinline__ void st4(float* p, const float (&v)[4], unsigned mask) {
     if (mask == 0xfu) {
         *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-    } else {
+    } else if (mask != 0u) {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if ((mask >> q) & 1u) p[q] = v[q];
