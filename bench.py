@@ -74,14 +74,19 @@ def hbm_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(cells: int):
-    """DRAM bytes (read + write) per step-kernel launch from the committed ncu summary, when it
-    was captured on this same workload (same interior cell count); else None."""
-    f = REPO / "profiles" / "strip_kernel_batch256.json"
-    if not f.exists():
-        return None
-    d = json.loads(f.read_text())
-    return int(d["dram_bytes_per_launch"]) if int(d.get("interior_cells", -1)) == int(cells) else None
+def profiled_traffic(cells: int, shape: int, fast: int):
+    """DRAM bytes (read + write) per step-kernel launch from the committed ncu summary of the
+    same kernel (launch shape and arithmetic) on this same workload (same interior cell
+    count); else None."""
+    for name in ("quad_kernel_fast_batch256.json", "strip_kernel_batch256.json"):
+        f = REPO / "profiles" / name
+        if not f.exists():
+            continue
+        d = json.loads(f.read_text())
+        if (int(d.get("interior_cells", -1)) == int(cells) and int(d.get("shape", -1)) == int(shape)
+                and int(d.get("fast_math", 0)) == int(fast)):
+            return int(d["dram_bytes_per_launch"])
+    return None
 
 
 class ClockSampler:
@@ -378,7 +383,7 @@ def run_b200(args, rank, world):
                    "arithmetic": "reciprocal form (fast_math=1)" if fast else "reference rounding (fast_math=0)",
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells),
+                     "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells, tile, fast),
                      "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell-update x {cells} cells per launch / "
                              f"mean launch time {launch_ms * 1e3:.2f} us; peak {peak_kind}"},
         "gpu_launches": args.steps * launches_per_forward,
