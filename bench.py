@@ -261,6 +261,37 @@ def gradient_cost(V, stream, reps: int = 3) -> dict:
             "ratio": round(a / f, 3), "ratio_with_ckpt_forward": round((c + a) / f, 3)}
 
 
+INV_TUBES = 64
+INV_SRATE_MUL = 30
+INV_STEPS = 26460                      # 20 ms at 44.1 kHz x 30
+
+
+def inversion_cost(iters: int) -> dict:
+    """Batched inversion: 64 tubes at fs = 44100 x 30 (ds 0.374 mm), 20 ms per
+    forward, Adam over 44 widths + 44 depths + z_inv per tube against the
+    spectra of other seeded tubes; each iteration = one batched checkpointed
+    forward + one batched adjoint (+ the depth model and loss in torch).
+    Seconds per iteration (median) and the mean spectral error."""
+    from vocalsim_b200.inversion import BatchInversion, synthetic_problem
+
+    ps, gs, targets, seeds = synthetic_problem(INV_TUBES, INV_SRATE_MUL, INV_STEPS)
+    inv = BatchInversion(ps, gs, targets, INV_STEPS, ckpt_every=512, lr=0.02)
+    cells = inv.batch.interior_cells
+    secs, losses = [], []
+    for _ in range(iters):
+        t0 = time.perf_counter()
+        losses.append(inv.step())
+        secs.append(time.perf_counter() - t0)
+    best = float(inv.best.mean())
+    inv.close()
+    return {"workload": f"{INV_TUBES} tubes (stable seeds {seeds[0]}..{seeds[-1]}), fs 44100 x {INV_SRATE_MUL}, "
+                        f"{INV_STEPS} steps, {cells} interior cells, checkpoints every 512",
+            "iterations": iters, "s_per_iteration": round(statistics.median(secs), 3),
+            "spectral_error_initial": round(float(np.nanmean(losses[0])), 4),
+            "spectral_error_best": round(best, 4),
+            "diverged_steps": int(sum(np.isnan(x).sum() for x in losses))}
+
+
 def run_b200(args, rank, world):
     import torch
     import vocalsim_b200 as V
@@ -360,6 +391,9 @@ def run_b200(args, rank, world):
     grad = None
     if not args.no_grad:
         grad = gradient_cost(V, stream)
+    inversion = None
+    if args.inversion_iters > 0 and rank == 0:
+        inversion = inversion_cost(args.inversion_iters)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -394,6 +428,7 @@ def run_b200(args, rank, world):
         "batched_vs_single": round(value / world / single["value"], 2) if single else None,
         "grad_fwd_ratio": grad["ratio"] if grad else None,
         "gradient": grad,
+        "inversion": inversion,
     }
     return line
 
@@ -412,6 +447,8 @@ def main():
     ap.add_argument("--no-single", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--inversion-iters", type=int, default=2,
+                    help="Adam iterations of the 64-tube inversion to time (0 = skip)")
     ap.add_argument("--arith", choices=["fast", "exact"], default="fast",
                     help="fast: reciprocal-form arithmetic (fast_math = 1); exact: the reference's rounding")
     args = ap.parse_args()

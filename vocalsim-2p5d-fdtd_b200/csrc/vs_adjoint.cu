@@ -27,7 +27,10 @@
 //   dL/d zinv  += g_x mS_x n_x (x2 Nout P'_c - x1 Nin P'_right) lamVx'_c + (same in y)
 //
 // The adjoint is evaluated in float with float coefficients (it is not meant
-// to be bit-identical to anything); accumulators are double.
+// to be bit-identical to anything); accumulators are double.  The static
+// coefficients (al, a, b, zc of each direction, 1 + sigma) of every cell come
+// from a per-tube table indexed by the cell's neighbourhood descriptor
+// (adjoint_coefficients, vs_capi.cpp).
 #include <cuda_runtime.h>
 
 #include "vs_device.h"
@@ -35,68 +38,27 @@
 namespace vsb {
 namespace {
 
-__constant__ float a_beta[16] = {0, 1, 0, 1, 1, 1, 1, 1, 1, 0, 0, 1, 0, 0, 0, 0};
-__constant__ float a_airN[4] = {0.0f, 1.0f, 1.0f, 0.707106f};
-__constant__ float a_wallN[4] = {1.0f, 1.0f, 1.0f, 0.0f};
-
-// Coefficients of one velocity component of a cell (see the file comment).
-struct VCoef {
-    float al, a, b;      // V' = al V + a P'_c - b P'_nbr + source
-    float zc_out, zc_in; // dV'/dzinv = zc_out P'_c - zc_in P'_nbr
-};
-
-// dirx = true: Vx of cell with code kc, right neighbour kn, top neighbour kt
-// dirx = false: Vy of cell with code kc, top neighbour kn (= kt), right kr
-__device__ inline VCoef vcoef(bool dirx, int kc, int kr, int kt, float zval, float bco,
-                              const float* __restrict__ sig) {
-    const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
-    const float bc = a_beta[tc], br = a_beta[tr], bt = a_beta[tt];
-    const int lut = (br == 0.0f ? 2 : 0) + (bt == 0.0f ? 1 : 0);
-    const float Nout = a_airN[lut] * bc, Nin = a_wallN[lut] * (1.0f - bc);
-    const int tn = dirx ? tr : tt;
-    const float bn = dirx ? br : bt;
-    const float mB = fminf(bc, bn), mS = fmaxf(sig[tc], sig[tn]);
-    const float bxy = mB != 0.0f ? bco : 0.0f;
-    const int ec = tc == VS_CELL_EXCITATION, en = tn == VS_CELL_EXCITATION;
-    const float nn = (float)((1 - ec) * (1 - en));
-    const float xout = bc * (1.0f - bn), xin = bn * (1.0f - bc);
-    const float z = (kc & CODE_ZINV_BIT) ? zval : 0.0f;
-    const float g = __frcp_rn(mB + mS);
-    VCoef v;
-    v.al = mB * g;
-    v.a = g * (bxy + mS * z * nn * xout * Nout);
-    v.b = g * (bxy + mS * z * nn * xin * Nin);
-    const bool zc = (kc & CODE_ZINV_BIT) != 0;
-    v.zc_out = zc ? g * mS * nn * xout * Nout : 0.0f;
-    v.zc_in = zc ? g * mS * nn * xin * Nin : 0.0f;
-    return v;
-}
-
-// mu of interior cell (r, c): the adjoint of P' (see the file comment).
-__device__ float mu_at(const TubeDev& T, const AdjTube& A, int par, int r, int c, int64_t n) {
-    const float* __restrict__ lam = A.lam[par];
+// mu of interior cell (r, c), the adjoint of P' (see the file comment), and
+// q = mu / D.  The coefficients come from the cell's neighbourhood
+// descriptor (AdjTube::desc / tab): A = (ax, ay, bx, by), B = (alx, aly,
+// 1 + sigma, Dirichlet no-pressure flag); the left cell's bx and the lower
+// cell's by from theirs.
+__device__ __forceinline__ float mu_at(const TubeDev& T, const AdjTube& A, int par, int r, int c, int64_t n,
+                                       float* q) {
     const int pitch = T.pitch;
     const int64_t pl = T.plane;
     const int64_t o = (int64_t)r * pitch + c;
-    const uint8_t* __restrict__ code = T.code;
-    const float* __restrict__ sig = T.sigma;
-    const int kc = code[o];
-    if ((T.flags & TUBE_DIRICHLET) && (kc & CODE_TYPE_MASK) == VS_CELL_NOPRESSURE) return 0.0f;
-    const int kr = code[o + 1], kt = code[o - pitch];
-    const VCoef cx = vcoef(true, kc, kr, kt, T.zinv, T.bcoef, sig);
-    const VCoef cy = vcoef(false, kc, kr, kt, T.zinv, T.bcoef, sig);
-    float mu = lam[o] + cx.a * lam[pl + o] + cy.a * lam[2 * pl + o];
-    if (c - 1 >= 1) {   // the left cell's Vx' depends on this P' as its right neighbour
-        const VCoef cl = vcoef(true, code[o - 1], kc, code[o - 1 - pitch], T.zinv, T.bcoef, sig);
-        mu -= cl.b * lam[pl + o - 1];
-    }
-    if (r + 1 <= T.H - 2) {   // the cell below's Vy' depends on this P' as its top neighbour
-        const VCoef cd = vcoef(false, code[o + pitch], code[o + pitch + 1], kc, T.zinv, T.bcoef, sig);
-        mu -= cd.b * lam[2 * pl + o + pitch];
-    }
+    const float* __restrict__ lam = A.lam[par];
+    const int d = A.desc[o];
+    const float4 ea = __ldg(A.tab + 3 * d), eb = __ldg(A.tab + 3 * d + 1);
+    if (eb.w != 0.0f) { *q = 0.0f; return 0.0f; }    // P' := 0 on a Dirichlet mouth
+    float mu = lam[o] + ea.x * lam[pl + o] + ea.y * lam[2 * pl + o];
+    if (c - 1 >= 1) mu -= __ldg(A.tab + 3 * A.desc[o - 1]).z * lam[pl + o - 1];
+    if (r + 1 <= T.H - 2) mu -= __ldg(A.tab + 3 * A.desc[o + pitch]).w * lam[2 * pl + o + pitch];
     if (r == T.lis_y && c == T.lis_x) mu += A.gtrace[n];
     // the two-mass flow of the step after this one read P' here
     if ((T.flags & TUBE_TMM) && r == T.exc_y && c == T.exc_x) mu += (float)A.lam_tmm[6 + par];
+    *q = mu / (eb.z * T.dP[o]);
     return mu;
 }
 
@@ -244,57 +206,59 @@ adjoint_step_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict
     const int tx = threadIdx.x % kAdjTileW, ty = threadIdx.x / kAdjTileW;
     const float* __restrict__ lam = A.lam[par];
     float* __restrict__ lout = A.lam[par ^ 1];
-    __shared__ float smu[kAdjTileH + 1][kAdjTileW + 1];   // row 0: row r0 - 1; column 32: column c0 + 32
+    // mu and q = mu / D of the tile, the row above (row 0) and the column to the right (column 32)
+    __shared__ float smu[kAdjTileH + 1][kAdjTileW + 1];
+    __shared__ float sq[kAdjTileH + 1][kAdjTileW + 1];
     const int r = r0 + ty, c = c0 + tx;
     const bool in = r <= H - 2 && c <= W - 2;
-    smu[ty + 1][tx] = in ? mu_at(T, A, par, r, c, n) : 0.0f;
+    {
+        float q = 0.0f;
+        smu[ty + 1][tx] = in ? mu_at(T, A, par, r, c, n, &q) : 0.0f;
+        sq[ty + 1][tx] = q;
+    }
     if (threadIdx.x < kAdjTileW) {
         const int rr = r0 - 1, cc = c0 + (int)threadIdx.x;
-        smu[0][threadIdx.x] = (rr >= 1 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n) : 0.0f;
+        float q = 0.0f;
+        smu[0][threadIdx.x] = (rr >= 1 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n, &q) : 0.0f;
+        sq[0][threadIdx.x] = q;
     } else if (threadIdx.x < kAdjTileW + kAdjTileH) {
         const int k = threadIdx.x - kAdjTileW, rr = r0 + k, cc = c0 + kAdjTileW;
-        smu[k + 1][kAdjTileW] = (rr <= H - 2 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n) : 0.0f;
+        float q = 0.0f;
+        smu[k + 1][kAdjTileW] = (rr <= H - 2 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n, &q) : 0.0f;
+        sq[k + 1][kAdjTileW] = q;
     }
     __syncthreads();
     if (in) {
         const int64_t pl = T.plane;
         const int64_t o = (int64_t)r * pitch + c;
-        const uint8_t* __restrict__ code = T.code;
-        const float* __restrict__ sig = T.sigma;
         const float* __restrict__ dP = T.dP;
         const float* __restrict__ dX = T.dP + pl;
         const float* __restrict__ dY = T.dP + 2 * pl;
         const float K1 = T.K1;
-        const int kc = code[o], kr = code[o + 1], kt = code[o - pitch];
-        const float muc = smu[ty + 1][tx], mur = smu[ty + 1][tx + 1], mut = smu[ty][tx];
-        const float Dc = (1.0f + sig[kc & CODE_TYPE_MASK]) * dP[o];
-        const float qc = muc / Dc;
-        // ring cells and no-pressure cells of a Dirichlet mouth have mu = 0
-        const float qr = mur != 0.0f ? mur / ((1.0f + sig[kr & CODE_TYPE_MASK]) * dP[o + 1]) : 0.0f;
-        const float qt = mut != 0.0f ? mut / ((1.0f + sig[kt & CODE_TYPE_MASK]) * dP[o - pitch]) : 0.0f;
+        const int d = A.desc[o];
+        const float4 eb = __ldg(A.tab + 3 * d + 1);
+        const float muc = smu[ty + 1][tx];
+        // ring cells and no-pressure cells of a Dirichlet mouth have mu = q = 0
+        const float qc = sq[ty + 1][tx], qr = sq[ty + 1][tx + 1], qt = sq[ty][tx];
         const float lamU = K1 * (qr - qc);
         const float lamW = K1 * (qt - qc);
-        const VCoef cx = vcoef(true, kc, kr, kt, T.zinv, T.bcoef, sig);
-        const VCoef cy = vcoef(false, kc, kr, kt, T.zinv, T.bcoef, sig);
         const float lvx1 = lam[pl + o], lvy1 = lam[2 * pl + o];
-        lout[o] = qc * dP[o];
-        lout[pl + o] = cx.al * lvx1 + dX[o] * lamU;
-        lout[2 * pl + o] = cy.al * lvy1 + dY[o] * lamW;
+        const float dpc = dP[o], dxc = dX[o], dyc = dY[o];
+        lout[o] = qc * dpc;
+        lout[pl + o] = eb.x * lvx1 + dxc * lamU;
+        lout[2 * pl + o] = eb.y * lvy1 + dyc * lamW;
         // state before the step (slot) and P' after it (slot + 1)
         const float* __restrict__ s0 = T.hist + slot * 3 * pl;
         const float* __restrict__ s1 = s0 + 3 * pl;
         const float vx = s0[pl + o], vy = s0[2 * pl + o];
-        const float S =
-            (vx * dX[o] - s0[pl + o - 1] * dX[o - 1]) + (vy * dY[o] - s0[2 * pl + o + pitch] * dY[o + pitch]);
-        const float sc = sig[kc & CODE_TYPE_MASK];
-        if (muc != 0.0f)
-            A.gP[o] += (double)muc * (double)K1 * (double)S / ((1.0 + (double)sc) * (double)dP[o] * (double)dP[o]);
+        const float S = (vx * dxc - s0[pl + o - 1] * dX[o - 1]) + (vy * dyc - s0[2 * pl + o + pitch] * dY[o + pitch]);
+        if (muc != 0.0f) A.gP[o] += (double)qc * (double)K1 * (double)S / (double)dpc;
         A.gX[o] += (double)vx * (double)lamU;
         A.gY[o] += (double)vy * (double)lamW;
-        if (kc & CODE_ZINV_BIT) {
+        if (T.code[o] & CODE_ZINV_BIT) {
+            const float4 ez = __ldg(A.tab + 3 * d + 2);
             const float pc = s1[o], pr = s1[o + 1], pt = s1[o - pitch];
-            A.gZ[o] += (double)(cx.zc_out * pc - cx.zc_in * pr) * (double)lvx1 +
-                       (double)(cy.zc_out * pc - cy.zc_in * pt) * (double)lvy1;
+            A.gZ[o] += (double)(ez.x * pc - ez.y * pr) * (double)lvx1 + (double)(ez.z * pc - ez.w * pt) * (double)lvy1;
         }
     }
 }

@@ -339,9 +339,10 @@ void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vecto
     }
 }
 
-void upload_static(vs_batch* b) {
-    // depth planes and code bytes, padded to the row pitch; written once
-    for (size_t i = 0; i < b->grids.size(); ++i) {
+// Depth planes, code bytes (and fast_math descriptors) of tube i, padded to
+// the row pitch.
+void upload_static_tube(vs_batch* b, size_t i) {
+    {
         const TubeGrid& g = b->grids[i];
         const TubeDev& t = b->h_tubes[i];
         const size_t pl = (size_t)g.H * g.pitch;
@@ -367,6 +368,10 @@ void upload_static(vs_batch* b) {
                "upload descriptor table");
         }
     }
+}
+
+void upload_static(vs_batch* b) {
+    for (size_t i = 0; i < b->grids.size(); ++i) upload_static_tube(b, i);
 }
 
 void reset_state(vs_batch* b) {
@@ -611,6 +616,75 @@ void excitation_list(const TubeGrid& g, int64_t plane, std::vector<int32_t>& off
         }
 }
 
+// Adjoint coefficients of one velocity component (the transposed forward
+// update, FDTDEngineCPU.cpp:364-410 with calculateSolverCoefficients,
+// FDTDSolver.cu:652-801): V' = al V + a P'_c - b P'_nbr + source, and
+// dV'/dzinv = zc_out P'_c - zc_in P'_nbr.  dirx: Vx of a cell with code kc,
+// right neighbour kr, top neighbour kt; else Vy (neighbour = the top cell).
+struct AdjCoef {
+    float al, a, b, zc_out, zc_in;
+};
+
+AdjCoef adjoint_direction(const TubeGrid& g, bool dirx, int kc, int kr, int kt) {
+    static const float air_n[4] = {0.0f, 1.0f, 1.0f, 0.707106f};    // DeviceSymbols.cu:20-21
+    static const float wall_n[4] = {1.0f, 1.0f, 1.0f, 0.0f};
+    const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
+    const float bc = g.beta[tc], br = g.beta[tr], bt = g.beta[tt];
+    const int lut = (br == 0.0f ? 2 : 0) + (bt == 0.0f ? 1 : 0);
+    const float nout = air_n[lut] * bc, nin = wall_n[lut] * (1.0f - bc);
+    const int tn = dirx ? tr : tt;
+    const float bn = dirx ? br : bt;
+    const float mB = std::min(bc, bn), mS = std::max(g.sigma[tc], g.sigma[tn]);
+    const float bxy = mB != 0.0f ? g.bcoef : 0.0f;
+    const int ec = tc == VS_CELL_EXCITATION, en = tn == VS_CELL_EXCITATION;
+    const float nn = (float)((1 - ec) * (1 - en));
+    const float xout = bc * (1.0f - bn), xin = bn * (1.0f - bc);
+    const bool zc = (kc & CODE_ZINV_BIT) != 0;
+    const float z = zc ? g.zinv_val : 0.0f;
+    const float gi = 1.0f / (mB + mS);
+    AdjCoef v;
+    v.al = mB * gi;
+    v.a = gi * (bxy + mS * z * nn * xout * nout);
+    v.b = gi * (bxy + mS * z * nn * xin * nin);
+    v.zc_out = zc ? gi * mS * nn * xout * nout : 0.0f;
+    v.zc_in = zc ? gi * mS * nn * xin * nin : 0.0f;
+    return v;
+}
+
+// Neighbourhood descriptors of a tube's interior cells, (code, right type,
+// top type), and the adjoint coefficient table (three float4 each, see
+// AdjTube); at most kMaxDescriptors distinct neighbourhoods.
+void adjoint_coefficients(const TubeGrid& g, std::vector<uint8_t>& desc, std::vector<float>& tab) {
+    desc.assign((size_t)g.H * g.pitch, 0);
+    tab.assign(12 * kMaxDescriptors, 0.0f);
+    std::vector<int> key_of_id, id_of_key(32 * 16 * 16, -1);
+    auto code_at = [&](int r, int c) { return (int)g.code[(size_t)r * g.pitch + c]; };
+    for (int r = 1; r <= g.H - 2; ++r)
+        for (int c = 1; c <= g.W - 2; ++c) {
+            const int k = ((code_at(r, c) & 0x1f) * 16 + (code_at(r, c + 1) & CODE_TYPE_MASK)) * 16 +
+                          (code_at(r - 1, c) & CODE_TYPE_MASK);
+            if (id_of_key[k] < 0) {
+                if ((int)key_of_id.size() >= kMaxDescriptors)
+                    throw VsFailure{VS_ERR_UNSUPPORTED, "adjoint: more than 256 distinct cell neighbourhoods"};
+                id_of_key[k] = (int)key_of_id.size();
+                key_of_id.push_back(k);
+            }
+            desc[(size_t)r * g.pitch + c] = (uint8_t)id_of_key[k];
+        }
+    for (size_t id = 0; id < key_of_id.size(); ++id) {
+        const int k = key_of_id[id];
+        const int kc = k / 256, tr = (k / 16) % 16, tt = k % 16;
+        const AdjCoef x = adjoint_direction(g, true, kc, tr, tt);
+        const AdjCoef y = adjoint_direction(g, false, kc, tr, tt);
+        const int tc = kc & CODE_TYPE_MASK;
+        float* e = &tab[12 * id];
+        e[0] = x.a; e[1] = y.a; e[2] = x.b; e[3] = y.b;
+        e[4] = x.al; e[5] = y.al; e[6] = 1.0f + g.sigma[tc];
+        e[7] = (g.dirichlet && tc == VS_CELL_NOPRESSURE) ? 1.0f : 0.0f;
+        e[8] = x.zc_out; e[9] = x.zc_in; e[10] = y.zc_out; e[11] = y.zc_in;
+    }
+}
+
 void capture(vs_batch* b, cudaGraphExec_t* out, const char* what, const std::function<cudaError_t(int)>& launch,
              int count) {
     if (*out) { cudaGraphExecDestroy(*out); *out = nullptr; }
@@ -665,13 +739,17 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     }
     ck(cudaMemcpyAsync(b->d_gtrace, gtrace, (size_t)n * steps * sizeof(float), cudaMemcpyHostToDevice, b->stream),
        "upload trace gradient");
-    // excitation lists
+    // excitation lists, neighbourhood descriptors and coefficient tables
     std::vector<std::vector<int32_t>> eoff(n);
     std::vector<std::vector<float>> ecoef(n);
+    std::vector<std::vector<uint8_t>> adesc(n);
+    std::vector<std::vector<float>> atab(n);
     size_t exc_total = 0;
     for (int i = 0; i < n; ++i) {
         excitation_list(b->grids[i], b->h_tubes[i].plane, eoff[i], ecoef[i]);
-        exc_total += align_up(eoff[i].size() * sizeof(int32_t)) + align_up(ecoef[i].size() * sizeof(float));
+        adjoint_coefficients(b->grids[i], adesc[i], atab[i]);
+        exc_total += align_up(eoff[i].size() * sizeof(int32_t)) + align_up(ecoef[i].size() * sizeof(float)) +
+                     align_up(adesc[i].size()) + align_up(atab[i].size() * sizeof(float));
     }
     if (exc_total > b->exc_bytes) {
         if (b->d_exc) { cudaFree(b->d_exc); b->d_exc = nullptr; b->exc_bytes = 0; }
@@ -712,6 +790,17 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
             ck(cudaMemcpyAsync(d_coef, ecoef[i].data(), nb * sizeof(float), cudaMemcpyHostToDevice, b->stream),
                "upload excitation coefficients");
         }
+        uint8_t* d_desc = reinterpret_cast<uint8_t*>(b->d_exc + eo);
+        eo += align_up(adesc[i].size());
+        float* d_tab = reinterpret_cast<float*>(b->d_exc + eo);
+        eo += align_up(atab[i].size() * sizeof(float));
+        ck(cudaMemcpyAsync(d_desc, adesc[i].data(), adesc[i].size(), cudaMemcpyHostToDevice, b->stream),
+           "upload adjoint descriptors");
+        ck(cudaMemcpyAsync(d_tab, atab[i].data(), atab[i].size() * sizeof(float), cudaMemcpyHostToDevice,
+                           b->stream),
+           "upload adjoint coefficient table");
+        adj[i].desc = d_desc;
+        adj[i].tab = reinterpret_cast<const float4*>(d_tab);
         adj[i].exc_off = d_off;
         adj[i].exc_coef = d_coef;
         adj[i].n_exc = (int32_t)nb;
@@ -820,7 +909,7 @@ void set_maps(vs_batch* b, int i, const float* dP, const float* dX, const float*
     if (!(zinv >= 0.0f) || !std::isfinite(zinv)) throw VsFailure{VS_ERR_INVALID_ARG, "z_inv must be finite and >= 0"};
     g.zinv_val = zinv;
     b->h_tubes[i].zinv = zinv;
-    upload_static(b);
+    upload_static_tube(b, (size_t)i);
     ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev), cudaMemcpyHostToDevice),
        "upload tube descriptors");
     b->ck_steps = 0;    // checkpoints no longer match the maps

@@ -197,6 +197,11 @@ struct AdjTube {
     const float* exc_coef;
     int32_t n_exc;
     int32_t tiles;        // 32 x 8 cell tiles of the interior
+    // per-cell neighbourhood descriptors (H x pitch bytes) into a table of
+    // three float4 per descriptor: (ax, ay, bx, by), (alx, aly, 1 + sigma,
+    // Dirichlet no-pressure flag), (zc_out x, zc_in x, zc_out y, zc_in y)
+    const uint8_t* desc;
+    const float4* tab;
 };
 
 // Segment of the reverse sweep, in device memory so that one captured graph

@@ -84,9 +84,6 @@ class SectionDepthModel:
         self.pivot = d["tube_mid_y"] * self.W + d["tube_end_x"]
         self._x = self._pack(writes_x)
         self._y = self._pack(writes_y)
-        self.clamp_p = torch.from_numpy(self.nominal["depth_p"] <= MIN_DEPTH)
-        self.clamp_x = torch.from_numpy(self.nominal["depth_x"] <= MIN_DEPTH)
-        self.clamp_y = torch.from_numpy(self.nominal["depth_y"] <= MIN_DEPTH)
 
     def _pack(self, writes):
         idx = np.array(list(writes.keys()), np.int64)
@@ -104,7 +101,10 @@ class SectionDepthModel:
         a = spec["a0"] * (w[spec["seg"]] / self.width0[spec["seg"]])
         b = dep[spec["seg"]] / 2.0
         y = spec["dist"] * self.ds
-        v = 2.0 * b * torch.sqrt(torch.clamp(1.0 - (y * y) / (a * a), min=0.0))
+        arg = 1.0 - (y * y) / (a * a)
+        pos = arg > 0
+        # sqrt of the positive part; the masked branch keeps the derivative finite at 0
+        v = torch.where(pos, 2.0 * b * torch.sqrt(torch.where(pos, arg, torch.ones_like(arg))), torch.zeros_like(arg))
         v = torch.where(spec["zero"], torch.zeros_like(v), v)
         out = torch.full((self.H * self.W,), OPEN_SPACE_DEPTH, dtype=torch.float64)
         return out.index_put((spec["idx"],), v)
@@ -128,11 +128,9 @@ class SectionDepthModel:
         xl = torch.cat([pxs.expand(H, 1), xs[:, :-1]], dim=1)
         yb = torch.cat([ys[1:, :], pys.expand(1, W)], dim=0)
         dp = 0.25 * (xs + ys + xl + yb)
-        lo = torch.tensor(MIN_DEPTH, dtype=torch.float64)
-        dp = torch.where(self.clamp_p, lo, dp)
-        xs = torch.where(self.clamp_x, lo, xs)
-        ys = torch.where(self.clamp_y, lo, ys)
-        return dp, xs, ys
+        # depths below the (float) minimum are raised to it (TubeDepth.cu:90)
+        lo = torch.tensor(float(np.float32(MIN_DEPTH)), dtype=torch.float64)
+        return torch.where(dp < lo, lo, dp), torch.where(xs < lo, lo, xs), torch.where(ys < lo, lo, ys)
 
 
 class TubeTrace(torch.autograd.Function):

@@ -9,6 +9,8 @@ format (TubeGeometry.cu:83-88).
                     cosine modes with seeded amplitudes/phases, 0.3, 5) cm^2
   batch_tube        vowel_area shape with a seeded length in [12, 20] cm and a
                     seeded maximum width in [2, 4] cm (3:1 elliptical major axis)
+  batch_target_tube the inversion target of batch tube `seed`: same length and
+                    maximum width, area shape of another seed
 """
 from __future__ import annotations
 
@@ -55,3 +57,12 @@ def batch_tube(seed: int, n: int = N_SECTIONS):
     a = vowel_area(seed, n).astype(np.float64)
     a = a * (ellipse_area_for_width(width) / a.max())
     return np.full(n, length / n, np.float32), a.astype(np.float32), length, width
+
+
+def batch_target_tube(seed: int, n: int = N_SECTIONS):
+    """Target of the batched inversion for batch tube `seed`: the same length and
+    maximum width, the area curve of seed 50 000 + seed."""
+    L, _, length, width = batch_tube(seed, n)
+    a = vowel_area(50_000 + seed, n).astype(np.float64)
+    a = a * (ellipse_area_for_width(width) / a.max())
+    return L, a.astype(np.float32), length, width
