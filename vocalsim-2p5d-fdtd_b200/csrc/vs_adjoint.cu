@@ -38,27 +38,42 @@
 namespace vsb {
 namespace {
 
+// Fields of a tube the reverse step reads, held in registers (the kernel's
+// stores go through other pointers, so nothing here changes during a launch).
+struct AdjView {
+    const float* lam;         // adjoint of the state after the step (read only)
+    const uint8_t* desc;
+    const float4* tab;
+    const float* dP;
+    const float* gtrace;
+    int64_t pl;
+    int pitch, H, lis_y, lis_x, exc_y, exc_x;
+    bool tmm;
+    float pending;            // d/d p1 of the step after this one, at the excitation point
+};
+
 // mu of interior cell (r, c), the adjoint of P' (see the file comment), and
 // q = mu / D.  The coefficients come from the cell's neighbourhood
-// descriptor (AdjTube::desc / tab): A = (ax, ay, bx, by), B = (alx, aly,
-// 1 + sigma, Dirichlet no-pressure flag); the left cell's bx and the lower
-// cell's by from theirs.
-__device__ __forceinline__ float mu_at(const TubeDev& T, const AdjTube& A, int par, int r, int c, int64_t n,
-                                       float* q) {
-    const int pitch = T.pitch;
-    const int64_t pl = T.plane;
-    const int64_t o = (int64_t)r * pitch + c;
-    const float* __restrict__ lam = A.lam[par];
-    const int d = A.desc[o];
-    const float4 ea = __ldg(A.tab + 3 * d), eb = __ldg(A.tab + 3 * d + 1);
+// descriptor: A = (ax, ay, bx, by), B = (alx, aly, 1 + sigma, Dirichlet
+// no-pressure flag); the left cell's bx and the lower cell's by from theirs.
+__device__ __forceinline__ float mu_at(const AdjView& v, int r, int c, int64_t n, float* q) {
+    const int64_t o = (int64_t)r * v.pitch + c;
+    const int d = __ldg(v.desc + o);
+    const int dl = c - 1 >= 1 ? __ldg(v.desc + o - 1) : -1;
+    const int dd = r + 1 <= v.H - 2 ? __ldg(v.desc + o + v.pitch) : -1;
+    const float l0 = __ldg(v.lam + o), lx = __ldg(v.lam + v.pl + o), ly = __ldg(v.lam + 2 * v.pl + o);
+    const float lxl = dl >= 0 ? __ldg(v.lam + v.pl + o - 1) : 0.0f;
+    const float lyd = dd >= 0 ? __ldg(v.lam + 2 * v.pl + o + v.pitch) : 0.0f;
+    const float dpc = __ldg(v.dP + o);
+    const float4 ea = __ldg(v.tab + 3 * d), eb = __ldg(v.tab + 3 * d + 1);
     if (eb.w != 0.0f) { *q = 0.0f; return 0.0f; }    // P' := 0 on a Dirichlet mouth
-    float mu = lam[o] + ea.x * lam[pl + o] + ea.y * lam[2 * pl + o];
-    if (c - 1 >= 1) mu -= __ldg(A.tab + 3 * A.desc[o - 1]).z * lam[pl + o - 1];
-    if (r + 1 <= T.H - 2) mu -= __ldg(A.tab + 3 * A.desc[o + pitch]).w * lam[2 * pl + o + pitch];
-    if (r == T.lis_y && c == T.lis_x) mu += A.gtrace[n];
+    float mu = l0 + ea.x * lx + ea.y * ly;
+    if (dl >= 0) mu -= __ldg(v.tab + 3 * dl).z * lxl;
+    if (dd >= 0) mu -= __ldg(v.tab + 3 * dd).w * lyd;
+    if (r == v.lis_y && c == v.lis_x) mu += __ldg(v.gtrace + n);
     // the two-mass flow of the step after this one read P' here
-    if ((T.flags & TUBE_TMM) && r == T.exc_y && c == T.exc_x) mu += (float)A.lam_tmm[6 + par];
-    *q = mu / (eb.z * T.dP[o]);
+    if (v.tmm && r == v.exc_y && c == v.exc_x) mu += v.pending;
+    *q = mu / (eb.z * dpc);
     return mu;
 }
 
@@ -185,7 +200,7 @@ __device__ void tmm_reverse(const TubeDev& T, const AdjTube& A, const float* __r
 // plus the row above and the column to the right into shared memory, then
 // lambda of the state before the step and the gradient terms of its cells;
 // the block holding the excitation point also runs the two-mass reverse step.
-__global__ void __launch_bounds__(kAdjTileW * kAdjTileH)
+__global__ void __launch_bounds__(kAdjTileW * kAdjTileH, 3)
 adjoint_step_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
                     const AdjRun* __restrict__ run, int local) {
     const TubeDev& T = tubes[blockIdx.y];
@@ -204,59 +219,89 @@ adjoint_step_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict
     const int tiles_x = (W - 2 + kAdjTileW - 1) / kAdjTileW;
     const int c0 = 1 + (int)(blockIdx.x % tiles_x) * kAdjTileW, r0 = 1 + (int)(blockIdx.x / tiles_x) * kAdjTileH;
     const int tx = threadIdx.x % kAdjTileW, ty = threadIdx.x / kAdjTileW;
-    const float* __restrict__ lam = A.lam[par];
+    AdjView v;
+    v.lam = A.lam[par];
+    v.desc = A.desc;
+    v.tab = A.tab;
+    v.dP = T.dP;
+    v.gtrace = A.gtrace;
+    v.pl = T.plane;
+    v.pitch = pitch; v.H = H;
+    v.lis_y = T.lis_y; v.lis_x = T.lis_x; v.exc_y = T.exc_y; v.exc_x = T.exc_x;
+    v.tmm = (T.flags & TUBE_TMM) != 0;
+    v.pending = v.tmm ? (float)A.lam_tmm[6 + par] : 0.0f;
     float* __restrict__ lout = A.lam[par ^ 1];
+    double* __restrict__ gP = A.gP;
+    double* __restrict__ gX = A.gX;
+    double* __restrict__ gY = A.gY;
+    const int64_t pl = v.pl;
+    const float K1 = T.K1;
+    const float* __restrict__ s0 = T.hist + slot * 3 * pl;   // state before the step
+    const float* __restrict__ s1 = s0 + 3 * pl;              // P' after it
+    const int r = r0 + ty, c = c0 + tx;
+    const bool in = r <= H - 2 && c <= W - 2;
+    const int64_t o = (int64_t)r * pitch + c;
+
+    // loads of this cell's update that do not depend on mu, issued before it
+    float lvx1 = 0.0f, lvy1 = 0.0f, dpc = 1.0f, dxc = 0.0f, dyc = 0.0f, dxl = 0.0f, dyd = 0.0f;
+    float vx = 0.0f, vy = 0.0f, vxl = 0.0f, vyd = 0.0f;
+    double gx0 = 0.0, gy0 = 0.0, gp0 = 0.0;
+    float4 eb = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    int d = 0;
+    if (in) {
+        d = __ldg(v.desc + o);
+        eb = __ldg(v.tab + 3 * d + 1);
+        lvx1 = __ldg(v.lam + pl + o);
+        lvy1 = __ldg(v.lam + 2 * pl + o);
+        dpc = __ldg(T.dP + o);
+        dxc = __ldg(T.dP + pl + o);
+        dyc = __ldg(T.dP + 2 * pl + o);
+        dxl = __ldg(T.dP + pl + o - 1);
+        dyd = __ldg(T.dP + 2 * pl + o + pitch);
+        vx = __ldg(s0 + pl + o);
+        vy = __ldg(s0 + 2 * pl + o);
+        vxl = __ldg(s0 + pl + o - 1);
+        vyd = __ldg(s0 + 2 * pl + o + pitch);
+        gx0 = gX[o];
+        gy0 = gY[o];
+        gp0 = gP[o];
+    }
+
     // mu and q = mu / D of the tile, the row above (row 0) and the column to the right (column 32)
     __shared__ float smu[kAdjTileH + 1][kAdjTileW + 1];
     __shared__ float sq[kAdjTileH + 1][kAdjTileW + 1];
-    const int r = r0 + ty, c = c0 + tx;
-    const bool in = r <= H - 2 && c <= W - 2;
     {
         float q = 0.0f;
-        smu[ty + 1][tx] = in ? mu_at(T, A, par, r, c, n, &q) : 0.0f;
+        smu[ty + 1][tx] = in ? mu_at(v, r, c, n, &q) : 0.0f;
         sq[ty + 1][tx] = q;
     }
     if (threadIdx.x < kAdjTileW) {
         const int rr = r0 - 1, cc = c0 + (int)threadIdx.x;
         float q = 0.0f;
-        smu[0][threadIdx.x] = (rr >= 1 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n, &q) : 0.0f;
+        smu[0][threadIdx.x] = (rr >= 1 && cc <= W - 2) ? mu_at(v, rr, cc, n, &q) : 0.0f;
         sq[0][threadIdx.x] = q;
     } else if (threadIdx.x < kAdjTileW + kAdjTileH) {
         const int k = threadIdx.x - kAdjTileW, rr = r0 + k, cc = c0 + kAdjTileW;
         float q = 0.0f;
-        smu[k + 1][kAdjTileW] = (rr <= H - 2 && cc <= W - 2) ? mu_at(T, A, par, rr, cc, n, &q) : 0.0f;
+        smu[k + 1][kAdjTileW] = (rr <= H - 2 && cc <= W - 2) ? mu_at(v, rr, cc, n, &q) : 0.0f;
         sq[k + 1][kAdjTileW] = q;
     }
     __syncthreads();
     if (in) {
-        const int64_t pl = T.plane;
-        const int64_t o = (int64_t)r * pitch + c;
-        const float* __restrict__ dP = T.dP;
-        const float* __restrict__ dX = T.dP + pl;
-        const float* __restrict__ dY = T.dP + 2 * pl;
-        const float K1 = T.K1;
-        const int d = A.desc[o];
-        const float4 eb = __ldg(A.tab + 3 * d + 1);
         const float muc = smu[ty + 1][tx];
         // ring cells and no-pressure cells of a Dirichlet mouth have mu = q = 0
         const float qc = sq[ty + 1][tx], qr = sq[ty + 1][tx + 1], qt = sq[ty][tx];
         const float lamU = K1 * (qr - qc);
         const float lamW = K1 * (qt - qc);
-        const float lvx1 = lam[pl + o], lvy1 = lam[2 * pl + o];
-        const float dpc = dP[o], dxc = dX[o], dyc = dY[o];
         lout[o] = qc * dpc;
         lout[pl + o] = eb.x * lvx1 + dxc * lamU;
         lout[2 * pl + o] = eb.y * lvy1 + dyc * lamW;
-        // state before the step (slot) and P' after it (slot + 1)
-        const float* __restrict__ s0 = T.hist + slot * 3 * pl;
-        const float* __restrict__ s1 = s0 + 3 * pl;
-        const float vx = s0[pl + o], vy = s0[2 * pl + o];
-        const float S = (vx * dxc - s0[pl + o - 1] * dX[o - 1]) + (vy * dyc - s0[2 * pl + o + pitch] * dY[o + pitch]);
-        if (muc != 0.0f) A.gP[o] += (double)qc * (double)K1 * (double)S / (double)dpc;
-        A.gX[o] += (double)vx * (double)lamU;
-        A.gY[o] += (double)vy * (double)lamW;
+        const float S = (vx * dxc - vxl * dxl) + (vy * dyc - vyd * dyd);
+        if (muc != 0.0f) gP[o] = gp0 + (double)qc * (double)K1 * (double)S / (double)dpc;
+        gX[o] = gx0 + (double)vx * (double)lamU;
+        gY[o] = gy0 + (double)vy * (double)lamW;
         if (T.code[o] & CODE_ZINV_BIT) {
-            const float4 ez = __ldg(A.tab + 3 * d + 2);
+            const float4 ez = __ldg(v.tab + 3 * d + 2);
             const float pc = s1[o], pr = s1[o + 1], pt = s1[o - pitch];
             A.gZ[o] += (double)(ez.x * pc - ez.y * pr) * (double)lvx1 + (double)(ez.z * pc - ez.w * pt) * (double)lvy1;
         }
