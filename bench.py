@@ -83,8 +83,12 @@ def profiled_traffic(cells: int, shape: int, fast: int):
         if not f.exists():
             continue
         d = json.loads(f.read_text())
-        if (int(d.get("interior_cells", -1)) == int(cells) and int(d.get("shape", -1)) == int(shape)
-                and int(d.get("fast_math", 0)) == int(fast)):
+        if int(d.get("interior_cells", -1)) != int(cells) or int(d.get("fast_math", 0)) != int(fast):
+            continue
+        by_shape = d.get("traffic_by_shape", {})
+        if str(shape) in by_shape:
+            return int(by_shape[str(shape)]["dram_bytes_per_launch"])
+        if int(d.get("shape", -1)) == int(shape):
             return int(d["dram_bytes_per_launch"])
     return None
 
