@@ -247,6 +247,18 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
 
 void vs_batch_destroy(vs_batch* b);
 
+/* Formants of listener traces on the device: for each of n_traces traces of
+ * n samples (device, row-major) at sampling rate fs, the first num_formants
+ * spectral peaks as the reference's get_formants_bw computes them
+ * (results/formants_bandwidths.py:5-80: level = 10 log10 |FFT|^2, df =
+ * fs / (n - 1), -3 dB crossings by numpy.interp).  out (device, doubles) =
+ * n_traces x [bandwidth Hz, centre Hz, peak dB] x num_formants, zeros where
+ * fewer peaks exist.  Uses cuFFT (double); allocates its work buffers and
+ * returns after the work on cuda_stream (a cudaStream_t; NULL = default) is
+ * done. */
+int vs_formants(const float* traces, int32_t n_traces, int64_t n, double fs, int32_t num_formants, double* out,
+                void* cuda_stream);
+
 /* ---- gradients: checkpointed forward + reverse-time discrete adjoint -----
  * No counterpart in the reference (it has no differentiation).  The adjoint
  * covers table sources (Gaussian, sine) and the two-mass source (whose flow

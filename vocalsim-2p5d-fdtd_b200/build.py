@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
               f"-I{INCLUDE}", "-Wno-deprecated-gpu-targets"]
 
-SOURCES = ["vs_grid.cpp", "vs_capi.cpp", "vs_step.cu", "vs_noalloc.cu", "vs_adjoint.cu"]
+SOURCES = ["vs_grid.cpp", "vs_capi.cpp", "vs_step.cu", "vs_noalloc.cu", "vs_adjoint.cu", "vs_spectrum.cu"]
 
 
 def nvcc() -> str:
@@ -57,8 +57,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
+        # cuFFT (vs_formants) is linked dynamically from the toolkit next to nvcc
+        cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-ldl", "-lrt",
-               "-lpthread"]
+               "-lpthread", f"-L{cuda_lib}", "-lcufft", "-Xlinker", f"-rpath={cuda_lib}"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

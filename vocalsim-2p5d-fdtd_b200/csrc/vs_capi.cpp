@@ -1049,6 +1049,17 @@ int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* be
     });
 }
 
+int vs_formants(const float* traces, int32_t n_traces, int64_t n, double fs, int32_t num_formants, double* out,
+                void* cuda_stream) {
+    if (!traces || !out || n_traces < 1 || n < 3 || num_formants < 1 || !(fs > 0.0) || n > INT32_MAX)
+        return set_error(VS_ERR_INVALID_ARG, "vs_formants arguments");
+    std::string err;
+    const int st = formants_device(traces, n_traces, n, fs, num_formants, out,
+                                   static_cast<cudaStream_t>(cuda_stream), &err);
+    if (st != VS_OK) return set_error(st, err.c_str());
+    return VS_OK;
+}
+
 int vs_tile_shape_count(void) { return tile_shape_count(); }
 
 int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime_api.h>
 
@@ -228,6 +229,12 @@ cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int nt
 // Copy each tube's state (parity par) into slot 0 of its history (and the
 // two-mass state into slot 0 of tmm_hist).
 cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_cells, int par, cudaStream_t stream);
+
+// Formants of ntr device traces of n samples at sampling rate fs (the
+// reference's get_formants_bw): out (device) = ntr x [bandwidth, centre,
+// level] x nf.  Synchronises `st`; returns a vs_status, err gets the text.
+int formants_device(const float* traces, int ntr, int64_t n, double fs, int nf, double* out, cudaStream_t st,
+                    std::string* err);
 
 // Set the text vs_last_error() returns on this host thread.
 void record_error(const char* msg);
