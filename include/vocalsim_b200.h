@@ -282,6 +282,21 @@ int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float*
 int vs_batch_adjoint(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, float* grad_depth_x,
                      float* grad_depth_y, float* grad_z_inv);
 
+/* Depth maps of every tube from section parameters, computed on the device:
+ * the reference's elliptical depth kernel and post-processing
+ * (TubeDepth.cu:392-490, 642-762) on each tube's nominal rasterisation (the
+ * wall rows stay where the nominal widths put them; a section's width
+ * scales the semi-major axis of its cells, its depth the minor axis).
+ * width_m, depth_m: the tubes' sections concatenated in tube order (m);
+ * z_inv: one value per tube (NULL keeps them).  2.5D 3:1 elliptical tubes
+ * only, fast_math = 0.  Invalidates stored checkpoints. */
+int vs_batch_set_sections(vs_batch* b, const double* width_m, const double* depth_m, const double* z_inv);
+
+/* dL/d width and dL/d depth of every section (host, concatenated like
+ * vs_batch_set_sections), from the map gradients of the last
+ * vs_batch_adjoint run on maps set by vs_batch_set_sections. */
+int vs_batch_section_gradients(vs_batch* b, double* grad_width, double* grad_depth);
+
 /* ---- running without allocating ------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * when they step a tube: a real-time audio host calling from its processing

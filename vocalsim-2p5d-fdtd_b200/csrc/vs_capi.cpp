@@ -100,6 +100,12 @@ struct vs_batch {
     size_t exc_bytes = 0;
     Tile* d_hist_tiles = nullptr;
     int n_hist_tiles = 0;
+    // section depth model (vs_batch_set_sections): per-tube descriptors and buffers
+    std::vector<SectionTube> h_sec;
+    SectionTube* d_sec = nullptr;
+    char* sec_mem = nullptr;
+    int64_t sec_max_cells = 0;
+    bool sec_maps = false;                 // the maps on the device came from set_sections
     cudaGraphExec_t hist_graph = nullptr;  // ck_every history steps
     cudaGraphExec_t adj_graph = nullptr;   // ck_every reverse steps
     int adj_graph_len = 0;
@@ -122,6 +128,9 @@ struct vs_batch {
         if (d_gtrace) cudaFree(d_gtrace);
         if (d_exc) cudaFree(d_exc);
         if (d_hist_tiles) cudaFree(d_hist_tiles);
+        if (d_sec) cudaFree(d_sec);
+        if (sec_mem) cudaFree(sec_mem);
+        d_sec = nullptr; sec_mem = nullptr;
         if (hist_graph) cudaGraphExecDestroy(hist_graph);
         if (adj_graph) cudaGraphExecDestroy(adj_graph);
         ckpt = nullptr; adj_mem = nullptr; d_adj = nullptr; d_adjrun = nullptr; d_gtrace = nullptr;
@@ -896,6 +905,142 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     b->step = steps;
 }
 
+// The depth kernel's writes of one tube, as autograd.SectionDepthModel lists
+// them (TubeDepth.cu:392-490): for each tube column from the first, the air
+// cells from the axis outwards on both sides, then the two wall rows (zero);
+// a later write to a cell replaces an earlier one.
+void section_cells(const TubeGrid& g, std::vector<SectionCell>& cx, std::vector<SectionCell>& cy) {
+    const int H = g.H, W = g.W;
+    cx.assign((size_t)H * W, SectionCell{kSectionUnwritten, 0.0f, 0.0});
+    cy = cx;
+    const double ds = (double)g.dims.ds;
+    const int sx = g.dims.tube_start_x;
+    for (size_t i = 0; i < g.upper.size(); ++i) {
+        const int x = sx + (int)i, u = g.upper[i], lo = g.lower[i], sg = g.colseg[i];
+        const int air = lo - u - 1;
+        const int half = (int)std::ceil(air * 0.5) - 1;
+        const double a0 = (air * ds) / 2.0;
+        for (int cc = half; cc >= 0; --cc) {
+            const int pu = u + (half - cc) + 1, pl = lo - (half - cc) - 1;
+            cx[(size_t)pu * W + x] = SectionCell{sg, (float)cc, a0};
+            cx[(size_t)pl * W + x] = SectionCell{sg, (float)cc, a0};
+            cy[(size_t)pu * W + x] = cc != half ? SectionCell{sg, (float)cc + 0.5f, a0}
+                                                : SectionCell{kSectionZero, 0.0f, a0};
+            cy[(size_t)pl * W + x] = SectionCell{sg, (float)cc - 0.5f, a0};
+        }
+        for (int r : {u, lo}) {
+            cx[(size_t)r * W + x] = SectionCell{kSectionZero, 0.0f, a0};
+            cy[(size_t)r * W + x] = SectionCell{kSectionZero, 0.0f, a0};
+        }
+    }
+}
+
+void section_setup(vs_batch* b) {
+    if (b->d_sec) return;
+    if (b->fast) throw VsFailure{VS_ERR_UNSUPPORTED, "section maps: use fast_math = 0"};
+    const int n = (int)b->grids.size();
+    std::vector<std::vector<SectionCell>> cx(n), cy(n);
+    std::vector<size_t> off(n);
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
+        const vs_params& p = g.src_params;
+        if (p.fdtd_solver_type != 1 || p.cross_sectional_shape != 2 || g.upper.empty())
+            throw VsFailure{VS_ERR_UNSUPPORTED, "section maps cover 2.5D tubes with 3:1 elliptical sections"};
+        section_cells(g, cx[i], cy[i]);
+        const int64_t pv = (int64_t)g.dims.tube_mid_y * g.W + g.dims.tube_end_x;
+        if (cx[i][pv].seg < 0 || cy[i][pv].seg < 0)
+            throw VsFailure{VS_ERR_UNSUPPORTED, "section maps: the pivot cell is not an air cell"};
+        const size_t cells = (size_t)g.H * g.W, ns = g.major_m.size();
+        off[i] = total;
+        total += align_up(2 * cells * sizeof(SectionCell)) + align_up(cells) + align_up(4 * cells * sizeof(double)) +
+                 align_up(5 * ns * sizeof(double)) + align_up(6 * sizeof(double));
+        b->sec_max_cells = std::max<int64_t>(b->sec_max_cells, (int64_t)cells);
+    }
+    ck(cudaMalloc(&b->sec_mem, total), "cudaMalloc(section model)");
+    b->h_sec.assign(n, SectionTube{});
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
+        const size_t cells = (size_t)g.H * g.W, ns = g.major_m.size();
+        char* p = b->sec_mem + off[i];
+        auto next = [&](size_t bytes) { char* q = p; p += align_up(bytes); return q; };
+        SectionTube& t = b->h_sec[i];
+        SectionCell* dcx = reinterpret_cast<SectionCell*>(next(2 * cells * sizeof(SectionCell)));
+        t.cx = dcx;
+        t.cy = dcx + cells;
+        t.clamp = reinterpret_cast<uint8_t*>(next(cells));
+        double* sc = reinterpret_cast<double*>(next(4 * cells * sizeof(double)));
+        t.gxs = sc; t.gys = sc + cells; t.gx = sc + 2 * cells; t.gy = sc + 3 * cells;
+        double* pr = reinterpret_cast<double*>(next(5 * ns * sizeof(double)));
+        t.w0 = pr; t.w = pr + ns; t.d = pr + 2 * ns; t.dw = pr + 3 * ns; t.dd = pr + 4 * ns;
+        t.acc = reinterpret_cast<double*>(next(6 * sizeof(double)));
+        t.ds = (double)g.dims.ds;
+        t.pivot = (int64_t)g.dims.tube_mid_y * g.W + g.dims.tube_end_x;
+        t.H = g.H; t.W = g.W; t.nsec = (int32_t)ns;
+        ck(cudaMemcpy(dcx, cx[i].data(), cells * sizeof(SectionCell), cudaMemcpyHostToDevice), "upload section cells");
+        ck(cudaMemcpy(dcx + cells, cy[i].data(), cells * sizeof(SectionCell), cudaMemcpyHostToDevice),
+           "upload section cells");
+        std::vector<double> w0(g.major_m.begin(), g.major_m.end());
+        ck(cudaMemcpy(const_cast<double*>(t.w0), w0.data(), ns * sizeof(double), cudaMemcpyHostToDevice),
+           "upload nominal widths");
+    }
+    ck(cudaMalloc(&b->d_sec, n * sizeof(SectionTube)), "cudaMalloc(section descriptors)");
+    ck(cudaMemcpy(b->d_sec, b->h_sec.data(), n * sizeof(SectionTube), cudaMemcpyHostToDevice),
+       "upload section descriptors");
+}
+
+void set_sections(vs_batch* b, const double* width, const double* depth, const double* zinv) {
+    section_setup(b);
+    const int n = (int)b->grids.size();
+    size_t k = 0;
+    for (int i = 0; i < n; ++i) {
+        const SectionTube& t = b->h_sec[i];
+        for (int j = 0; j < t.nsec; ++j)
+            if (!(width[k + j] > 0.0) || !(depth[k + j] > 0.0) || !std::isfinite(width[k + j]) ||
+                !std::isfinite(depth[k + j]))
+                throw VsFailure{VS_ERR_INVALID_ARG, "section widths and depths must be finite and > 0"};
+        if (zinv && (!(zinv[i] >= 0.0) || !std::isfinite(zinv[i])))
+            throw VsFailure{VS_ERR_INVALID_ARG, "z_inv must be finite and >= 0"};
+        ck(cudaMemcpyAsync(const_cast<double*>(t.w), width + k, t.nsec * sizeof(double), cudaMemcpyHostToDevice,
+                           b->stream), "upload widths");
+        ck(cudaMemcpyAsync(const_cast<double*>(t.d), depth + k, t.nsec * sizeof(double), cudaMemcpyHostToDevice,
+                           b->stream), "upload depths");
+        k += t.nsec;
+        if (zinv) {
+            b->grids[i].zinv_val = (float)zinv[i];
+            b->h_tubes[i].zinv = (float)zinv[i];
+        }
+    }
+    ck(cudaMemcpyAsync(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice, b->stream),
+       "upload tube descriptors");
+    ck(launch_section_maps(b->d_sec, b->d_tubes, n, b->sec_max_cells, b->stream), "section maps");
+    ck(cudaStreamSynchronize(b->stream), "section maps sync");
+    b->sec_maps = true;
+    b->ck_steps = 0;    // checkpoints no longer match the maps
+}
+
+void section_gradients(vs_batch* b, double* dwidth, double* ddepth) {
+    if (!b->d_sec || !b->sec_maps || !b->d_adj || b->ck_steps <= 0)
+        throw VsFailure{VS_ERR_INVALID_ARG,
+                        "vs_batch_section_gradients needs vs_batch_set_sections, vs_batch_forward_ckpt and "
+                        "vs_batch_adjoint first"};
+    const int n = (int)b->grids.size();
+    for (int i = 0; i < n; ++i) {
+        const SectionTube& t = b->h_sec[i];
+        ck(cudaMemsetAsync(t.dw, 0, 2 * t.nsec * sizeof(double), b->stream), "zero section gradients");
+        ck(cudaMemsetAsync(t.acc, 0, 6 * sizeof(double), b->stream), "zero accumulators");
+    }
+    ck(launch_section_vjp(b->d_sec, b->d_tubes, b->d_adj, n, b->sec_max_cells, b->stream), "section vjp");
+    ck(cudaStreamSynchronize(b->stream), "section vjp sync");
+    size_t k = 0;
+    for (int i = 0; i < n; ++i) {
+        const SectionTube& t = b->h_sec[i];
+        if (dwidth) ck(cudaMemcpy(dwidth + k, t.dw, t.nsec * sizeof(double), cudaMemcpyDeviceToHost), "read dwidth");
+        if (ddepth) ck(cudaMemcpy(ddepth + k, t.dd, t.nsec * sizeof(double), cudaMemcpyDeviceToHost), "read ddepth");
+        k += t.nsec;
+    }
+}
+
 void set_maps(vs_batch* b, int i, const float* dP, const float* dX, const float* dY, float zinv) {
     TubeGrid& g = b->grids[i];
     const size_t n = (size_t)g.H * g.W;
@@ -910,6 +1055,7 @@ void set_maps(vs_batch* b, int i, const float* dP, const float* dX, const float*
     g.zinv_val = zinv;
     b->h_tubes[i].zinv = zinv;
     upload_static_tube(b, (size_t)i);
+    b->sec_maps = false;
     ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev), cudaMemcpyHostToDevice),
        "upload tube descriptors");
     b->ck_steps = 0;    // checkpoints no longer match the maps
@@ -1076,6 +1222,16 @@ int vs_batch_set_maps(vs_batch* b, int32_t tube, const float* depth_p, const flo
                       float z_inv) {
     if (!b || tube < 0 || tube >= (int)b->grids.size()) return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_maps");
     return guarded([&] { set_maps(b, tube, depth_p, depth_x, depth_y, z_inv); });
+}
+
+int vs_batch_set_sections(vs_batch* b, const double* width_m, const double* depth_m, const double* z_inv) {
+    if (!b || !width_m || !depth_m) return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_sections arguments");
+    return guarded([&] { set_sections(b, width_m, depth_m, z_inv); });
+}
+
+int vs_batch_section_gradients(vs_batch* b, double* grad_width, double* grad_depth) {
+    if (!b) return set_error(VS_ERR_INVALID_ARG, "null batch");
+    return guarded([&] { section_gradients(b, grad_width, grad_depth); });
 }
 
 int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces) {

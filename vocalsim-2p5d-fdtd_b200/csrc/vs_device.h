@@ -230,6 +230,48 @@ cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int nt
 // two-mass state into slot 0 of tmm_hist).
 cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_cells, int par, cudaStream_t stream);
 
+// ---- section depth model (vs_sections.cu) -----------------------------------
+// A frame cell the reference's elliptical depth kernel writes: its section,
+// the nominal semi-major axis a0 (m) of its column and its distance from the
+// tube axis in cells; seg = kSectionZero for the cells it sets to 0 (walls),
+// kSectionUnwritten for the cells it leaves (they take the pivot's value).
+constexpr int32_t kSectionUnwritten = -1;
+constexpr int32_t kSectionZero = -2;
+
+struct SectionCell {
+    int32_t seg;
+    float dist;
+    double a0;
+};
+
+struct SectionTube {
+    const SectionCell* cx;    // depth_x writes, H x W (unpitched)
+    const SectionCell* cy;    // depth_y writes
+    const double* w0;         // nominal section widths (m)
+    const double* w;          // current section widths and depths (m)
+    const double* d;
+    double* dw;               // dL/d width, dL/d depth per section (reverse pass)
+    double* dd;
+    uint8_t* clamp;           // per cell: bit 0 dp, bit 1 xs, bit 2 ys raised to the minimum
+    double* gxs;              // reverse-pass scratch planes, H x W
+    double* gys;
+    double* gx;
+    double* gy;
+    double* acc;              // 6 pivot accumulators of the reverse pass
+    double ds;
+    int64_t pivot;            // cell (mid row, tube end), H x W index
+    int32_t H, W, nsec, pad;
+};
+
+// Depth maps of every tube from its current section parameters, written into
+// the tubes' dP / dX / dY planes; max_cells = the largest H x W.
+cudaError_t launch_section_maps(const SectionTube* tubes, const TubeDev* devs, int ntubes, int64_t max_cells,
+                                cudaStream_t st);
+// dL/d width and dL/d depth per section from the per-cell map gradients of
+// the last adjoint (AdjTube gP, gX, gY); dw, dd and acc zeroed by the caller.
+cudaError_t launch_section_vjp(const SectionTube* tubes, const TubeDev* devs, const AdjTube* adj, int ntubes,
+                               int64_t max_cells, cudaStream_t st);
+
 // Formants of ntr device traces of n samples at sampling rate fs (the
 // reference's get_formants_bw): out (device) = ntr x [bandwidth, centre,
 // level] x nf.  Synchronises `st`; returns a vs_status, err gets the text.

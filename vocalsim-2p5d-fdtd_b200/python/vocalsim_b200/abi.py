@@ -161,6 +161,8 @@ def load_library(path: os.PathLike | None = None) -> C.CDLL:
         "vs_batch_adjoint": (C.c_int, [C.c_void_p, fp, fp, fp, fp, fp]),
         "vs_run_noalloc": (C.c_int, [vp, vd, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+        "vs_batch_set_sections": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "vs_batch_section_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "vs_formants": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_int32, C.c_void_p,
                                   C.c_void_p]),
         "vs_last_error": (C.c_char_p, []),

@@ -14,6 +14,9 @@
 * TubeTrace -- torch.autograd.Function over vs_batch_set_maps /
   vs_batch_forward_ckpt (forward) and vs_batch_adjoint (backward): listener
   traces as a function of the depth maps and z_inv of each tube.
+* SectionTrace -- the same from section widths / depths directly, with the
+  depth model and its reverse pass on the device (vs_batch_set_sections,
+  vs_batch_section_gradients).
 * spectral_loss -- L2 between log power spectra over 0..fmax, the transfer
   function the reference plots (results/plt_transfer_function.py:20-24).
 """
@@ -156,6 +159,30 @@ class TubeTrace(torch.autograd.Function):
             out += [torch.from_numpy(gp.astype(np.float64)), torch.from_numpy(gx.astype(np.float64)),
                     torch.from_numpy(gy.astype(np.float64))]
         return tuple(out)
+
+
+class SectionTrace(torch.autograd.Function):
+    """Listener traces (n, steps) of a Batch as a function of each tube's
+    section widths and depths (m) and z_inv, with the depth maps built on the
+    device (vs_batch_set_sections) and the section gradients reduced there
+    (vs_batch_section_gradients).  widths / depths: one 1-D tensor per tube."""
+
+    @staticmethod
+    def forward(ctx, batch: Batch, steps: int, ckpt_every: int, z_inv: torch.Tensor, *sections: torch.Tensor):
+        n = batch.n
+        ws = [t.detach().cpu().numpy() for t in sections[:n]]
+        ds = [t.detach().cpu().numpy() for t in sections[n:]]
+        batch.set_sections(ws, ds, z_inv.detach().cpu().numpy())
+        tr = batch.forward_ckpt(steps, ckpt_every)
+        ctx.batch = batch
+        return torch.from_numpy(tr).to(torch.float64)
+
+    @staticmethod
+    def backward(ctx, grad_trace: torch.Tensor):
+        _, gz = ctx.batch.adjoint(grad_trace.detach().to(torch.float32).cpu().numpy(), maps=False)
+        g = ctx.batch.section_gradients()
+        return (None, None, None, torch.from_numpy(gz.astype(np.float64)),
+                *[torch.from_numpy(w) for w, _ in g], *[torch.from_numpy(d) for _, d in g])
 
 
 def log_power_spectrum(trace: torch.Tensor, fs: float, fmax: float = 5000.0, floor: float = 1e-30) -> torch.Tensor:

@@ -170,9 +170,39 @@ class Batch:
         self._ck_steps = steps
         return tr
 
-    def adjoint(self, dL_dtrace: np.ndarray):
-        """Per-cell gradients (list of (dP, dX, dY) frames per tube) and dL/dz_inv per tube."""
+    def set_sections(self, widths, depths, z_inv=None) -> None:
+        """Depth maps of every tube from its section widths / depths (m), computed
+        on the device (vs_batch_set_sections); z_inv per tube or None."""
+        w = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64).ravel() for x in widths]))
+        d = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64).ravel() for x in depths]))
+        z = None if z_inv is None else np.ascontiguousarray(np.asarray(z_inv, np.float64).ravel())
+        dp = C.POINTER(C.c_double)
+        check(self.lib, self.lib.vs_batch_set_sections(self.h, w.ctypes.data_as(dp), d.ctypes.data_as(dp),
+                                                       None if z is None else z.ctypes.data_as(dp)),
+              "vs_batch_set_sections")
+        self._nsec = [len(np.asarray(x).ravel()) for x in widths]
+
+    def section_gradients(self):
+        """(dL/d widths, dL/d depths) per tube after set_sections / forward_ckpt / adjoint."""
+        tot = sum(self._nsec)
+        gw, gd = np.zeros(tot), np.zeros(tot)
+        dp = C.POINTER(C.c_double)
+        check(self.lib, self.lib.vs_batch_section_gradients(self.h, gw.ctypes.data_as(dp), gd.ctypes.data_as(dp)),
+              "vs_batch_section_gradients")
+        out, k = [], 0
+        for m in self._nsec:
+            out.append((gw[k:k + m], gd[k:k + m]))
+            k += m
+        return out
+
+    def adjoint(self, dL_dtrace: np.ndarray, maps: bool = True):
+        """Per-cell gradients (list of (dP, dX, dY) frames per tube; None with
+        maps=False, leaving them on the device) and dL/dz_inv per tube."""
         g = np.ascontiguousarray(dL_dtrace, dtype=np.float32).reshape(self.n, -1)
+        if not maps:
+            gz = np.zeros(self.n, np.float32)
+            check(self.lib, self.lib.vs_batch_adjoint(self.h, _fp(g), None, None, None, _fp(gz)), "vs_batch_adjoint")
+            return None, gz
         sizes = [d["frame_h"] * d["frame_w"] for d in self.dims]
         tot = sum(sizes)
         gp, gx, gy = (np.zeros(tot, np.float32) for _ in range(3))
