@@ -1,18 +1,19 @@
 """Batched inversion: fit each tube's section widths, section depths and wall
 admittance to a target transfer function.
 
-Every Adam iteration runs one batched checkpointed forward
+Every Adam iteration builds the depth maps from the section parameters on the
+device (vs_batch_set_sections), runs one batched checkpointed forward
 (vs_batch_forward_ckpt) and one batched reverse-time adjoint
-(vs_batch_adjoint) for all tubes together, through SectionDepthModel (the
-per-section parameters -> depth maps, in torch) and TubeTrace (the
-autograd.Function over the C ABI).  The loss of a tube is the mean squared
+(vs_batch_adjoint) for all tubes together, and reduces the map gradients to
+section gradients on the device (vs_batch_section_gradients), through the
+autograd.Function SectionTrace.  The loss of a tube is the mean squared
 difference of log power spectra over 0..5 kHz (the transfer function the
 reference plots, results/plt_transfer_function.py:20-24); the optimiser
 works on log-multipliers of the nominal parameters, so widths, depths and
 z_inv stay positive.
 
 Bounds.  The depth model keeps the wall rows of the nominal rasterisation
-(autograd.SectionDepthModel).  A section narrower than its rasterised air
+(vs_batch_set_sections, autograd.SectionDepthModel).  A section narrower than its rasterised air
 band would put the cells next to its walls outside the ellipse, at the 1 mm
 depth floor beside deeper faces, where the reference's 2.5D update is
 unstable (the FP32 oracle diverges within a few hundred steps for a 5 %
@@ -36,7 +37,7 @@ import time
 import numpy as np
 import torch
 
-from .autograd import SectionDepthModel, TubeTrace, log_power_spectrum
+from .autograd import SectionTrace, log_power_spectrum, tube_layout
 from .solver import Batch, Geometry, params
 
 
@@ -53,7 +54,9 @@ class BatchInversion:
                  fmax: float = 5000.0):
         if any(p.fast_math for p in ps):
             raise ValueError("the adjoint recomputes with the reference arithmetic: use fast_math = 0")
-        self.models = [SectionDepthModel(p, g) for p, g in zip(ps, gs)]
+        lays = [tube_layout(p, g) for p, g in zip(ps, gs)]
+        self.width0 = [torch.tensor(lay["major"], dtype=torch.float64) for lay in lays]
+        self.depth0 = [torch.tensor(lay["minor"], dtype=torch.float64) for lay in lays]
         self.batch = Batch(ps, gs)
         self.n = len(ps)
         self.steps = steps
@@ -64,23 +67,25 @@ class BatchInversion:
         self.target_spec = log_power_spectrum(targets, self.fs, fmax)
         self.amp_limit = 100.0 * targets.abs().amax(dim=1)
         self.best = torch.full((self.n,), float("inf"), dtype=torch.float64)
-        ns = [len(m.width0) for m in self.models]
+        ns = [len(w) for w in self.width0]
         self.log_w = torch.zeros(self.n, max(ns), dtype=torch.float64, requires_grad=True)
         self.log_d = torch.zeros(self.n, max(ns), dtype=torch.float64, requires_grad=True)
         self.log_z = torch.zeros(self.n, dtype=torch.float64, requires_grad=True)
-        self.z0 = torch.tensor([float(m.nominal["dims"]["z_inv_val"]) for m in self.models], dtype=torch.float64)
+        self.z0 = torch.tensor([float(lay["dims"]["z_inv_val"]) for lay in lays], dtype=torch.float64)
         self.opt = torch.optim.Adam([self.log_w, self.log_d, self.log_z], lr=lr)
         self.good = [t.detach().clone() for t in (self.log_w, self.log_d, self.log_z)]
         self.scale = torch.ones(self.n, dtype=torch.float64)
 
     def loss(self) -> torch.Tensor:
-        """Per-tube spectral loss of the current parameters (differentiable)."""
-        maps = []
-        for i, m in enumerate(self.models):
-            k = len(m.width0)
-            maps += list(m.maps(m.width0 * torch.exp(self.log_w[i, :k]), m.depth0 * torch.exp(self.log_d[i, :k])))
+        """Per-tube spectral loss of the current parameters (differentiable); the
+        depth maps are built and differentiated on the device (SectionTrace)."""
+        ws, ds = [], []
+        for i, (w0, d0) in enumerate(zip(self.width0, self.depth0)):
+            k = len(w0)
+            ws.append(w0 * torch.exp(self.log_w[i, :k]))
+            ds.append(d0 * torch.exp(self.log_d[i, :k]))
         z = self.z0 * torch.exp(self.log_z)
-        tr = TubeTrace.apply(self.batch, self.steps, self.ckpt_every, z, *maps)
+        tr = SectionTrace.apply(self.batch, self.steps, self.ckpt_every, z, *ws, *ds)
         d = log_power_spectrum(tr, self.fs, self.fmax) - self.target_spec
         per_tube = (d * d).mean(dim=-1)
         # a diverging trace counts as not finite
