@@ -273,12 +273,14 @@ INV_STEPS = 26460                      # 20 ms at 44.1 kHz x 30
 def inversion_cost(iters: int) -> dict:
     """Batched inversion: 64 tubes at fs = 44100 x 30 (ds 0.374 mm), 20 ms per
     forward, Adam over 44 widths + 44 depths + z_inv per tube against the
-    spectra of other seeded tubes; each iteration = one batched checkpointed
-    forward + one batched adjoint (+ the depth model and loss in torch).
+    spectra of other seeded tubes, reciprocal-form arithmetic; each iteration
+    = depth maps from the sections on the device + one batched checkpointed
+    forward + one batched adjoint + the section reverse pass (+ Adam and the
+    FFT loss in torch).
     Seconds per iteration (median) and the mean spectral error."""
     from vocalsim_b200.inversion import BatchInversion, synthetic_problem
 
-    ps, gs, targets, seeds = synthetic_problem(INV_TUBES, INV_SRATE_MUL, INV_STEPS)
+    ps, gs, targets, seeds = synthetic_problem(INV_TUBES, INV_SRATE_MUL, INV_STEPS, fast_math=1)
     inv = BatchInversion(ps, gs, targets, INV_STEPS, ckpt_every=512, lr=0.02)
     cells = inv.batch.interior_cells
     secs, losses = [], []
@@ -289,7 +291,7 @@ def inversion_cost(iters: int) -> dict:
     best = float(inv.best.mean())
     inv.close()
     return {"workload": f"{INV_TUBES} tubes (stable seeds {seeds[0]}..{seeds[-1]}), fs 44100 x {INV_SRATE_MUL}, "
-                        f"{INV_STEPS} steps, {cells} interior cells, checkpoints every 512",
+                        f"{INV_STEPS} steps, {cells} interior cells, checkpoints every 512, fast_math=1",
             "iterations": iters, "s_per_iteration": round(statistics.median(secs), 3),
             "spectral_error_initial": round(float(np.nanmean(losses[0])), 4),
             "spectral_error_best": round(best, 4),

@@ -289,7 +289,7 @@ int vs_batch_adjoint(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, f
  * scales the semi-major axis of its cells, its depth the minor axis).
  * width_m, depth_m: the tubes' sections concatenated in tube order (m);
  * z_inv: one value per tube (NULL keeps them).  2.5D 3:1 elliptical tubes
- * only, fast_math = 0.  Invalidates stored checkpoints. */
+ * only.  Invalidates stored checkpoints. */
 int vs_batch_set_sections(vs_batch* b, const double* width_m, const double* depth_m, const double* z_inv);
 
 /* dL/d width and dL/d depth of every section (host, concatenated like

@@ -112,3 +112,13 @@ def test_coupled_wall_adjoint_unsupported(cuda_ok):
     with pytest.raises(V.VsError) as e:
         b.forward_ckpt(50, 10)
     assert e.value.status == 7
+
+
+@pytest.mark.parametrize("kw", [dict(cross_sectional_shape=2, mu3d=0.025),
+                                dict(cross_sectional_shape=2, mu3d=0.025, source_type=V.SRC_TMM, tmm_ps_pa=800.0,
+                                     tmm_f64=1)])
+def test_fast_math_gradients(kw, cuda_ok):
+    # reciprocal-form forward and recomputation (quad strips); the finite
+    # differences are of the FP64 oracle as before
+    L, A = S.vowel_tube(3)
+    _check(dict(fast_math=1, **kw), L, A, steps=1200, every=256, parts="PXYZ", seed=4)

@@ -825,7 +825,7 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     // strip list of the history-capturing step kernel (static per batch)
     int64_t cells = 0;
     for (const TubeGrid& g : b->grids) cells += (int64_t)(g.H - 2) * (g.W - 2);
-    const int hshape = history_shape(cells);
+    const int hshape = history_shape(cells, b->fast);
     if (!b->d_hist_tiles) {
         const int keep_shape = b->tiles_shape;
         Tile* keep_tiles = b->d_tiles;
@@ -937,7 +937,6 @@ void section_cells(const TubeGrid& g, std::vector<SectionCell>& cx, std::vector<
 
 void section_setup(vs_batch* b) {
     if (b->d_sec) return;
-    if (b->fast) throw VsFailure{VS_ERR_UNSUPPORTED, "section maps: use fast_math = 0"};
     const int n = (int)b->grids.size();
     std::vector<std::vector<SectionCell>> cx(n), cy(n);
     std::vector<size_t> off(n);
@@ -1013,6 +1012,19 @@ void set_sections(vs_batch* b, const double* width, const double* depth, const d
     }
     ck(cudaMemcpyAsync(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice, b->stream),
        "upload tube descriptors");
+    if (b->fast && zinv) {
+        // the fast_math coefficient tables hold z_inv
+        for (int i = 0; i < n; ++i) {
+            std::vector<uint8_t> desc;
+            std::vector<float> ta, tb;
+            build_descriptors(b->grids[i], desc, ta, tb);
+            const TubeDev& t = b->h_tubes[i];
+            ck(cudaMemcpyAsync((void*)t.desc_a, ta.data(), ta.size() * sizeof(float), cudaMemcpyHostToDevice,
+                               b->stream), "upload descriptor table");
+            ck(cudaMemcpyAsync((void*)t.desc_b, tb.data(), tb.size() * sizeof(float), cudaMemcpyHostToDevice,
+                               b->stream), "upload descriptor table");
+        }
+    }
     ck(launch_section_maps(b->d_sec, b->d_tubes, n, b->sec_max_cells, b->stream), "section maps");
     ck(cudaStreamSynchronize(b->stream), "section maps sync");
     b->sec_maps = true;

@@ -174,13 +174,14 @@ bool shape_has_fast(int shape);
 size_t shape_smem_bytes(int shape, int max_pitch);
 cudaError_t prepare_shape(int shape, int max_pitch);
 
-// One step of the strip kernel that also stores the new state into the tube's
-// history (TubeDev::hist); tubes without a wall oscillator only.  `shape` is
-// history_shape() of the batch's interior cell count (the strips in `tiles`
+// One step that also stores the new state into the tube's history
+// (TubeDev::hist); tubes without a wall oscillator only.  `shape` is
+// history_shape() of the batch's interior cell count and arithmetic (strips,
+// or quad strips in the reciprocal form for fast_math; the tiles in `tiles`
 // must be built for it).
 cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
                                 int local, cudaStream_t stream);
-int history_shape(int64_t cells);
+int history_shape(int64_t cells, bool fast);
 
 // Adjoint buffers of one tube (device memory).
 struct AdjTube {

@@ -571,7 +571,7 @@ __host__ __device__ constexpr uint32_t quad_warp_smem(int stages) {
     return stages > 0 ? kQBars + (uint32_t)stages * kQStage : 0;
 }
 
-template <int TR, int WARPS, int MINB, int STAGES, bool FAST>
+template <int TR, int WARPS, int MINB, int STAGES, bool FAST, bool HIST = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
             RunState* __restrict__ rs, int local) {
@@ -672,7 +672,8 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
                 const int ex = T->exc_x - c0;
                 const bool owner =
                     T->exc_y >= r0 && T->exc_y < r0 + TR && ex >= kQuadLead && ex < kQuadLead + kQuadCommit;
-                exeV = glottal_step(T, par, Pin[(size_t)T->exc_y * pitch + T->exc_x], owner, nullptr);
+                exeV = glottal_step(T, par, Pin[(size_t)T->exc_y * pitch + T->exc_x], owner,
+                                    HIST ? T->tmm_hist + 6 * (n + 1 - rs->run_start) : nullptr);
             }
             exeV = __shfl_sync(kFull, exeV, 0);
         } else {
@@ -862,6 +863,13 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
             }
             st4(Vxout + o, vx, commit_m);
             st4(Vyout + o, vy, commit_m);
+            if constexpr (HIST) {
+                // the state after step n, for the adjoint's segment recomputation
+                float* h = T->hist + (n + 1 - rs->run_start) * 3 * pl;
+                st4(h + o, pn, commit_m);
+                st4(h + pl + o, vx, commit_m);
+                st4(h + 2 * pl + o, vy, commit_m);
+            }
         }
         // ---- shift the row pipeline
         k_above = k_c;
@@ -1151,7 +1159,10 @@ cudaError_t launch_step(int shape, bool wall, bool fast, const TubeDev* tubes, c
     return cudaGetLastError();
 }
 
-int history_shape(int64_t cells) { return cells < 200000 ? 7 : 2; }
+int history_shape(int64_t cells, bool fast) {
+    if (fast) return cells < 200000 ? 21 : 17;
+    return cells < 200000 ? 7 : 2;
+}
 
 cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
                                 int local, cudaStream_t stream) {
@@ -1159,10 +1170,16 @@ cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* til
     // whose step time is the latency of a strip; shape 2 (8-row strips, 4
     // warps per CTA) otherwise
     if (ntiles <= 0) return cudaSuccess;
+    // with fast_math the quad strips of shapes 21 (2 rows, 2 warps) and 17
+    // (16 rows, 4 warps), in the reciprocal form
     if (shape == 7)
         strip_kernel<2, 4, false, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else if (shape == 2)
         strip_kernel<8, 4, false, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else if (shape == 21)
+        quad_kernel<2, 2, 8, 0, true, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else if (shape == 17)
+        quad_kernel<16, 4, 4, 0, true, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

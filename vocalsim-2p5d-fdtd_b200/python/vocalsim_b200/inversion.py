@@ -52,8 +52,8 @@ class BatchInversion:
 
     def __init__(self, ps, gs, targets, steps: int, ckpt_every: int = 512, lr: float = 0.02,
                  fmax: float = 5000.0):
-        if any(p.fast_math for p in ps):
-            raise ValueError("the adjoint recomputes with the reference arithmetic: use fast_math = 0")
+        if len({int(p.fast_math) for p in ps}) != 1:
+            raise ValueError("every tube of a batch needs the same fast_math")
         lays = [tube_layout(p, g) for p, g in zip(ps, gs)]
         self.width0 = [torch.tensor(lay["major"], dtype=torch.float64) for lay in lays]
         self.depth0 = [torch.tensor(lay["minor"], dtype=torch.float64) for lay in lays]
@@ -126,7 +126,7 @@ class BatchInversion:
         self.batch.close()
 
 
-def synthetic_problem(n_tubes: int, srate_mul: int, steps: int, seed0: int = 0):
+def synthetic_problem(n_tubes: int, srate_mul: int, steps: int, seed0: int = 0, fast_math: int = 0):
     """n batch tubes (3:1 elliptical sections, Gaussian source) and the traces
     of their targets (synthetic.batch_target_tube), run on the GPU.
 
@@ -139,7 +139,7 @@ def synthetic_problem(n_tubes: int, srate_mul: int, steps: int, seed0: int = 0):
     n_tubes seeds from seed0 on that are stable for both are used.
     Returns (params, geometries, targets, seeds)."""
     from . import synthetic as S
-    kw = dict(cross_sectional_shape=2, srate_mul=srate_mul, num_steps=steps)
+    kw = dict(cross_sectional_shape=2, srate_mul=srate_mul, num_steps=steps, fast_math=fast_math)
     chosen, targets = [], []
     start = seed0
     while len(chosen) < n_tubes:
@@ -171,9 +171,10 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--lr", type=float, default=0.02)
     ap.add_argument("--ckpt-every", type=int, default=512)
+    ap.add_argument("--fast-math", type=int, default=1, help="1: reciprocal-form arithmetic (quad strips)")
     a = ap.parse_args(argv)
     steps = int(round(a.ms * 1e-3 * 44100 * a.srate_mul))
-    ps, gs, targets, seeds = synthetic_problem(a.tubes, a.srate_mul, steps)
+    ps, gs, targets, seeds = synthetic_problem(a.tubes, a.srate_mul, steps, fast_math=a.fast_math)
     inv = BatchInversion(ps, gs, targets, steps, a.ckpt_every, a.lr)
     print(json.dumps({"tubes": a.tubes, "srate_mul": a.srate_mul, "steps": steps, "seeds": seeds,
                       "interior_cells": inv.batch.interior_cells}), flush=True)
