@@ -311,6 +311,19 @@ def run_b200(args, rank, world):
     batch.set_stream(stream.cuda_stream)
     cells = batch.interior_cells
     sim_steps = args.sim_steps
+    if args.profile_adjoint:
+        # profiling workload of the reverse sweep: 16 stable fs x 30 tubes,
+        # checkpointed forward + adjoint over `profile_adjoint` steps
+        from vocalsim_b200 import synthetic as S
+        seeds = [1, 2, 3, 5, 6, 8, 9, 11, 14, 16, 17, 18, 19, 20, 21, 22]
+        k = args.profile_adjoint
+        pa = [V.params(cross_sectional_shape=2, srate_mul=30, num_steps=k) for _ in seeds]
+        ga = [V.Geometry(*S.batch_tube(sd)[:2]) for sd in seeds]
+        ba = V.Batch(pa, ga)
+        tr = ba.forward_ckpt(k, 512)
+        ba.adjoint((tr * 1e-3).astype(np.float32))
+        ba.close()
+        return None
     if args.profile_steps:
         if args.tile >= 0:
             batch.set_tile(args.tile)
@@ -448,6 +461,8 @@ def main():
     ap.add_argument("--tubes", type=int, default=N_TUBES)
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--profile-steps", type=int, default=0)
+    ap.add_argument("--profile-adjoint", type=int, default=0,
+                    help="run a 16-tube checkpointed forward + adjoint of this many steps, untimed, for ncu")
     ap.add_argument("--tile", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-single", action="store_true")
