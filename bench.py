@@ -356,8 +356,12 @@ def run_b200(args, rank, world):
     ms_step = ms_total / args.steps
     cell_updates_rank = cells * sim_steps
     value = cell_updates_rank * world / (ms_step / 1e3) / 1e9
-    launches_per_forward = sim_steps + math.ceil(sim_steps / 128)
-    launch_ms = ms_step / sim_steps            # average per step-kernel launch incl. graph gaps
+    # a two-step shape advances two time steps per launch and moves the state
+    # planes once per launch: algorithmic bytes per launch = 37 B x cells
+    per_launch = V.tile_shape_steps(tile)
+    step_launches = sim_steps // per_launch + sim_steps % per_launch
+    launches_per_forward = step_launches + math.ceil(sim_steps / 128)
+    launch_ms = ms_step / step_launches        # average per step-kernel launch incl. graph gaps
     achieved_gbs = BYTES_PER_CELL_UPDATE * cells / (launch_ms / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
 
@@ -437,8 +441,9 @@ def run_b200(args, rank, world):
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells, tile, fast),
-                     "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell-update x {cells} cells per launch / "
-                             f"mean launch time {launch_ms * 1e3:.2f} us; peak {peak_kind}"},
+                     "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell per launch x {cells} cells / "
+                             f"mean launch time {launch_ms * 1e3:.2f} us ({per_launch} time step(s) per launch); "
+                             f"peak {peak_kind}"},
         "gpu_launches": args.steps * launches_per_forward,
         "clocks": clocks.summary(),
         "e2e": e2e,

@@ -245,6 +245,11 @@ int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* be
 int vs_tile_shape_count(void);
 int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
 
+/* Time steps one kernel launch of shape i advances: 1, or 2 for the two-step
+ * shapes (fast_math batches without the two-mass source or the coupled wall;
+ * they keep a third set of state planes beside the two parity sets). */
+int vs_tile_shape_steps(int32_t i, int32_t* steps_per_launch);
+
 void vs_batch_destroy(vs_batch* b);
 
 /* Formants of listener traces on the device: for each of n_traces traces of

@@ -194,6 +194,36 @@ def test_fast_math_shapes_agree_and_batch_rows_equal_single(cuda_ok):
         assert np.array_equal(ref[i], single)
 
 
+def test_two_step_shapes_equal_single_step(cuda_ok):
+    """Without the two-mass source a fast_math batch also offers the two-step
+    shapes (two time steps per launch, the state alternating with a third
+    buffer set).  Runs of odd and even lengths, in and out of the captured
+    128-step chunks, must give the traces of the single-step shapes exactly."""
+    n = 4
+    tubes = [S.batch_tube(i)[:2] for i in range(n)]
+    kws = [dict(cross_sectional_shape=2, fast_math=1),
+           dict(cross_sectional_shape=2, fast_math=1, mouth_radiation_cond=1),
+           dict(cross_sectional_shape=1, fast_math=1, source_type=0),
+           dict(cross_sectional_shape=2, fast_math=1, srate_mul=2)]
+    b = V.Batch([V.params(**k) for k in kws], [V.Geometry(L, A) for L, A in tubes])
+    segments = [1, 2, 3, 128, 131, 257, 64]
+    ref = None
+    ran = 0
+    for k in range(len(V.tile_shapes())):
+        try:
+            b.set_tile(k)
+        except V.VsError:
+            continue
+        b.reset()
+        tr = np.concatenate([b.run(m) for m in segments], axis=1)
+        ran += 1
+        if ref is None:
+            ref = tr
+        assert np.array_equal(tr, ref), f"tile shape {k}"
+    assert ran >= 22
+    assert np.all(np.isfinite(ref)) and np.abs(ref).max() > 0
+
+
 def test_fast_math_must_agree_within_a_batch(cuda_ok):
     L, A = S.vowel_tube(1)
     with pytest.raises(V.VsError) as e:

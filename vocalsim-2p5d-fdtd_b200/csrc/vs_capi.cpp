@@ -100,6 +100,10 @@ struct vs_batch {
     size_t exc_bytes = 0;
     Tile* d_hist_tiles = nullptr;
     int n_hist_tiles = 0;
+    Tile* d_odd_tiles = nullptr;           // single-step tiles beside a two-step shape
+    char* x_mem = nullptr;                 // third state set of the two-step shapes (TubeDev::X)
+    int n_odd_tiles = 0;
+    int odd_shape = -1;
     // section depth model (vs_batch_set_sections): per-tube descriptors and buffers
     std::vector<SectionTube> h_sec;
     SectionTube* d_sec = nullptr;
@@ -128,6 +132,10 @@ struct vs_batch {
         if (d_gtrace) cudaFree(d_gtrace);
         if (d_exc) cudaFree(d_exc);
         if (d_hist_tiles) cudaFree(d_hist_tiles);
+        if (d_odd_tiles) cudaFree(d_odd_tiles);
+        d_odd_tiles = nullptr;
+        if (x_mem) cudaFree(x_mem);
+        x_mem = nullptr;
         if (d_sec) cudaFree(d_sec);
         if (sec_mem) cudaFree(sec_mem);
         d_sec = nullptr; sec_mem = nullptr;
@@ -151,11 +159,13 @@ namespace {
 // Default launch shapes when no autotune ran: 16-row strips with 4 warps per
 // CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells;
 // with fast_math the quad strips of the same heights (16 rows x 4 warps,
-// 2 rows x 2 warps).
+// 2 rows x 2 warps), and for large fast_math batches without the two-mass
+// source the two-step strips (32 rows x 4 warps of 64 columns).
 constexpr int kDefaultShape = 1;
 constexpr int kSmallShape = 8;
 constexpr int kFastShape = 17;
 constexpr int kFastSmallShape = 21;
+constexpr int kTwoStepShape = 36;
 constexpr int64_t kSmallGridCells = 200000;
 
 int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
@@ -204,13 +214,24 @@ size_t smem_optin_limit(int device) {
     return (size_t)v;
 }
 
+bool any_tmm(const vs_batch* b) {
+    for (const TubeGrid& g : b->grids)
+        if (g.tmm) return true;
+    return false;
+}
+
 bool shape_fits(const vs_batch* b, int shape) {
-    if (b->wall && tile_shape(shape).kind == SHAPE_QUAD) return false;   // no wall-oscillator variant
+    const int kind = tile_shape(shape).kind;
+    if (b->wall && (kind == SHAPE_QUAD || kind == SHAPE_QUAD2)) return false;   // no wall-oscillator variant
+    // two-step kernels: fast_math with table sources only
+    if (kind == SHAPE_QUAD2 && (!b->fast || any_tmm(b))) return false;
     if (b->fast && !shape_has_fast(shape)) return false;
     return shape_smem_bytes(shape, b->max_pitch) <= smem_optin_limit(b->device);
 }
 
-int default_shape(const vs_batch* b) {
+// single-step default (also the shape of the last step of an odd count
+// run with a two-step shape)
+int single_step_shape(const vs_batch* b) {
     int64_t cells = 0;
     for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
     const bool small = cells < kSmallGridCells;
@@ -218,8 +239,16 @@ int default_shape(const vs_batch* b) {
     return small ? kSmallShape : kDefaultShape;
 }
 
-void build_tiles(vs_batch* b, int shape) {
-    if (b->tiles_shape == shape && b->d_tiles) return;
+int default_shape(const vs_batch* b) {
+    int64_t cells = 0;
+    for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
+    if (cells >= kSmallGridCells && tile_shape(kTwoStepShape).kind == SHAPE_QUAD2 && shape_fits(b, kTwoStepShape))
+        return kTwoStepShape;
+    return single_step_shape(b);
+}
+
+// Tile list of a launch shape, uploaded to a new device buffer (*n tiles).
+Tile* make_tiles(vs_batch* b, int shape, int* n) {
     const TileShape ts = tile_shape(shape);
     if (!shape_fits(b, shape)) throw VsFailure{VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)"};
     ck(prepare_shape(shape, b->max_pitch), "kernel attributes");
@@ -241,25 +270,66 @@ void build_tiles(vs_batch* b, int shape) {
             }
             // strips start at c0 = commit*k - lead and commit columns
             // c0+lead .. c0+lead+commit-1; rows r0 .. r0+rows-1
-            const bool quad = ts.kind == SHAPE_QUAD;
-            const int lead = quad ? kQuadLead : kStripLead, commit = quad ? kQuadCommit : kStripCommit;
+            const bool quad = ts.kind == SHAPE_QUAD || ts.kind == SHAPE_QUAD2;
+            const int nc = ts.lane_cols;
+            const int lead = ts.kind == SHAPE_QUAD2 ? nc : quad ? kQuadLead : kStripLead;
+            const int commit = ts.cols;
             for (int c0 = -lead; c0 + lead <= g.W - 2; c0 += commit) {
                 Tile t{};
                 t.tube = (int32_t)i;
                 t.r0 = r0;
                 t.c0 = c0;
-                classify_strip(code_at, g.H, g.W, r0, ts.rows, c0, t, lead, commit);
+                if (ts.kind == SHAPE_QUAD2)
+                    classify_strip(code_at, g.H, g.W, r0 - 1, ts.rows + 2, c0, t, nc / 2, 31 * nc);
+                else
+                    classify_strip(code_at, g.H, g.W, r0, ts.rows, c0, t, lead, commit);
                 tiles.push_back(t);
             }
         }
     }
-    if (b->d_tiles) { cudaFree(b->d_tiles); b->d_tiles = nullptr; }
-    ck(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile)), "cudaMalloc(tiles)");
-    ck(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice),
-       "upload tiles");
-    b->ntiles = (int)tiles.size();
+    Tile* d = nullptr;
+    ck(cudaMalloc(&d, tiles.size() * sizeof(Tile)), "cudaMalloc(tiles)");
+    const cudaError_t e = cudaMemcpy(d, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) cudaFree(d);
+    ck(e, "upload tiles");
+    *n = (int)tiles.size();
+    return d;
+}
+
+void build_tiles(vs_batch* b, int shape) {
+    if (b->tiles_shape == shape && b->d_tiles) return;
+    int n = 0;
+    Tile* d = make_tiles(b, shape, &n);
+    if (b->d_tiles) cudaFree(b->d_tiles);
+    b->d_tiles = d;
+    b->ntiles = n;
     b->tiles_shape = shape;
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; b->graph_shape = -1; }
+    if (tile_shape(shape).kind == SHAPE_QUAD2) {
+        // a two-step shape advances an odd step count's last step with the
+        // single-step shape of the batch
+        if (!b->d_odd_tiles) {
+            b->odd_shape = single_step_shape(b);
+            b->d_odd_tiles = make_tiles(b, b->odd_shape, &b->n_odd_tiles);
+        }
+        // and alternates the state with a third set of planes (zero ring
+        // cells; kGuard bytes around it for the strips' edge reads)
+        if (!b->x_mem) {
+            size_t total = kGuard;
+            for (const TubeDev& t : b->h_tubes) total += 3 * (size_t)t.plane * sizeof(float);
+            total += kGuard;
+            ck(cudaMalloc(&b->x_mem, total), "cudaMalloc(third state set)");
+            ck(cudaMemset(b->x_mem, 0, total), "zero third state set");
+            size_t off = kGuard;
+            for (TubeDev& t : b->h_tubes) {
+                t.X = reinterpret_cast<float*>(b->x_mem + off);
+                off += 3 * (size_t)t.plane * sizeof(float);
+            }
+            ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev),
+                          cudaMemcpyHostToDevice),
+               "upload tube descriptors");
+        }
+    }
 }
 
 void ensure_graph(vs_batch* b) {
@@ -268,9 +338,12 @@ void ensure_graph(vs_batch* b) {
     cudaGraph_t g = nullptr;
     ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
-    for (int i = 0; i < kChunk && err == cudaSuccess; ++i)
+    const bool two = tile_shape(b->shape).kind == SHAPE_QUAD2;
+    const int launches = two ? kChunk / 2 : kChunk;     // a two-step launch advances two steps
+    for (int i = 0; i < launches && err == cudaSuccess; ++i)
         err = launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch);
-    if (err == cudaSuccess) err = launch_advance(b->d_rs, kChunk, b->stream);
+    if (err == cudaSuccess)
+        err = two ? launch_advance2(b->d_rs, kChunk, (kChunk / 2) & 1, b->stream) : launch_advance(b->d_rs, kChunk, b->stream);
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     ck(err, "capture step launches");
     ck(e2, "end capture");
@@ -385,8 +458,13 @@ void upload_static(vs_batch* b) {
 
 void reset_state(vs_batch* b) {
     // fields, wall state and the two-mass state all restart at zero
-    for (size_t i = 0; i < b->grids.size(); ++i)
+    for (size_t i = 0; i < b->grids.size(); ++i) {
         ck(cudaMemsetAsync(b->state_base[i], 0, b->state_bytes[i], b->stream), "zero state");
+        // the two-step kernels' third set: its ring cells must read as zero
+        if (b->h_tubes[i].X)
+            ck(cudaMemsetAsync(b->h_tubes[i].X, 0, 3 * (size_t)b->h_tubes[i].plane * sizeof(float), b->stream),
+               "zero third state set");
+    }
     RunState rs{};
     ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "reset run state");
     ck(cudaStreamSynchronize(b->stream), "reset sync");
@@ -482,6 +560,48 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
     b->shape = default_shape(b);
 }
 
+// Issue `count` steps from the device step counter (graph chunks of kChunk
+// plus direct launches), RunState already set with bsel = 0.  With a
+// two-step shape the launches alternate between the parity set and the third
+// set; an odd number of them is followed by a copy back, and an odd step
+// count ends with one launch of the batch's single-step shape, so the state
+// of the final step is in its parity set (bsel = 0) when the call returns.
+void issue_steps(vs_batch* b, int64_t count) {
+    const bool two = tile_shape(b->shape).kind == SHAPE_QUAD2;
+    int64_t done = 0;
+    if (count >= kChunk) {
+        ensure_graph(b);
+        for (; done + kChunk <= count; done += kChunk) ck(cudaGraphLaunch(b->graph, b->stream), "graph launch");
+    }
+    const int rem = (int)(count - done);
+    if (!two) {
+        for (int i = 0; i < rem; ++i)
+            ck(launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream,
+                           b->max_pitch),
+               "step launch");
+        if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
+        return;
+    }
+    const int pairs = rem / 2;
+    for (int i = 0; i < pairs; ++i)
+        ck(launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream,
+                       b->max_pitch),
+           "two-step launch");
+    if (pairs) ck(launch_advance2(b->d_rs, 2 * pairs, pairs & 1, b->stream), "advance");
+    if (pairs & 1) {
+        int64_t max_plane = 0;
+        for (const TubeDev& t : b->h_tubes) max_plane = std::max<int64_t>(max_plane, t.plane);
+        ck(launch_copy_back(b->d_tubes, (int)b->grids.size(), (int)max_plane, b->d_rs, b->stream), "copy back");
+        ck(launch_advance2(b->d_rs, 0, 1, b->stream), "advance");
+    }
+    if (rem & 1) {
+        ck(launch_step(b->odd_shape, b->wall, b->fast, b->d_tubes, b->d_odd_tiles, b->n_odd_tiles, b->d_rs, 0,
+                       b->stream, b->max_pitch),
+           "step launch");
+        ck(launch_advance(b->d_rs, 1, b->stream), "advance");
+    }
+}
+
 void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     const int n = (int)b->grids.size();
     if (b->shape < 0) b->shape = default_shape(b);
@@ -500,15 +620,7 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     rs.trace = b->d_trace;
     rs.trace_stride = steps;
     ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
-    int64_t done = 0;
-    if (steps >= kChunk) {
-        ensure_graph(b);
-        for (; done + kChunk <= steps; done += kChunk) ck(cudaGraphLaunch(b->graph, b->stream), "graph launch");
-    }
-    const int rem = (int)(steps - done);
-    for (int i = 0; i < rem; ++i)
-        ck(launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch), "step launch");
-    if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
+    issue_steps(b, steps);
     b->step += steps;
     if (traces) {
         ck(cudaMemcpyAsync(traces, b->d_trace, need * sizeof(float),
@@ -531,21 +643,6 @@ void check_adjoint_support(const vs_batch* b) {
     for (const TubeGrid& g : b->grids) {
         if (g.wall_ode) throw VsFailure{VS_ERR_UNSUPPORTED, "adjoint of the coupled wall oscillator is not implemented"};
     }
-}
-
-// Issue `count` step launches from the device step counter (graph chunks of
-// kChunk plus direct launches), RunState already set.
-void issue_steps(vs_batch* b, int64_t count) {
-    int64_t done = 0;
-    if (count >= kChunk) {
-        ensure_graph(b);
-        for (; done + kChunk <= count; done += kChunk) ck(cudaGraphLaunch(b->graph, b->stream), "graph launch");
-    }
-    const int rem = (int)(count - done);
-    for (int i = 0; i < rem; ++i)
-        ck(launch_step(b->shape, b->wall, b->fast, b->d_tubes, b->d_tiles, b->ntiles, b->d_rs, i, b->stream, b->max_pitch),
-           "step launch");
-    if (rem) ck(launch_advance(b->d_rs, rem, b->stream), "advance");
 }
 
 void copy_state(vs_batch* b, int k, bool save) {
@@ -826,24 +923,7 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     int64_t cells = 0;
     for (const TubeGrid& g : b->grids) cells += (int64_t)(g.H - 2) * (g.W - 2);
     const int hshape = history_shape(cells, b->fast);
-    if (!b->d_hist_tiles) {
-        const int keep_shape = b->tiles_shape;
-        Tile* keep_tiles = b->d_tiles;
-        const int keep_n = b->ntiles;
-        b->d_tiles = nullptr;
-        b->tiles_shape = -1;
-        cudaGraphExec_t keep_graph = b->graph;
-        const int keep_graph_shape = b->graph_shape;
-        b->graph = nullptr;
-        build_tiles(b, hshape);
-        b->d_hist_tiles = b->d_tiles;
-        b->n_hist_tiles = b->ntiles;
-        b->d_tiles = keep_tiles;
-        b->ntiles = keep_n;
-        b->tiles_shape = keep_shape;
-        b->graph = keep_graph;
-        b->graph_shape = keep_graph_shape;
-    }
+    if (!b->d_hist_tiles) b->d_hist_tiles = make_tiles(b, hshape, &b->n_hist_tiles);
     auto hist_step = [&](int j) {
         return launch_step_history(hshape, b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, j, b->stream);
     };
@@ -1225,6 +1305,13 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {
     const TileShape s = tile_shape(i);
     if (rows) *rows = s.rows;
     if (cols) *cols = s.cols * s.warps;
+    return VS_OK;
+}
+
+int vs_tile_shape_steps(int32_t i, int32_t* steps_per_launch) {
+    if (i < 0 || i >= tile_shape_count() || !steps_per_launch)
+        return set_error(VS_ERR_INVALID_ARG, "vs_tile_shape_steps arguments");
+    *steps_per_launch = tile_shape(i).kind == SHAPE_QUAD2 ? 2 : 1;
     return VS_OK;
 }
 

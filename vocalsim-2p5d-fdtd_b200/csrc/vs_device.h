@@ -52,6 +52,7 @@ struct TubeDev {
     const uint8_t* desc;
     const float4* desc_a;
     const float4* desc_b;
+    float* X;             // fast_math: a third P, Vx, Vy set (`plane` apart) for the two-step kernels
     TmmConsts tmmc;
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
     // state history for the adjoint's recomputation (strip kernel with
@@ -70,7 +71,7 @@ struct RunState {
     float* trace;         // device trace buffer, [ntubes][trace_stride]
     int64_t trace_stride;
     int32_t error;        // sticky device error word (0 = ok)
-    int32_t pad;
+    int32_t bsel;         // two-step kernels: 1 = the state of `step` is in TubeDev::X
 };
 
 // Strip geometry of the step kernel: lane i of a warp holds column c0 + i;
@@ -133,7 +134,7 @@ __host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0
             for (int c = cfirst; c <= plast; ++c)
                 if ((code(r, c) & CODE_TYPE_MASK) != VS_CELL_AIR) { t.p_rows |= 1ull << (r - r0 + 1); break; }
         }
-        if (r >= r0) {
+        if (r >= r0 && r >= 1) {
             int cls = V_PLAIN;
             for (int c = cfirst; c <= vlast; ++c) {
                 const int kc = code(r, c);
@@ -151,10 +152,15 @@ __host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0
 // rows per strip, committed columns per strip, warps per CTA.  Bands: rows
 // per band (a band spans the full frame width; cols = 0), warps per CTA.
 // Quad strips have no wall-oscillator variant.
-enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1, SHAPE_QUAD = 2 };
+enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1, SHAPE_QUAD = 2, SHAPE_QUAD2 = 3 };
 
+// Two-step quad strips of NC columns per lane start at c0 = 30 NC k - NC,
+// commit columns c0 + NC .. c0 + 31 NC - 1 and classify an extended region:
+// rows from r0 - 2 (p_rows) / r0 - 1 (velocity masks), columns c0 + NC/2 ..
+// c0 + 32 NC - NC/2 - 1.
 struct TileShape {
     int rows, cols, warps, kind;
+    int lane_cols;        // quad strips: columns per lane
 };
 
 int tile_shape_count();
@@ -284,5 +290,10 @@ void record_error(const char* msg);
 
 // RunState::step += k (the tail node of a captured chunk).
 cudaError_t launch_advance(RunState* rs, int k, cudaStream_t stream);
+// Two-step kernels: RunState::step += k, RunState::bsel ^= toggle.
+cudaError_t launch_advance2(RunState* rs, int k, int toggle, cudaStream_t stream);
+// Move each tube's state from TubeDev::X back to the parity set of RunState::step.
+cudaError_t launch_copy_back(const TubeDev* tubes, int ntubes, int max_plane_cells, const RunState* rs,
+                             cudaStream_t stream);
 
 }  // namespace vsb

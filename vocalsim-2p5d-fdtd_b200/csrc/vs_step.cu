@@ -896,6 +896,278 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 }
 
 // ---------------------------------------------------------------------------
+// Two-step quad-strip kernel (fast_math, table sources, no coupled wall):
+// every strip advances TWO time steps per launch.  A lane holds NC adjacent
+// columns (NC = 4 or 2), a warp 32 NC columns, of which lanes 1..30 commit.
+// Step n runs the quad-strip row pipeline over rows r0-2 .. rlast+1 and all
+// columns of the warp; step n+1 follows one row behind on the values step n
+// just produced in registers, and only step n+1 is stored.  The halo this
+// needs -- two columns on each side (lanes 0 and 31) and two rows above /
+// one below -- is recomputed by the neighbouring strips, so the state of
+// step n+1 is never written or read back: per two steps the planes are read
+// and written once.  The step n+2 state goes to the other of two buffer sets
+// (the parity set of step n and a third set TubeDev::X, alternating per
+// launch); per cell and step the arithmetic is that of the quad-strip kernel
+// in the reciprocal form, so the values are those of two single steps.
+// Tile masks classify the extended region (rows from r0-2 / r0-1, columns
+// c0 + NC/2 .. c0 + 32 NC - NC/2 - 1): bit j of v_generic = row r0-1+j.
+// ---------------------------------------------------------------------------
+template <int NC>
+__device__ __forceinline__ void ldn(float (&d)[NC], const float* p) {
+    if constexpr (NC == 4) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    } else {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+        d[0] = v.x; d[1] = v.y;
+    }
+}
+
+template <int NC>
+__device__ __forceinline__ void stn(float* p, const float (&v)[NC], unsigned mask) {
+    if constexpr (NC == 4) {
+        st4(p, v, mask);
+    } else if (mask == 0x3u) {
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    } else if (mask != 0u) {
+        if (mask & 1u) p[0] = v[0];
+        if (mask & 2u) p[1] = v[1];
+    }
+}
+
+template <int TR, int WARPS, int MINB, int NC>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
+             RunState* __restrict__ rs, int local) {
+    const int lane = threadIdx.x & 31;
+    const int wi = blockIdx.x * WARPS + (threadIdx.x >> 5);
+    if (wi >= nitems) return;
+    const Tile it = items[wi];
+    const TubeDev* __restrict__ T = tubes + it.tube;
+    const int64_t n = rs->step + 2 * (int64_t)local;
+    const int par = (int)(n & 1);
+    const bool from_x = ((rs->bsel ^ local) & 1) != 0;
+    const int H = T->H, W = T->W, pitch = T->pitch;
+    const int r0 = it.r0, c0 = it.c0, x0 = c0 + NC * lane;
+    unsigned int_m = 0, commit_m = 0;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const bool in = x0 + q >= 1 && x0 + q <= W - 2;
+        int_m |= (unsigned)in << q;
+        commit_m |= (unsigned)(in && lane >= 1 && lane <= 30) << q;
+    }
+    const int64_t pl = T->plane;
+    float* __restrict__ Bp = T->P[0] + par * pl;          // P, Vx, Vy of step n's parity: +0, +2pl, +4pl
+    float* __restrict__ Xp = T->X;                        // third set: +0, +pl, +2pl
+    const float* __restrict__ Pin = from_x ? Xp : Bp;
+    const float* __restrict__ Vxin = from_x ? Xp + pl : Bp + 2 * pl;
+    const float* __restrict__ Vyin = from_x ? Xp + 2 * pl : Bp + 4 * pl;
+    float* __restrict__ Pout = from_x ? Bp : Xp;
+    float* __restrict__ Vxout = from_x ? Bp + 2 * pl : Xp + pl;
+    float* __restrict__ Vyout = from_x ? Bp + 4 * pl : Xp + 2 * pl;
+    const float* __restrict__ dPp = T->dP;
+    const float* __restrict__ dXp = dPp + pl;
+    const float* __restrict__ dYp = dPp + 2 * pl;
+    const uint8_t* __restrict__ desc = T->desc;
+    const float4* __restrict__ ta = T->desc_a;
+    const float4* __restrict__ tb = T->desc_b;
+    const float K1 = T->K1, bco = T->bcoef;
+    const int lis_y = T->lis_y, lis_q = T->lis_x - x0;
+    const bool lis_here = lis_q >= 0 && lis_q < NC && ((commit_m >> lis_q) & 1u);
+    const uint64_t vgen = it.v_generic;
+    float exe1 = 0.0f, exe2 = 0.0f;
+    if (it.has_exc) {
+        exe1 = n < T->src_len ? T->src[n] : 0.0f;
+        exe2 = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+    }
+    const int rlast = min(r0 + TR - 1, H - 2);
+    float* __restrict__ trace = rs->trace + (int64_t)it.tube * rs->trace_stride + (n - rs->run_start);
+
+    // rows outside the frame read as zeros (they only feed values that are not used)
+    auto ldr = [&](float (&d)[NC], const float* base, int row) {
+        if (row >= 0 && row <= H - 1) {
+            ldn<NC>(d, base + (int64_t)row * pitch + x0);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NC; ++q) d[q] = 0.0f;
+        }
+    };
+    auto ldk = [&](int row) -> uint32_t {
+        if (row < 0 || row > H - 1) return 0u;
+        const uint8_t* p = desc + (int64_t)row * pitch + x0;
+        if constexpr (NC == 4) return __ldg(reinterpret_cast<const unsigned int*>(p));
+        else return (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(p));
+    };
+
+    // step-n pipeline at row r: state and maps of row r, Vy dY of row r+1
+    int r = r0 - 2;
+    float vx_c[NC], dx_c[NC], p_c[NC], dp_c[NC], vy_c[NC], dy_c[NC], vy_n[NC], dy_n[NC];
+    ldr(vx_c, Vxin, r);
+    ldr(dx_c, dXp, r);
+    ldr(p_c, Pin, r);
+    ldr(dp_c, dPp, r);
+    uint32_t k_c = ldk(r);
+    ldr(vy_c, Vyin, r);
+    ldr(dy_c, dYp, r);
+    ldr(vy_n, Vyin, r + 1);
+    ldr(dy_n, dYp, r + 1);
+    // step-n results of the previous row (r-1) for step n+1, and P'' of the row above it
+    float pn1_p[NC], v1x_p[NC], v1y_p[NC], u1_p[NC], w1_p[NC], dp_p[NC], pn2_p[NC];
+    uint32_t k_p = 0;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        pn1_p[q] = 0.0f; v1x_p[q] = 0.0f; v1y_p[q] = 0.0f; u1_p[q] = 0.0f; w1_p[q] = 0.0f;
+        dp_p[q] = 1.0f; pn2_p[q] = 0.0f;
+    }
+
+    for (int j = 0; r <= rlast + 1; ++j, ++r) {
+        // ---- loads for the next row (read-only this launch)
+        float vx_1[NC], dx_1[NC], p_1[NC], dp_1[NC], vy_2[NC], dy_2[NC];
+        ldr(vx_1, Vxin, r + 1);
+        ldr(dx_1, dXp, r + 1);
+        ldr(p_1, Pin, r + 1);
+        ldr(dp_1, dPp, r + 1);
+        const uint32_t k_1 = ldk(r + 1);
+        ldr(vy_2, Vyin, r + 2);
+        ldr(dy_2, dYp, r + 2);
+
+        // ---- step n, pressure of row r (FDTDEngineCPU.cpp:316-339, reciprocal form)
+        const bool prow1 = r >= 1 && r <= H - 2;
+        const unsigned cm1 = prow1 ? int_m : 0u;
+        float ux_c[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) ux_c[q] = fmul(vx_c[q], dx_c[q]);
+        const float ux_l = __shfl_up_sync(kFull, ux_c[NC - 1], 1);
+        float4 da[NC];
+        float pn1[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            da[q] = __ldg(ta + code_byte(k_c, q));
+            const float uxl = q == 0 ? ux_l : ux_c[q - 1];
+            const float ks = fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(fmul(vy_c[q], dy_c[q]), fmul(vy_n[q], dy_n[q]))));
+            const float v = fmul(__fmaf_rn(-ks, rcp_approx(dp_c[q]), p_c[q]), da[q].z);
+            pn1[q] = ((cm1 >> q) & 1u) ? v : 0.0f;
+        }
+        const float p_r = __shfl_down_sync(kFull, pn1[0], 1);
+        // ---- step n, velocity of row r (FDTDEngineCPU.cpp:364-410)
+        const bool vrow1 = r >= r0 - 1 && prow1;
+        const unsigned vm1 = vrow1 ? int_m : 0u;
+        const bool gen1 = j >= 1 && ((vgen >> (j - 1)) & 1);
+        float v1x[NC], v1y[NC], u1[NC], w1[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            const float pr = q < NC - 1 ? pn1[q + 1] : p_r;
+            float vx = fmul(fsub(vx_c[q], fmul(bco, fsub(pr, pn1[q]))), da[q].x);
+            float vy = fmul(fsub(vy_c[q], fmul(bco, fsub(pn1_p[q], pn1[q]))), da[q].y);
+            if (gen1) {
+                const float4 db = __ldg(tb + code_byte(k_c, q));
+                vx = __fmaf_rn(da[q].w, exe1, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn1[q], vx)));
+                vy = __fmaf_rn(-db.w, pn1_p[q], __fmaf_rn(db.z, pn1[q], vy));
+            }
+            v1x[q] = ((vm1 >> q) & 1u) ? vx : 0.0f;
+            v1y[q] = ((vm1 >> q) & 1u) ? vy : 0.0f;
+            u1[q] = fmul(v1x[q], dx_c[q]);
+            w1[q] = fmul(v1y[q], dy_c[q]);
+        }
+        if (r == lis_y && r >= r0 && r <= rlast && lis_here) {
+            float pv = pn1[0];
+#pragma unroll
+            for (int q = 1; q < NC; ++q) if (lis_q == q) pv = pn1[q];
+            trace[0] = pv;
+        }
+
+        // ---- step n+1 at row s = r - 1
+        const int s = r - 1;
+        if (s >= r0 - 1) {
+            const bool prow2 = s >= 1 && s <= H - 2;
+            const unsigned cm2 = prow2 ? int_m : 0u;
+            const float ul = __shfl_up_sync(kFull, u1_p[NC - 1], 1);
+            float pn2[NC];
+            float4 da_p[NC];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                da_p[q] = __ldg(ta + code_byte(k_p, q));
+                const float uxl = q == 0 ? ul : u1_p[q - 1];
+                const float ks = fmul(K1, fadd(fsub(u1_p[q], uxl), fsub(w1_p[q], w1[q])));
+                const float v = fmul(__fmaf_rn(-ks, rcp_approx(dp_p[q]), pn1_p[q]), da_p[q].z);
+                pn2[q] = ((cm2 >> q) & 1u) ? v : 0.0f;
+            }
+            const float p2_r = __shfl_down_sync(kFull, pn2[0], 1);
+            if (s >= r0 && s <= rlast) {
+                const bool gen2 = ((vgen >> (j - 2)) & 1);
+                float vx2[NC], vy2[NC];
+#pragma unroll
+                for (int q = 0; q < NC; ++q) {
+                    const float pr = q < NC - 1 ? pn2[q + 1] : p2_r;
+                    float vx = fmul(fsub(v1x_p[q], fmul(bco, fsub(pr, pn2[q]))), da_p[q].x);
+                    float vy = fmul(fsub(v1y_p[q], fmul(bco, fsub(pn2_p[q], pn2[q]))), da_p[q].y);
+                    if (gen2) {
+                        const float4 db = __ldg(tb + code_byte(k_p, q));
+                        vx = __fmaf_rn(da_p[q].w, exe2, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn2[q], vx)));
+                        vy = __fmaf_rn(-db.w, pn2_p[q], __fmaf_rn(db.z, pn2[q], vy));
+                    }
+                    vx2[q] = vx;
+                    vy2[q] = vy;
+                }
+                const int64_t o = (int64_t)s * pitch + x0;
+                stn<NC>(Pout + o, pn2, commit_m);
+                stn<NC>(Vxout + o, vx2, commit_m);
+                stn<NC>(Vyout + o, vy2, commit_m);
+                if (s == lis_y && lis_here) {
+                    float pv = pn2[0];
+#pragma unroll
+                    for (int q = 1; q < NC; ++q) if (lis_q == q) pv = pn2[q];
+                    trace[1] = pv;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NC; ++q) pn2_p[q] = pn2[q];
+        }
+
+        // ---- shift the row pipelines
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            pn1_p[q] = pn1[q];
+            v1x_p[q] = v1x[q];
+            v1y_p[q] = v1y[q];
+            u1_p[q] = u1[q];
+            w1_p[q] = w1[q];
+            dp_p[q] = dp_c[q];
+            vx_c[q] = vx_1[q];
+            dx_c[q] = dx_1[q];
+            p_c[q] = p_1[q];
+            dp_c[q] = dp_1[q];
+            vy_c[q] = vy_n[q];
+            dy_c[q] = dy_n[q];
+            vy_n[q] = vy_2[q];
+            dy_n[q] = dy_2[q];
+        }
+        k_p = k_c;
+        k_c = k_1;
+    }
+}
+
+// After an odd number of two-step launches the state sits in TubeDev::X:
+// copy it back to the parity set of the current step.
+__global__ void copy_back_kernel(const TubeDev* __restrict__ tubes, const RunState* __restrict__ rs) {
+    const TubeDev& T = tubes[blockIdx.y];
+    const int64_t n = (int64_t)T.H * T.pitch;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int par = (int)(rs->step & 1);
+    const int64_t pl = T.plane;
+    float* B = T.P[0] + par * pl;
+    B[i] = T.X[i];
+    B[2 * pl + i] = T.X[pl + i];
+    B[4 * pl + i] = T.X[2 * pl + i];
+}
+
+__global__ void advance2_kernel(RunState* rs, int k, int toggle) {
+    rs->step += k;
+    rs->bsel ^= toggle;
+}
+
+// ---------------------------------------------------------------------------
 // Band kernel: one CTA per band of R rows of a tube.  A band's rows are
 // contiguous in every plane (rows are `pitch` apart), so the rows r0-1 ..
 // r0+R of P, Vx, Vy, dP, dX, dY and the codes arrive with one bulk copy per
@@ -1081,6 +1353,7 @@ struct ShapeEntry {
     StepFn plain, wall;   // wall = nullptr: no wall-oscillator variant
     int stages;           // quad strips: shared-memory row stages per warp (0 = register prefetch)
     StepFn fast;          // reciprocal-form arithmetic (fast_math); nullptr: none
+    int lane_cols = 4;    // two-step quad strips: columns per lane
 };
 
 #define VS_STRIP(R, WARPS, MINB) \
@@ -1088,6 +1361,8 @@ struct ShapeEntry {
 #define VS_BAND(R) {SHAPE_BAND, R, kBandThreads / 32, band_kernel<R, false>, band_kernel<R, true>, 0, nullptr}
 #define VS_QUAD(R, WARPS, MINB)                                                                          \
     {SHAPE_QUAD, R, WARPS, quad_kernel<R, WARPS, MINB, 0, false>, nullptr, 0, quad_kernel<R, WARPS, MINB, 0, true>}
+#define VS_QUAD2(R, WARPS, MINB, NC) \
+    {SHAPE_QUAD2, R, WARPS, nullptr, nullptr, 0, quad2_kernel<R, WARPS, MINB, NC>, NC}
 #define VS_QPIPE(R, WARPS, MINB, ST)                                                                     \
     {SHAPE_QUAD, R, WARPS, quad_kernel<R, WARPS, MINB, ST, false>, nullptr, ST,                          \
      quad_kernel<R, WARPS, MINB, ST, true>}
@@ -1103,7 +1378,11 @@ const ShapeEntry kShapes[] = {
     VS_QUAD(16, 2, 8),  VS_QUAD(2, 2, 8),   VS_QUAD(8, 8, 2),   VS_QUAD(32, 4, 4),
     VS_QPIPE(16, 4, 4, 4), VS_QPIPE(32, 4, 4, 4), VS_QPIPE(16, 2, 8, 4), VS_QPIPE(32, 2, 8, 4),
     VS_QPIPE(16, 4, 2, 6), VS_QPIPE(32, 4, 2, 6), VS_QPIPE(8, 4, 4, 4), VS_QPIPE(48, 4, 4, 4),
+    VS_QUAD2(16, 2, 4, 4), VS_QUAD2(32, 2, 4, 4), VS_QUAD2(16, 4, 4, 2), VS_QUAD2(24, 4, 4, 2),
+    VS_QUAD2(32, 4, 4, 2), VS_QUAD2(32, 2, 8, 2), VS_QUAD2(48, 4, 4, 2), VS_QUAD2(24, 2, 8, 2),
+    VS_QUAD2(32, 8, 2, 2), VS_QUAD2(40, 4, 4, 2),
 };
+#undef VS_QUAD2
 #undef VS_STRIP
 #undef VS_BAND
 #undef VS_QUAD
@@ -1116,8 +1395,11 @@ int tile_shape_count() { return kNumShapes; }
 
 TileShape tile_shape(int i) {
     const ShapeEntry& e = kShapes[i];
-    return {e.rows, e.kind == SHAPE_STRIP ? kStripCommit : (e.kind == SHAPE_QUAD ? kQuadCommit : 0), e.warps,
-            e.kind};
+    const int cols = e.kind == SHAPE_STRIP ? kStripCommit
+                     : e.kind == SHAPE_BAND ? 0
+                     : e.kind == SHAPE_QUAD2 ? 30 * e.lane_cols
+                                             : kQuadCommit;
+    return {e.rows, cols, e.warps, e.kind, e.kind == SHAPE_QUAD2 ? e.lane_cols : 4};
 }
 
 size_t shape_smem_bytes(int shape, int max_pitch) {
@@ -1153,7 +1435,7 @@ cudaError_t launch_step(int shape, bool wall, bool fast, const TubeDev* tubes, c
         fn<<<ntiles, kBandThreads, band_smem_bytes(e.rows, max_pitch), stream>>>(tubes, tiles, ntiles, rs, local);
     } else {
         const int wpb = e.warps;
-        const size_t smem = e.kind == SHAPE_QUAD ? (size_t)wpb * quad_warp_smem(e.stages) : 0;
+        const size_t smem = e.kind == SHAPE_QUAD ? (size_t)wpb * quad_warp_smem(e.stages) : 0;   // QUAD2: none
         fn<<<(ntiles + wpb - 1) / wpb, wpb * 32, smem, stream>>>(tubes, tiles, ntiles, rs, local);
     }
     return cudaGetLastError();
@@ -1182,6 +1464,18 @@ cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* til
         quad_kernel<16, 4, 4, 0, true, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else
         return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance2(RunState* rs, int k, int toggle, cudaStream_t stream) {
+    advance2_kernel<<<1, 1, 0, stream>>>(rs, k, toggle);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_back(const TubeDev* tubes, int ntubes, int max_plane_cells, const RunState* rs,
+                             cudaStream_t stream) {
+    const dim3 grid((max_plane_cells + 255) / 256, ntubes);
+    copy_back_kernel<<<grid, 256, 0, stream>>>(tubes, rs);
     return cudaGetLastError();
 }
 

@@ -155,6 +155,7 @@ def load_library(path: os.PathLike | None = None) -> C.CDLL:
         "vs_batch_autotune": (C.c_int, [C.c_void_p, C.c_int64, i32p, fp]),
         "vs_tile_shape_count": (C.c_int, []),
         "vs_tile_shape": (C.c_int, [C.c_int32, i32p, i32p]),
+        "vs_tile_shape_steps": (C.c_int, [C.c_int32, i32p]),
         "vs_batch_destroy": (None, [C.c_void_p]),
         "vs_batch_set_maps": (C.c_int, [C.c_void_p, C.c_int32, fp, fp, fp, C.c_float]),
         "vs_batch_forward_ckpt": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, fp]),

@@ -242,3 +242,12 @@ def tile_shapes() -> list[tuple[int, int]]:
         check(lib, lib.vs_tile_shape(i, C.byref(r), C.byref(c)), "vs_tile_shape")
         out.append((r.value, c.value))
     return out
+
+
+def tile_shape_steps(index: int) -> int:
+    """Time steps one launch of tile shape `index` advances (1, or 2 for the
+    two-step shapes)."""
+    lib = load_library()
+    k = C.c_int32()
+    check(lib, lib.vs_tile_shape_steps(index, C.byref(k)), "vs_tile_shape_steps")
+    return k.value
