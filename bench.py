@@ -78,7 +78,7 @@ def profiled_traffic(cells: int, shape: int, fast: int):
     """DRAM bytes (read + write) per step-kernel launch from the committed ncu summary of the
     same kernel (launch shape and arithmetic) on this same workload (same interior cell
     count); else None."""
-    for name in ("quad_kernel_fast_batch256.json", "strip_kernel_batch256.json"):
+    for name in ("quad2_kernel_fast_batch256.json", "quad_kernel_fast_batch256.json", "strip_kernel_batch256.json"):
         f = REPO / "profiles" / name
         if not f.exists():
             continue

@@ -59,6 +59,9 @@ def test_tile_shapes_listed():
     shapes = V.tile_shapes()
     assert len(shapes) >= 4
     assert all(r > 0 and c % 30 == 0 for r, c in shapes)     # strips commit 30 columns per warp
+    steps = [V.tile_shape_steps(i) for i in range(len(shapes))]
+    assert set(steps) == {1, 2} and steps.count(2) >= 8     # single-step and two-step shapes
+    assert V.load_library().vs_tile_shape_steps(len(shapes), None) == 1
 
 
 def test_device_entry_points_fail_loudly_without_gpu():

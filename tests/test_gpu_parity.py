@@ -89,6 +89,10 @@ def test_every_tile_shape_gives_the_same_bits(cuda_ok):
     b = V.Batch(ps, gs)
     ref = None
     for k in range(len(V.tile_shapes())):
+        if V.tile_shape_steps(k) == 2:
+            with pytest.raises(V.VsError):      # the two-step shapes are fast_math only
+                b.set_tile(k)
+            continue
         b.reset()
         b.set_tile(k)
         tr = b.run(300)
