@@ -287,6 +287,14 @@ Tile* make_tiles(vs_batch* b, int shape, int* n) {
             }
         }
     }
+    if (ts.kind == SHAPE_QUAD2) {
+        // tallest strips first: the last strips to start are the short ones
+        auto height = [&](const Tile& t) {
+            return std::min(t.r0 + ts.rows - 1, b->grids[(size_t)t.tube].H - 2) - t.r0 + 1;
+        };
+        std::stable_sort(tiles.begin(), tiles.end(),
+                         [&](const Tile& x, const Tile& y) { return height(x) > height(y); });
+    }
     Tile* d = nullptr;
     ck(cudaMalloc(&d, tiles.size() * sizeof(Tile)), "cudaMalloc(tiles)");
     const cudaError_t e = cudaMemcpy(d, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice);
