@@ -369,7 +369,7 @@ void ensure_graph(vs_batch* b) {
 //   zi = mS zinv n x_in Nin rden; ce = ew mS rden; g = 1 / (1 + sigma_c)
 // (g = 0 on the no-pressure cells of a Dirichlet mouth).  Index 0 is plain
 // air.  Ring cells keep index 0 (they are never computed).
-constexpr int kMaxDescriptors = 256;
+constexpr int kMaxDescriptors = kDescEntries;
 constexpr size_t kDescTableBytes = 2 * kMaxDescriptors * 4 * sizeof(float);
 
 void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vector<float>& ta,
@@ -540,7 +540,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         if (b->fast) {
             t.desc = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
             t.desc_a = (const float4*)next(kDescTableBytes / 2);
-            t.desc_b = (const float4*)next(kDescTableBytes / 2);
+            t.desc_b = (const float4*)next(kDescTableBytes / 2);    // desc_a + kDescEntries
         }
         t.H = g.H; t.W = g.W; t.pitch = g.pitch;
         t.plane = (int64_t)(pl / sizeof(float));

@@ -51,7 +51,7 @@ struct TubeDev {
     // V' = al (V - bcoef (P'n - P'c)) + zo P'c - zi P'n + ce exeV (x and y)
     const uint8_t* desc;
     const float4* desc_a;
-    const float4* desc_b;
+    const float4* desc_b;  // = desc_a + kDescEntries (the two tables are contiguous)
     float* X;             // fast_math: a third P, Vx, Vy set (`plane` apart) for the two-step kernels
     TmmConsts tmmc;
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
@@ -65,6 +65,9 @@ struct TubeDev {
 
 // Mutable run bookkeeping kept in device memory so that CUDA graphs captured
 // once can be replayed for any run length.
+// Entries of each fast_math descriptor table (desc_a, desc_b).
+constexpr int kDescEntries = 256;
+
 struct RunState {
     int64_t step;         // global step of the next launch with local index 0
     int64_t run_start;    // global step that lands in trace column 0

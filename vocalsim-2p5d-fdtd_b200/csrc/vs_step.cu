@@ -536,10 +536,31 @@ __device__ __forceinline__ bool mbar_wait_parity_bounded(uint64_t* bar, uint32_t
 // sets RunState::error, and the warp waits (bounded) for its remaining
 // copies before it leaves.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void ld4(float (&d)[4], const float* p) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+// Streamed rows are read once per warp: they bypass L1 (no_allocate), which
+// keeps the descriptor tables resident there.
+template <int NC>
+__device__ __forceinline__ void ldn(float (&d)[NC], const float* p) {
+    if constexpr (NC == 4) {
+        asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+            : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3]) : "l"(p));
+    } else {
+        asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(d[0]), "=f"(d[1]) : "l"(p));
+    }
 }
+
+__device__ __forceinline__ uint32_t ld_desc2(const uint8_t* p) {
+    unsigned short v;
+    asm("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_desc4(const uint8_t* p) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void ld4(float (&d)[4], const float* p) { ldn<4>(d, p); }
 
 __device__ __forceinline__ void lds4(float (&d)[4], const unsigned char* p) {
     const float4 v = *reinterpret_cast<const float4*>(p);
@@ -697,7 +718,7 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
         for (int q = 0; q < 4; ++q) ux_c[q] = fmul(vx_c[q], t4[q]);
         ld4(p_c, Pin + o);
         ld4(dp_c, dPp + o);
-        k_c = __ldg(reinterpret_cast<const unsigned int*>(code + o));
+        k_c = ld_desc4(code + o);
         ld4(vy_c, Vyin + o);
         ld4(t4, dYp + o);
     }
@@ -747,7 +768,7 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
             ld4(dx_1, dXp + o1);
             ld4(p_1, Pin + o1);
             ld4(dp_1, dPp + o1);
-            k_1 = __ldg(reinterpret_cast<const unsigned int*>(code + o1));
+            k_1 = ld_desc4(code + o1);
             if (r + 2 <= H - 1) {
                 ld4(vy_2, Vyin + o1 + pitch);
                 ld4(dy_2, dYp + o1 + pitch);
@@ -912,16 +933,7 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 // Tile masks classify the extended region (rows from r0-2 / r0-1, columns
 // c0 + NC/2 .. c0 + 32 NC - NC/2 - 1): bit j of v_generic = row r0-1+j.
 // ---------------------------------------------------------------------------
-template <int NC>
-__device__ __forceinline__ void ldn(float (&d)[NC], const float* p) {
-    if constexpr (NC == 4) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-    } else {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
-        d[0] = v.x; d[1] = v.y;
-    }
-}
+
 
 template <int NC>
 __device__ __forceinline__ void stn(float* p, const float (&v)[NC], unsigned mask) {
@@ -970,11 +982,13 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     const float* __restrict__ dYp = dPp + 2 * pl;
     const uint8_t* __restrict__ desc = T->desc;
     const float4* __restrict__ ta = T->desc_a;
-    const float4* __restrict__ tb = T->desc_b;
+    // desc_b follows desc_a (kDescEntries entries each): one base, immediate offsets
     const float K1 = T->K1, bco = T->bcoef;
     const int lis_y = T->lis_y, lis_q = T->lis_x - x0;
     const bool lis_here = lis_q >= 0 && lis_q < NC && ((commit_m >> lis_q) & 1u);
-    const uint64_t vgen = it.v_generic;
+    // bit 1 of gm = velocity class of step n's row r (v_generic bit j-1),
+    // bit 0 = that of step n+1's row r-1 (bit j-2); shifted once per row
+    uint64_t gm = it.v_generic << 2;
     float exe1 = 0.0f, exe2 = 0.0f;
     if (it.has_exc) {
         exe1 = n < T->src_len ? T->src[n] : 0.0f;
@@ -995,8 +1009,8 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     auto ldk = [&](int row) -> uint32_t {
         if (row < 0 || row > H - 1) return 0u;
         const uint8_t* p = desc + (int64_t)row * pitch + x0;
-        if constexpr (NC == 4) return __ldg(reinterpret_cast<const unsigned int*>(p));
-        else return (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(p));
+        if constexpr (NC == 4) return ld_desc4(p);
+        else return ld_desc2(p);
     };
 
     // step-n pipeline at row r: state and maps of row r, Vy dY of row r+1
@@ -1052,7 +1066,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         // ---- step n, velocity of row r (FDTDEngineCPU.cpp:364-410)
         const bool vrow1 = r >= r0 - 1 && prow1;
         const unsigned vm1 = vrow1 ? int_m : 0u;
-        const bool gen1 = j >= 1 && ((vgen >> (j - 1)) & 1);
+        const bool gen1 = (gm & 2u) != 0;
         float v1x[NC], v1y[NC], u1[NC], w1[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
@@ -1060,7 +1074,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             float vx = fmul(fsub(vx_c[q], fmul(bco, fsub(pr, pn1[q]))), da[q].x);
             float vy = fmul(fsub(vy_c[q], fmul(bco, fsub(pn1_p[q], pn1[q]))), da[q].y);
             if (gen1) {
-                const float4 db = __ldg(tb + code_byte(k_c, q));
+                const float4 db = __ldg(ta + (kDescEntries + code_byte(k_c, q)));
                 vx = __fmaf_rn(da[q].w, exe1, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn1[q], vx)));
                 vy = __fmaf_rn(-db.w, pn1_p[q], __fmaf_rn(db.z, pn1[q], vy));
             }
@@ -1094,7 +1108,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             }
             const float p2_r = __shfl_down_sync(kFull, pn2[0], 1);
             if (s >= r0 && s <= rlast) {
-                const bool gen2 = ((vgen >> (j - 2)) & 1);
+                const bool gen2 = (gm & 1u) != 0;
                 float vx2[NC], vy2[NC];
 #pragma unroll
                 for (int q = 0; q < NC; ++q) {
@@ -1102,7 +1116,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                     float vx = fmul(fsub(v1x_p[q], fmul(bco, fsub(pr, pn2[q]))), da_p[q].x);
                     float vy = fmul(fsub(v1y_p[q], fmul(bco, fsub(pn2_p[q], pn2[q]))), da_p[q].y);
                     if (gen2) {
-                        const float4 db = __ldg(tb + code_byte(k_p, q));
+                        const float4 db = __ldg(ta + (kDescEntries + code_byte(k_p, q)));
                         vx = __fmaf_rn(da_p[q].w, exe2, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn2[q], vx)));
                         vy = __fmaf_rn(-db.w, pn2_p[q], __fmaf_rn(db.z, pn2[q], vy));
                     }
@@ -1144,6 +1158,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         }
         k_p = k_c;
         k_c = k_1;
+        gm >>= 1;
     }
 }
 
