@@ -246,8 +246,8 @@ int vs_tile_shape_count(void);
 int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
 
 /* Time steps one kernel launch of shape i advances: 1, or 2 for the two-step
- * shapes (fast_math batches without the two-mass source or the coupled wall;
- * they keep a third set of state planes beside the two parity sets). */
+ * shapes (fast_math batches without the coupled wall; they keep a third set
+ * of state planes and a third two-mass state slot beside the two parity sets). */
 int vs_tile_shape_steps(int32_t i, int32_t* steps_per_launch);
 
 void vs_batch_destroy(vs_batch* b);

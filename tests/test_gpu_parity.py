@@ -199,16 +199,19 @@ def test_fast_math_shapes_agree_and_batch_rows_equal_single(cuda_ok):
 
 
 def test_two_step_shapes_equal_single_step(cuda_ok):
-    """Without the two-mass source a fast_math batch also offers the two-step
-    shapes (two time steps per launch, the state alternating with a third
-    buffer set).  Runs of odd and even lengths, in and out of the captured
-    128-step chunks, must give the traces of the single-step shapes exactly."""
-    n = 4
+    """fast_math batches also offer the two-step shapes (two time steps per
+    launch, the state and the two-mass state alternating with a third set).
+    Runs of odd and even lengths, in and out of the captured 128-step chunks,
+    with table and two-mass (float and double) sources, must give the traces
+    of the single-step shapes exactly."""
+    n = 6
     tubes = [S.batch_tube(i)[:2] for i in range(n)]
     kws = [dict(cross_sectional_shape=2, fast_math=1),
            dict(cross_sectional_shape=2, fast_math=1, mouth_radiation_cond=1),
            dict(cross_sectional_shape=1, fast_math=1, source_type=0),
-           dict(cross_sectional_shape=2, fast_math=1, srate_mul=2)]
+           dict(cross_sectional_shape=2, fast_math=1, srate_mul=2),
+           dict(cross_sectional_shape=2, fast_math=1, source_type=2, tmm_ps_pa=800.0),
+           dict(cross_sectional_shape=2, fast_math=1, source_type=2, tmm_ps_pa=800.0, tmm_f64=1)]
     b = V.Batch([V.params(**k) for k in kws], [V.Geometry(L, A) for L, A in tubes])
     segments = [1, 2, 3, 128, 131, 257, 64]
     ref = None

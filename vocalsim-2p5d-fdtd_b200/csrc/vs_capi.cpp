@@ -101,7 +101,8 @@ struct vs_batch {
     Tile* d_hist_tiles = nullptr;
     int n_hist_tiles = 0;
     Tile* d_odd_tiles = nullptr;           // single-step tiles beside a two-step shape
-    char* x_mem = nullptr;                 // third state set of the two-step shapes (TubeDev::X)
+    char* x_mem = nullptr;                 // third state set of the two-step shapes (TubeDev::X, tmm_x)
+    size_t x_bytes = 0;
     int n_odd_tiles = 0;
     int odd_shape = -1;
     // section depth model (vs_batch_set_sections): per-tube descriptors and buffers
@@ -159,13 +160,15 @@ namespace {
 // Default launch shapes when no autotune ran: 16-row strips with 4 warps per
 // CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells;
 // with fast_math the quad strips of the same heights (16 rows x 4 warps,
-// 2 rows x 2 warps), and for large fast_math batches without the two-mass
-// source the two-step strips (32 rows x 4 warps of 64 columns).
+// 2 rows x 2 warps), and for fast_math batches without the two-mass source
+// the two-step strips of 64 columns (32 rows x 4 warps; 2 rows x 2 warps
+// below kSmallGridCells).
 constexpr int kDefaultShape = 1;
 constexpr int kSmallShape = 8;
 constexpr int kFastShape = 17;
 constexpr int kFastSmallShape = 21;
 constexpr int kTwoStepShape = 36;
+constexpr int kTwoStepSmallShape = 42;
 constexpr int64_t kSmallGridCells = 200000;
 
 int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
@@ -214,17 +217,11 @@ size_t smem_optin_limit(int device) {
     return (size_t)v;
 }
 
-bool any_tmm(const vs_batch* b) {
-    for (const TubeGrid& g : b->grids)
-        if (g.tmm) return true;
-    return false;
-}
-
 bool shape_fits(const vs_batch* b, int shape) {
     const int kind = tile_shape(shape).kind;
     if (b->wall && (kind == SHAPE_QUAD || kind == SHAPE_QUAD2)) return false;   // no wall-oscillator variant
-    // two-step kernels: fast_math with table sources only
-    if (kind == SHAPE_QUAD2 && (!b->fast || any_tmm(b))) return false;
+    // two-step kernels: fast_math only
+    if (kind == SHAPE_QUAD2 && !b->fast) return false;
     if (b->fast && !shape_has_fast(shape)) return false;
     return shape_smem_bytes(shape, b->max_pitch) <= smem_optin_limit(b->device);
 }
@@ -242,8 +239,8 @@ int single_step_shape(const vs_batch* b) {
 int default_shape(const vs_batch* b) {
     int64_t cells = 0;
     for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
-    if (cells >= kSmallGridCells && tile_shape(kTwoStepShape).kind == SHAPE_QUAD2 && shape_fits(b, kTwoStepShape))
-        return kTwoStepShape;
+    const int two = cells >= kSmallGridCells ? kTwoStepShape : kTwoStepSmallShape;
+    if (tile_shape(two).kind == SHAPE_QUAD2 && shape_fits(b, two)) return two;
     return single_step_shape(b);
 }
 
@@ -323,15 +320,20 @@ void build_tiles(vs_batch* b, int shape) {
         // and alternates the state with a third set of planes (zero ring
         // cells; kGuard bytes around it for the strips' edge reads)
         if (!b->x_mem) {
+            const size_t slots = align_up(sizeof(TmmState)) + align_up(sizeof(TmmState64));
             size_t total = kGuard;
-            for (const TubeDev& t : b->h_tubes) total += 3 * (size_t)t.plane * sizeof(float);
+            for (const TubeDev& t : b->h_tubes) total += 3 * (size_t)t.plane * sizeof(float) + slots;
             total += kGuard;
             ck(cudaMalloc(&b->x_mem, total), "cudaMalloc(third state set)");
             ck(cudaMemset(b->x_mem, 0, total), "zero third state set");
+            b->x_bytes = total;
             size_t off = kGuard;
             for (TubeDev& t : b->h_tubes) {
                 t.X = reinterpret_cast<float*>(b->x_mem + off);
                 off += 3 * (size_t)t.plane * sizeof(float);
+                t.tmm_x = reinterpret_cast<TmmState*>(b->x_mem + off);
+                t.tmm64_x = reinterpret_cast<TmmState64*>(b->x_mem + off + align_up(sizeof(TmmState)));
+                off += slots;
             }
             ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev),
                           cudaMemcpyHostToDevice),
@@ -466,13 +468,10 @@ void upload_static(vs_batch* b) {
 
 void reset_state(vs_batch* b) {
     // fields, wall state and the two-mass state all restart at zero
-    for (size_t i = 0; i < b->grids.size(); ++i) {
+    for (size_t i = 0; i < b->grids.size(); ++i)
         ck(cudaMemsetAsync(b->state_base[i], 0, b->state_bytes[i], b->stream), "zero state");
-        // the two-step kernels' third set: its ring cells must read as zero
-        if (b->h_tubes[i].X)
-            ck(cudaMemsetAsync(b->h_tubes[i].X, 0, 3 * (size_t)b->h_tubes[i].plane * sizeof(float), b->stream),
-               "zero third state set");
-    }
+    // the two-step kernels' third set: its ring cells must read as zero
+    if (b->x_mem) ck(cudaMemsetAsync(b->x_mem, 0, b->x_bytes, b->stream), "zero third state set");
     RunState rs{};
     ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "reset run state");
     ck(cudaStreamSynchronize(b->stream), "reset sync");

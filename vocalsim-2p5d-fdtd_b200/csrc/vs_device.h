@@ -53,6 +53,8 @@ struct TubeDev {
     const float4* desc_a;
     const float4* desc_b;  // = desc_a + kDescEntries (the two tables are contiguous)
     float* X;             // fast_math: a third P, Vx, Vy set (`plane` apart) for the two-step kernels
+    TmmState* tmm_x;      // the two-step kernels' third two-mass state slot (float and double model)
+    TmmState64* tmm64_x;
     TmmConsts tmmc;
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
     // state history for the adjoint's recomputation (strip kernel with

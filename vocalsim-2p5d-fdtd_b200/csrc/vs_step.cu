@@ -222,6 +222,26 @@ __device__ __noinline__ float glottal_step(const TubeDev* T, int par, float p1, 
     return e;
 }
 
+// Two-mass steps n and n+1 for the two-step kernels: the state of step n is
+// in the parity slot (from_x = false) or the third slot, that of step n+2
+// goes to the other one (stored by the owning strip only).
+__device__ __noinline__ float2 glottal_two_steps(const TubeDev* T, int par, bool from_x, float p1, float p2,
+                                                 bool store) {
+    float2 e;
+    if (T->flags & TUBE_TMM64) {
+        TmmState64 s = from_x ? *T->tmm64_x : T->tmm64[par];
+        e.x = tmm_step64(T->tmmd, s, p1);
+        e.y = tmm_step64(T->tmmd, s, p2);
+        if (store) *(from_x ? &T->tmm64[par] : T->tmm64_x) = s;
+    } else {
+        TmmState s = from_x ? *T->tmm_x : T->tmm[par];
+        e.x = tmm_step(T->tmmc, s, p1);
+        e.y = tmm_step(T->tmmc, s, p2);
+        if (store) *(from_x ? &T->tmm[par] : T->tmm_x) = s;
+    }
+    return e;
+}
+
 // a / b for b > 0 with the signed zero returned directly when a is zero:
 // the same value as the division, without sending the zero fields of a cold
 // start through the slow path of the IEEE divide.
@@ -990,11 +1010,32 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     // bit 0 = that of step n+1's row r-1 (bit j-2); shifted once per row
     uint64_t gm = it.v_generic << 2;
     float exe1 = 0.0f, exe2 = 0.0f;
-    if (it.has_exc) {
-        exe1 = n < T->src_len ? T->src[n] : 0.0f;
-        exe2 = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
-    }
     const int rlast = min(r0 + TR - 1, H - 2);
+    if (it.has_exc) {
+        if (T->flags & TUBE_TMM) {
+            // two-mass source: exe of step n from P(n) at the glottis cell, that
+            // of step n+1 from P'(n) there, evaluated from the input planes
+            // with the strip's own arithmetic; the strip that commits the
+            // cell stores the state of step n+2 in the other slot
+            if (lane == 0) {
+                const int64_t e = (int64_t)T->exc_y * pitch + T->exc_x;
+                const float p1 = Pin[e];
+                const float ks = fmul(K1, fadd(fsub(fmul(Vxin[e], dXp[e]), fmul(Vxin[e - 1], dXp[e - 1])),
+                                               fsub(fmul(Vyin[e], dYp[e]), fmul(Vyin[e + pitch], dYp[e + pitch]))));
+                const float p2 = fmul(__fmaf_rn(-ks, rcp_approx(dPp[e]), p1), __ldg(ta + desc[e]).z);
+                const bool owner = T->exc_y >= r0 && T->exc_y <= rlast && T->exc_x >= c0 + NC &&
+                                   T->exc_x < c0 + 31 * NC;
+                const float2 ee = glottal_two_steps(T, par, from_x, p1, p2, owner);
+                exe1 = ee.x;
+                exe2 = ee.y;
+            }
+            exe1 = __shfl_sync(kFull, exe1, 0);
+            exe2 = __shfl_sync(kFull, exe2, 0);
+        } else {
+            exe1 = n < T->src_len ? T->src[n] : 0.0f;
+            exe2 = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+        }
+    }
     float* __restrict__ trace = rs->trace + (int64_t)it.tube * rs->trace_stride + (n - rs->run_start);
 
     // rows outside the frame read as zeros (they only feed values that are not used)
@@ -1175,6 +1216,10 @@ __global__ void copy_back_kernel(const TubeDev* __restrict__ tubes, const RunSta
     B[i] = T.X[i];
     B[2 * pl + i] = T.X[pl + i];
     B[4 * pl + i] = T.X[2 * pl + i];
+    if (i == 0 && (T.flags & TUBE_TMM)) {
+        T.tmm[par] = *T.tmm_x;
+        T.tmm64[par] = *T.tmm64_x;
+    }
 }
 
 __global__ void advance2_kernel(RunState* rs, int k, int toggle) {
@@ -1395,7 +1440,8 @@ const ShapeEntry kShapes[] = {
     VS_QPIPE(16, 4, 2, 6), VS_QPIPE(32, 4, 2, 6), VS_QPIPE(8, 4, 4, 4), VS_QPIPE(48, 4, 4, 4),
     VS_QUAD2(16, 2, 4, 4), VS_QUAD2(32, 2, 4, 4), VS_QUAD2(16, 4, 4, 2), VS_QUAD2(24, 4, 4, 2),
     VS_QUAD2(32, 4, 4, 2), VS_QUAD2(32, 2, 8, 2), VS_QUAD2(48, 4, 4, 2), VS_QUAD2(24, 2, 8, 2),
-    VS_QUAD2(32, 8, 2, 2), VS_QUAD2(40, 4, 4, 2),
+    VS_QUAD2(32, 8, 2, 2), VS_QUAD2(40, 4, 4, 2), VS_QUAD2(2, 2, 8, 2), VS_QUAD2(4, 2, 8, 2),
+    VS_QUAD2(8, 2, 8, 2), VS_QUAD2(4, 1, 16, 2),
 };
 #undef VS_QUAD2
 #undef VS_STRIP
