@@ -10,6 +10,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <mutex>
+#include <thread>
 #include <functional>
 #include <cmath>
 #include <cstring>
@@ -49,6 +53,36 @@ constexpr size_t kAlign = 256;
 constexpr size_t kGuard = 1024;  // bytes of slack around the tube planes of an arena
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// fn(i) for i in [0, n) on up to hardware_concurrency host threads (host
+// work only: map building, source tables, staging images); the first
+// exception thrown by a call is rethrown here after every thread joined.
+void parallel_for(size_t n, const std::function<void(size_t)>& fn) {
+    size_t nt = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+    nt = std::min<size_t>(nt, 64);
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::exception_ptr err;
+    std::mutex m;
+    std::vector<std::thread> pool;
+    pool.reserve(nt);
+    for (size_t t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (size_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
+                try {
+                    fn(i);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lock(m);
+                    if (!err) err = std::current_exception();
+                }
+            }
+        });
+    for (std::thread& t : pool) t.join();
+    if (err) std::rethrow_exception(err);
+}
 
 }  // namespace
 }  // namespace vsb
@@ -179,19 +213,20 @@ void upload_sources(vs_batch* b, int64_t need) {
     for (size_t i = 0; i < b->grids.size(); ++i)
         if (!b->grids[i].tmm && b->src_len[i] < need) ok = false;
     if (ok && b->src_arena) return;
+    parallel_for(b->grids.size(), [&](size_t i) {
+        TubeGrid& g = b->grids[i];
+        if (g.tmm || (int64_t)g.source.size() >= need) return;
+        vs_params p;
+        std::memcpy(&p, &g.src_params, sizeof(p));
+        build_source(&p, g.dt, need, g.source);
+    });
     size_t total = 0;
     std::vector<size_t> off(b->grids.size(), 0);
     for (size_t i = 0; i < b->grids.size(); ++i) {
-        TubeGrid& g = b->grids[i];
+        const TubeGrid& g = b->grids[i];
         if (g.tmm) continue;
-        const int64_t len = std::max<int64_t>(need, (int64_t)g.source.size());
-        if ((int64_t)g.source.size() < len) {
-            vs_params p;
-            std::memcpy(&p, &g.src_params, sizeof(p));
-            build_source(&p, g.dt, len, g.source);
-        }
         off[i] = total;
-        total += align_up((size_t)len * sizeof(float));
+        total += align_up(g.source.size() * sizeof(float));
     }
     if (b->src_arena) { cudaFree(b->src_arena); b->src_arena = nullptr; }
     if (total) ck(cudaMalloc(&b->src_arena, total), "cudaMalloc(source tables)");
@@ -249,8 +284,9 @@ Tile* make_tiles(vs_batch* b, int shape, int* n) {
     const TileShape ts = tile_shape(shape);
     if (!shape_fits(b, shape)) throw VsFailure{VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)"};
     ck(prepare_shape(shape, b->max_pitch), "kernel attributes");
-    std::vector<Tile> tiles;
-    for (size_t i = 0; i < b->grids.size(); ++i) {
+    std::vector<std::vector<Tile>> per_tube(b->grids.size());
+    parallel_for(b->grids.size(), [&](size_t i) {
+        std::vector<Tile>& tiles = per_tube[i];
         const TubeGrid& g = b->grids[i];
         auto code_at = [&g](int r, int c) { return (int)g.code[(size_t)r * g.pitch + c]; };
         for (int r0 = 1; r0 <= g.H - 2; r0 += ts.rows) {
@@ -283,7 +319,9 @@ Tile* make_tiles(vs_batch* b, int shape, int* n) {
                 tiles.push_back(t);
             }
         }
-    }
+    });
+    std::vector<Tile> tiles;
+    for (const std::vector<Tile>& v : per_tube) tiles.insert(tiles.end(), v.begin(), v.end());
     if (ts.kind == SHAPE_QUAD2) {
         // tallest strips first: the last strips to start are the short ones
         auto height = [&](const Tile& t) {
@@ -462,8 +500,41 @@ void upload_static_tube(vs_batch* b, size_t i) {
     }
 }
 
+// Every tube's read-only block (depth planes, codes, fast_math descriptors
+// and tables, from TubeDev::dP on, as laid out in the arena), staged on the
+// host in parallel and copied with one transfer per tube.
 void upload_static(vs_batch* b) {
-    for (size_t i = 0; i < b->grids.size(); ++i) upload_static_tube(b, i);
+    const size_t n = b->grids.size();
+    std::vector<std::vector<char>> img(n);
+    parallel_for(n, [&](size_t i) {
+        const TubeGrid& g = b->grids[i];
+        const TubeDev& t = b->h_tubes[i];
+        const char* base = reinterpret_cast<const char*>(t.dP);
+        auto at = [&](const void* p) { return (size_t)(reinterpret_cast<const char*>(p) - base); };
+        const size_t end = b->fast ? at(t.desc_b) + kDescTableBytes / 2 : at(t.code) + align_up((size_t)g.H * g.pitch);
+        std::vector<char>& m = img[i];
+        m.assign(end, 0);
+        auto plane = [&](const std::vector<float>& src, const float* dst) {
+            float* d = reinterpret_cast<float*>(m.data() + at(dst));
+            for (int r = 0; r < g.H; ++r)
+                std::memcpy(d + (size_t)r * g.pitch, &src[(size_t)r * g.W], g.W * sizeof(float));
+        };
+        plane(g.dP, t.dP);
+        plane(g.dX, t.dX);
+        plane(g.dY, t.dY);
+        std::memcpy(m.data() + at(t.code), g.code.data(), g.code.size());
+        if (b->fast) {
+            std::vector<uint8_t> desc;
+            std::vector<float> ta, tb;
+            build_descriptors(g, desc, ta, tb);
+            std::memcpy(m.data() + at(t.desc), desc.data(), desc.size());
+            std::memcpy(m.data() + at(t.desc_a), ta.data(), ta.size() * sizeof(float));
+            std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
+        }
+    });
+    for (size_t i = 0; i < n; ++i)
+        ck(cudaMemcpy((void*)b->h_tubes[i].dP, img[i].data(), img[i].size(), cudaMemcpyHostToDevice),
+           "upload maps");
 }
 
 void reset_state(vs_batch* b) {
@@ -481,10 +552,10 @@ void reset_state(vs_batch* b) {
 void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_batch* b) {
     ck(cudaGetDevice(&b->device), "cudaGetDevice");
     b->grids.resize(n);
-    for (int i = 0; i < n; ++i) {
+    parallel_for((size_t)n, [&](size_t i) {
         build_tube(&params[i], geoms ? &geoms[i] : nullptr, b->grids[i], 0);
         std::memcpy(&b->grids[i].src_params, &params[i], sizeof(vs_params));
-    }
+    });
     // arena layout: per tube, planes of H*pitch floats (+ codes) + two-mass
     // state, with kGuard bytes before the first and after the last tube: the
     // step kernel reads one element before and up to 29 after a plane
