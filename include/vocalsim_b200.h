@@ -264,6 +264,20 @@ void vs_batch_destroy(vs_batch* b);
 int vs_formants(const float* traces, int32_t n_traces, int64_t n, double fs, int32_t num_formants, double* out,
                 void* cuda_stream);
 
+/* WAV samples of listener traces on the device, as results/generate_audio.py
+ * (lines 14-42) makes them from recorded-pressure.txt: each trace divided by
+ * its largest |P| and clipped to [-1, 1]; for srate_mul > 1 low-passed by the
+ * 2nd-order Butterworth filter at 5050 Hz (vs_audio_filter) with
+ * scipy.signal.lfilter's direct form II transposed recursion in double, and
+ * every srate_mul-th sample kept.  traces: device, n_traces x n floats; out:
+ * device, n_traces x ceil(n / srate_mul) floats (the 44100 Hz WAV samples).
+ * Returns after the work on cuda_stream (a cudaStream_t; NULL = default). */
+int vs_audio(const float* traces, int32_t n_traces, int64_t n, int32_t srate_mul, float* out, void* cuda_stream);
+
+/* The filter vs_audio applies for srate_mul (scipy.signal.butter(2, 5050 /
+ * (44100 srate_mul / 2)) coefficients, a[0] = 1); host only. */
+int vs_audio_filter(int32_t srate_mul, double* b3, double* a3);
+
 /* ---- gradients: checkpointed forward + reverse-time discrete adjoint -----
  * No counterpart in the reference (it has no differentiation).  The adjoint
  * covers table sources (Gaussian, sine) and the two-mass source (whose flow

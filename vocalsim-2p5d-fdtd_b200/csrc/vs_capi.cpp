@@ -1376,6 +1376,21 @@ int vs_formants(const float* traces, int32_t n_traces, int64_t n, double fs, int
     return VS_OK;
 }
 
+int vs_audio(const float* traces, int32_t n_traces, int64_t n, int32_t srate_mul, float* out, void* cuda_stream) {
+    if (!traces || !out || n_traces < 1 || n < 1 || srate_mul < 1 || srate_mul > 64)
+        return set_error(VS_ERR_INVALID_ARG, "vs_audio arguments");
+    std::string err;
+    const int st = audio_device(traces, n_traces, n, srate_mul, out, static_cast<cudaStream_t>(cuda_stream), &err);
+    if (st != VS_OK) return set_error(st, err.c_str());
+    return VS_OK;
+}
+
+int vs_audio_filter(int32_t srate_mul, double* b3, double* a3) {
+    if (!b3 || !a3 || srate_mul < 2 || srate_mul > 64) return set_error(VS_ERR_INVALID_ARG, "vs_audio_filter arguments");
+    audio_filter(srate_mul, b3, a3);
+    return VS_OK;
+}
+
 int vs_tile_shape_count(void) { return tile_shape_count(); }
 
 int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {

@@ -287,6 +287,10 @@ cudaError_t launch_section_vjp(const SectionTube* tubes, const TubeDev* devs, co
 // Formants of ntr device traces of n samples at sampling rate fs (the
 // reference's get_formants_bw): out (device) = ntr x [bandwidth, centre,
 // level] x nf.  Synchronises `st`; returns a vs_status, err gets the text.
+// WAV samples of listener traces (vs_audio.cu).
+void audio_filter(int srate_mul, double b[3], double a[3]);
+int audio_device(const float* traces, int ntr, int64_t n, int mul, float* out, cudaStream_t st, std::string* err);
+
 int formants_device(const float* traces, int ntr, int64_t n, double fs, int nf, double* out, cudaStream_t st,
                     std::string* err);
 

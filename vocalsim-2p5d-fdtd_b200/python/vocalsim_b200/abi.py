@@ -156,6 +156,8 @@ def load_library(path: os.PathLike | None = None) -> C.CDLL:
         "vs_tile_shape_count": (C.c_int, []),
         "vs_tile_shape": (C.c_int, [C.c_int32, i32p, i32p]),
         "vs_tile_shape_steps": (C.c_int, [C.c_int32, i32p]),
+        "vs_audio": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
+        "vs_audio_filter": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "vs_batch_destroy": (None, [C.c_void_p]),
         "vs_batch_set_maps": (C.c_int, [C.c_void_p, C.c_int32, fp, fp, fp, C.c_float]),
         "vs_batch_forward_ckpt": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, fp]),
