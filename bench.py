@@ -441,6 +441,10 @@ def run_b200(args, rank, world):
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells, tile, fast),
+                     # the metric's own form: Gcell-updates/s per GPU against the one-step
+                     # roofline (37 B per cell-update moved once per step at the peak)
+                     "gcell_roofline": round(peak / BYTES_PER_CELL_UPDATE, 1),
+                     "gcell_frac": round(value / world / (peak / BYTES_PER_CELL_UPDATE), 4),
                      "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell per launch x {cells} cells / "
                              f"mean launch time {launch_ms * 1e3:.2f} us ({per_launch} time step(s) per launch); "
                              f"peak {peak_kind}"},

@@ -231,6 +231,33 @@ def test_two_step_shapes_equal_single_step(cuda_ok):
     assert np.all(np.isfinite(ref)) and np.abs(ref).max() > 0
 
 
+def test_two_step_small_and_open_frames(cuda_ok):
+    """A frame narrower than one 64-column strip (with the two-mass source), a
+    short tube with odd sizes, and the open-space frame (no tube; the source
+    cell mid-frame): the two-step shapes equal the single-step ones there too."""
+    kws = [dict(fast_math=1, source_type=2, tmm_ps_pa=800.0), dict(fast_math=1, cross_sectional_shape=2),
+           dict(fast_math=1, simulation_type=0)]
+    geoms = [V.Geometry(*S.uniform_tube(2.0, 1.2)), V.Geometry(*S.uniform_tube(4.1, 2.3)), None]
+    b = V.Batch([V.params(**k) for k in kws], geoms)
+    assert min(d["frame_w"] for d in b.dims) < 64
+    segments = [3, 130, 5]
+    ref = None
+    two = 0
+    for k in range(len(V.tile_shapes())):
+        try:
+            b.set_tile(k)
+        except V.VsError:
+            continue
+        b.reset()
+        tr = np.concatenate([b.run(m) for m in segments], axis=1)
+        two += V.tile_shape_steps(k) == 2
+        if ref is None:
+            ref = tr
+        assert np.array_equal(tr, ref), f"tile shape {k}"
+    assert two >= 10
+    assert np.all(np.isfinite(ref)) and np.all(np.abs(ref).max(axis=1) > 0)
+
+
 def test_fast_math_must_agree_within_a_batch(cuda_ok):
     L, A = S.vowel_tube(1)
     with pytest.raises(V.VsError) as e:
