@@ -317,6 +317,20 @@ __device__ __forceinline__ float rcp_approx(float x) {
 //   V_GENERIC  walls, excitation cells, admittance: the full expression
 // Every shortened path drops only operations whose operands are exact 0 / 1
 // (x*1, x+0, x/1), so values equal the full reference expression.
+// Scalar row loads of the strip kernel: read once per warp, so they bypass
+// L1 (no_allocate) and leave it to the tube descriptors and tables.
+__device__ __forceinline__ float ld1(const float* p) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ int ldcode(const uint8_t* p) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=r"(v) : "l"(p));
+    return (int)v;
+}
+
 template <int TR, int MINB, bool WALL, bool HIST = false>
 __global__ void __launch_bounds__(256, MINB)
 strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
@@ -381,14 +395,14 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     // own P' is recomputed, not committed.
     int r = r0 - 1;
     int o = r * pitch + x;
-    float vx_c = __ldg(Vxin + o);
-    float ux_c = fmul(vx_c, __ldg(dXp + o));
-    float p_c = __ldg(Pin + o), dp_c = __ldg(dPp + o);
-    int k_c = __ldg(code + o);
-    float vy_c = __ldg(Vyin + o);
-    float uy_c = fmul(vy_c, __ldg(dYp + o));
-    float vy_n = __ldg(Vyin + o + pitch);
-    float uy_n = fmul(vy_n, __ldg(dYp + o + pitch));
+    float vx_c = ld1(Vxin + o);
+    float ux_c = fmul(vx_c, ld1(dXp + o));
+    float p_c = ld1(Pin + o), dp_c = ld1(dPp + o);
+    int k_c = ldcode(code + o);
+    float vy_c = ld1(Vyin + o);
+    float uy_c = fmul(vy_c, ld1(dYp + o));
+    float vy_n = ld1(Vyin + o + pitch);
+    float uy_n = fmul(vy_n, ld1(dYp + o + pitch));
     float p_above = 0.0f;
     int k_above = VS_CELL_DEAD;
 
@@ -396,11 +410,11 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         // ---- loads for the next iterations
         const int o1 = o + pitch;
         // (read-only this step: the input planes are not the ones written)
-        const float vx_1 = __ldg(Vxin + o1), dx_1 = __ldg(dXp + o1);
-        const float p_1 = __ldg(Pin + o1), dp_1 = __ldg(dPp + o1);
-        const int k_1 = __ldg(code + o1);
+        const float vx_1 = ld1(Vxin + o1), dx_1 = ld1(dXp + o1);
+        const float p_1 = ld1(Pin + o1), dp_1 = ld1(dPp + o1);
+        const int k_1 = ldcode(code + o1);
         float vy_2 = 0.0f, dy_2 = 0.0f;
-        if (r + 2 <= H - 1) { vy_2 = __ldg(Vyin + o1 + pitch); dy_2 = __ldg(dYp + o1 + pitch); }
+        if (r + 2 <= H - 1) { vy_2 = ld1(Vyin + o1 + pitch); dy_2 = ld1(dYp + o1 + pitch); }
 
         // ---- pressure of row r (FDTDEngineCPU.cpp:316-339)
         const float ux_l = __shfl_up_sync(kFull, ux_c, 1);
