@@ -194,7 +194,7 @@ namespace {
 // Default launch shapes when no autotune ran: 16-row strips with 4 warps per
 // CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells;
 // with fast_math the quad strips of the same heights (16 rows x 4 warps,
-// 2 rows x 2 warps), and for fast_math batches without the two-mass source
+// 2 rows x 2 warps), and for fast_math batches without the coupled wall
 // the two-step strips of 64 columns (32 rows x 4 warps; 2 rows x 2 warps
 // below kSmallGridCells).
 constexpr int kDefaultShape = 1;

@@ -951,7 +951,7 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 }
 
 // ---------------------------------------------------------------------------
-// Two-step quad-strip kernel (fast_math, table sources, no coupled wall):
+// Two-step quad-strip kernel (fast_math, no coupled wall):
 // every strip advances TWO time steps per launch.  A lane holds NC adjacent
 // columns (NC = 4 or 2), a warp 32 NC columns, of which lanes 1..30 commit.
 // Step n runs the quad-strip row pipeline over rows r0-2 .. rlast+1 and all
