@@ -258,6 +258,22 @@ def test_two_step_small_and_open_frames(cuda_ok):
     assert np.all(np.isfinite(ref)) and np.all(np.abs(ref).max(axis=1) > 0)
 
 
+def test_batch_creation_reports_a_bad_tube_among_many(cuda_ok):
+    """The host builds the tubes' maps on several threads; an unusable area
+    function in the middle of a batch still fails the creation with
+    VS_ERR_GEOMETRY, and a good batch built afterwards runs."""
+    tubes = [S.batch_tube(i)[:2] for i in range(24)]
+    L, A = tubes[13]
+    A = A.copy()
+    A[5] = 0.0
+    gs = [V.Geometry(*t) for t in tubes[:13]] + [V.Geometry(L, A)] + [V.Geometry(*t) for t in tubes[14:]]
+    with pytest.raises(V.VsError) as e:
+        V.Batch([V.params(fast_math=1)] * 24, gs)
+    assert e.value.status == 2
+    b = V.Batch([V.params(fast_math=1)] * 3, [V.Geometry(*t) for t in tubes[:3]])
+    assert np.all(np.isfinite(b.run(50)))
+
+
 def test_fast_math_must_agree_within_a_batch(cuda_ok):
     L, A = S.vowel_tube(1)
     with pytest.raises(V.VsError) as e:
