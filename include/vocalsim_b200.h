@@ -71,7 +71,8 @@ enum { VS_LISTENER_REFERENCE = 0, VS_LISTENER_EXPLICIT = 1 };
 typedef struct vs_params {
     int32_t fdtd_solver_type;      /* 0 = 2D, 1 = 2.5D                                   */
     int32_t simulation_type;       /* 0 = open space (43 x 341 domain), 1 = tube         */
-    int32_t cross_sectional_shape; /* 1 = circular, 2 = elliptical 3:1                   */
+    int32_t cross_sectional_shape; /* 1 = circular, 2 = elliptical 3:1, 3 = single-plane   */
+                                   /* symmetric (ShapeGenerator.cpp:35-197; host build)  */
     int32_t mouth_radiation_cond;  /* 0 = open end, 1 = Dirichlet p = 0 column           */
     int32_t srate_mul;             /* fs = 44100 * srate_mul                             */
     int32_t source_type;           /* VS_SRC_*                                           */

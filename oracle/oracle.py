@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
         L.orc_run_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, dp]
         L.orc_run_maps_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, C.c_double, dp]
         L.orc_run_maps_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, C.c_float, fp]
+        L.orc_set_sps_diameters.argtypes = [fp, C.c_int]
         _orc = L
     return _orc
 
@@ -115,6 +116,14 @@ class Geometry:
 
     def ref(self):
         return C.byref(self.g)
+
+
+def set_sps_diameters(diameters_m) -> None:
+    """Section diameters (m) for the next single-plane-symmetric (shape 3)
+    builds: the oracle rasterises such tubes from them but does not construct
+    the sections itself (their depths come in through run_maps_f32)."""
+    d = np.ascontiguousarray(np.asarray(diameters_m, np.float32).ravel())
+    _check(lib().orc_set_sps_diameters(_fp(d), int(d.size)), "set_sps_diameters")
 
 
 def maps(p: VsParams, g: Geometry | None):

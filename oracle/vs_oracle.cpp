@@ -137,11 +137,22 @@ struct Tube {
     std::vector<int> upper, lower;
 };
 
+/* Section diameters of single-plane-symmetric sections (shape 3) are not
+   restated here (their construction needs Boost.Geometry in the reference):
+   the tests supply them with orc_set_sps_diameters, and the depth maps with
+   orc_run_maps_f32. */
+std::vector<float> g_sps_diameters;
+
 void tube_widths(const vs_params* p, const vs_geometry* g, Tube& t) {
+    if (p->cross_sectional_shape == 3 && (int)g_sps_diameters.size() != g->n_sections)
+        throw OracleError{VS_ERR_UNSUPPORTED, "shape 3 needs the section diameters (orc_set_sps_diameters)"};
     for (int i = 0; i < g->n_sections; i++) {
         float area = g->section_area_cm2[i];
         float a_m2 = area * U_CENTIMETER * U_CENTIMETER;
-        if (p->cross_sectional_shape == 1) {
+        if (p->cross_sectional_shape == 3) {
+            t.diam_m.push_back(g_sps_diameters[i]);
+            t.minor_m.push_back(0.0f);
+        } else if (p->cross_sectional_shape == 1) {
             float d = (float)(2.0 * std::sqrt((double)a_m2 / K_PI));
             t.diam_m.push_back(d);
             t.minor_m.push_back(0.0f);
@@ -226,8 +237,8 @@ void build_grid(const vs_params* p, const vs_geometry* g, Grid& G) {
             if (!(g->section_area_cm2[i] > 0.0f) || !(g->section_length_cm[i] > 0.0f))
                 throw OracleError{VS_ERR_GEOMETRY, "section length / area must be > 0"};
         }
-        if (p->cross_sectional_shape != 1 && p->cross_sectional_shape != 2)
-            throw OracleError{VS_ERR_UNSUPPORTED, "cross_sectional_shape must be 1 or 2"};
+        if (p->cross_sectional_shape < 1 || p->cross_sectional_shape > 3)
+            throw OracleError{VS_ERR_UNSUPPORTED, "cross_sectional_shape must be 1, 2 or 3"};
         Tube t;
         tube_widths(p, g, t);
         /* TubeGeometry.cu:105-106 */
@@ -368,7 +379,7 @@ void build_grid(const vs_params* p, const vs_geometry* g, Grid& G) {
 
         /* depth, FDTDSolver.cu:627-641 */
         G.dP.assign(N, 1.0f); G.dX.assign(N, 1.0f); G.dY.assign(N, 1.0f);
-        if (p->fdtd_solver_type == 1) {
+        if (p->fdtd_solver_type == 1 && p->cross_sectional_shape != 3) {
             /* TubeDepth::setTubeDepth, TubeDepth.cu:95-169 */
             const float min_depth = 0.001f;
             float osd = (float)(1.0 * open_space_depth);
@@ -913,6 +924,13 @@ void fill_dims(const Grid& G, vs_dims* d) {
 extern "C" {
 
 const char* orc_last_error(void) { return g_err.c_str(); }
+
+/* Diameters (m) of the single-plane-symmetric sections of the next shape-3
+   builds (n = 0 clears them). */
+int orc_set_sps_diameters(const float* d, int n) {
+    g_sps_diameters.assign(d, d + (n > 0 ? n : 0));
+    return VS_OK;
+}
 
 /* The reference's run configuration: main.cu:160-187 (2.5D, tube, circular,
  * srate_mul 15, Gaussian, 100 ms) with the open mouth and PML on, and the

@@ -171,7 +171,7 @@ def test_invalid_geometry_rejected(bad):
 
 @pytest.mark.parametrize("field,value,status", [
     ("srate_mul", 0, 1), ("fdtd_solver_type", 3, 1), ("pml_flag", 2, 1), ("engine", 0, 1),
-    ("source_type", 9, 1), ("cross_sectional_shape", 3, 7), ("listener_mode", 5, 1), ("tmm_f64", 2, 1),
+    ("source_type", 9, 1), ("cross_sectional_shape", 4, 7), ("listener_mode", 5, 1), ("tmm_f64", 2, 1),
     ("fast_math", 2, 1),
 ])
 def test_invalid_params_rejected(field, value, status):

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-
               f"-I{INCLUDE}", "-Wno-deprecated-gpu-targets"]
 
 SOURCES = ["vs_grid.cpp", "vs_capi.cpp", "vs_step.cu", "vs_noalloc.cu", "vs_adjoint.cu", "vs_spectrum.cu",
-           "vs_sections.cu", "vs_audio.cu"]
+           "vs_sections.cu", "vs_audio.cu", "vs_shapes.cpp"]
 
 
 def nvcc() -> str:

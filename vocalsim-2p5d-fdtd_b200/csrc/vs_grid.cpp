@@ -14,10 +14,12 @@
 //   * PML rows are painted before PML columns (FDTDSolver.cu:373-464)
 //   * depth smoothing pivots on the cell (mid row, tube end) (TubeDepth.cu:642-748)
 #include "vs_grid.h"
+#include "vs_shapes.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 
 namespace vsb {
 namespace {
@@ -93,6 +95,7 @@ private:
     Physics k_{};
     int pml_ = 0;
     std::vector<int> seg_;      // boundary_segment_type, H*W
+    std::vector<std::vector<ShapePt>> shapes_;   // single-plane-symmetric sections (aligned contours)
     float osd_ = 0.5f;          // open_space_depth (FDTDSolver.cu:292, TubeDepth.cu:91)
 
     int& type(int r, int c) { return T_.cell_type[(size_t)r * T_.W + c]; }
@@ -121,8 +124,11 @@ private:
                 if (!(g_->section_length_cm[i] > 0.0f) || !(g_->section_area_cm2[i] > 0.0f) ||
                     !std::isfinite(g_->section_length_cm[i]) || !std::isfinite(g_->section_area_cm2[i]))
                     raise(VS_ERR_GEOMETRY, "every section needs a finite length > 0 and area > 0");
-            if (p_.cross_sectional_shape != 1 && p_.cross_sectional_shape != 2)
-                raise(VS_ERR_UNSUPPORTED, "cross_sectional_shape must be 1 (circular) or 2 (elliptical)");
+            if (p_.cross_sectional_shape < 1 || p_.cross_sectional_shape > 3)
+                raise(VS_ERR_UNSUPPORTED,
+                      "cross_sectional_shape must be 1 (circular), 2 (elliptical) or 3 (single-plane symmetric)");
+            if (p_.cross_sectional_shape == 3 && p_.uniform_depth_m > 0.0f)
+                raise(VS_ERR_UNSUPPORTED, "uniform_depth_m applies to circular and elliptical sections");
         }
     }
 
@@ -185,11 +191,17 @@ private:
     void tube() {
         const int n = g_->n_sections;
         const bool ellipse = p_.cross_sectional_shape == 2;
-        // computeTubeWidthCircle / Ellipse (TubeGeometry.cu:316-364)
+        const bool sps = p_.cross_sectional_shape == 3;
+        // computeTubeWidthCircle / Ellipse / SinglePlaneSymmetry (TubeGeometry.cu:316-431)
         std::vector<float> width(n), minor(n, 0.0f), len_m(n);
+        if (sps) shapes_.assign(n, {});
         for (int i = 0; i < n; ++i) {
             const float a = g_->section_area_cm2[i] * kCm * kCm;
-            if (!ellipse) {
+            if (sps) {
+                std::string err;
+                shapes_[i] = sps_shape(a, &width[i], &err);
+                if (shapes_[i].empty()) raise(VS_ERR_GEOMETRY, err.c_str());
+            } else if (!ellipse) {
                 width[i] = (float)(2.0 * std::sqrt((double)a / kPi));
             } else {
                 const float lx = sqrtf((float)((double)a / ((double)(3.0f * 1.0f) * kPi)));
@@ -209,7 +221,8 @@ private:
         for (int i = 0; i < n; ++i) {
             int c = (int)std::round(width[i] / k_.ds);
             if (c == 0) ++c;
-            if (c % 2 == 0) c += ((float)c - (width[i] / k_.ds) > 0) ? -1 : 1;
+            // an even count rounds down, and always down for shape 3 (TubeGeometry.cu:139-146)
+            if (c % 2 == 0) c += (sps || (float)c - (width[i] / k_.ds) > 0) ? -1 : 1;
             dcell[i] = c;
         }
         const int dmax = *std::max_element(dcell.begin(), dcell.end());
@@ -331,6 +344,11 @@ private:
         const float ds = k_.ds;
         const bool ellipse = p_.cross_sectional_shape == 2;
         const float ud = p_.uniform_depth_m;
+        if (p_.cross_sectional_shape == 3) {
+            sps_depth(col, sx, column_max_seg);
+            finish_depth(my, ex);
+            return;
+        }
         for (size_t i = 0; i < col.size(); ++i) {
             const int x = sx + (int)i;
             const int air = col[i].down - col[i].up - 1;
@@ -373,6 +391,52 @@ private:
             dX(col[i].up, x) = 0; dX(col[i].down, x) = 0;
             dY(col[i].up, x) = 0; dY(col[i].down, x) = 0;
         }
+        finish_depth(my, ex);
+    }
+
+    // TubeDepth::generateTubeDepthSinglePlaneSymmetricShape (TubeDepth.cu:493-640):
+    // per tube column, with the aligned contour of its section, dX of the
+    // k-th air cell above the lower wall = half the contour's z extent along
+    // y = minY + (k - 1/2) ds, dY along y = minY + k ds (0 for the top cell);
+    // the wall cells 0.
+    template <class ColMax>
+    void sps_depth(const std::vector<Column>& col, int sx, ColMax column_max_seg) {
+        const float ds = k_.ds;
+        for (size_t i = 0; i < col.size(); ++i) {
+            const int x = sx + (int)i;
+            const int up = col[i].up, down = col[i].down;
+            const int air = down - up - 1;
+            const int s = column_max_seg(x);
+            if (s < 1 || s > (int)shapes_.size()) raise(VS_ERR_GEOMETRY, "tube column without a segment id");
+            const std::vector<ShapePt>& sh = shapes_[(size_t)s - 1];
+            float minZ = std::numeric_limits<float>::infinity(), maxZ = -minZ;
+            float minY = minZ;
+            for (const ShapePt& p : sh) {
+                minZ = std::min(minZ, p.z);
+                maxZ = std::max(maxZ, p.z);
+                minY = std::min(minY, p.y);
+            }
+            const float zlo = (float)((double)minZ - 0.001), zhi = (float)((double)maxZ + 0.001);
+            for (int k = 1; k <= air; ++k) {
+                const int row = down - k;
+                const float off_x = (float)((k - 0.5) * (double)ds);
+                const float off_y = k * ds;
+                float vx = 0.0f, vy = 0.0f;
+                if (!sps_half_depth(sh, minY + off_x, zlo, zhi, &vx))
+                    raise(VS_ERR_GEOMETRY, "single-plane-symmetric depth: the line misses the section");
+                if (k < air && !sps_half_depth(sh, minY + off_y, zlo, zhi, &vy))
+                    raise(VS_ERR_GEOMETRY, "single-plane-symmetric depth: the line misses the section");
+                if (vx < 0.0f || vy < 0.0f) raise(VS_ERR_GEOMETRY, "negative single-plane-symmetric depth");
+                dX(row, x) = vx;
+                dY(row, x) = vy;
+            }
+            dX(down, x) = 0; dX(up, x) = 0;
+            dY(down, x) = 0; dY(up, x) = 0;
+        }
+    }
+
+    // generateDepthP and setMinDepth (TubeDepth.cu:215-253, 642-762)
+    void finish_depth(int my, int ex) {
         // generateDepthP (TubeDepth.cu:215-253)
         const int H = T_.H, W = T_.W;
         const size_t n = (size_t)H * W, pivot = (size_t)my * W + ex;
