@@ -72,6 +72,21 @@ def test_cell_types_equal_the_oracle_rasterisation(built):
         assert om["dims"][k] == maps["dims"][k]
 
 
+def test_shape3_in_the_2d_solver(built):
+    """The 2D solver scales the section diameters (tubeAreaScaling) and keeps
+    unit depths; the oracle rasteriser agrees given the same diameters."""
+    _, layout, _ = built
+    p = V.params(cross_sectional_shape=3, fdtd_solver_type=0)
+    maps = V.build_maps(p, V.Geometry(LENGTHS, AREAS))
+    assert np.all(maps["depth_p"] == 1.0) and np.all(maps["depth_x"] == 1.0)
+    O.set_sps_diameters(layout["major"])
+    try:
+        om = O.maps(O.params(cross_sectional_shape=3, fdtd_solver_type=0), O.Geometry(LENGTHS, AREAS))
+    finally:
+        O.set_sps_diameters([])
+    assert np.array_equal(om["cell_type"], maps["cell_type"])
+
+
 def test_shape3_rejects_the_uniform_depth_override():
     with pytest.raises(V.VsError) as e:
         V.build_maps(V.params(cross_sectional_shape=3, uniform_depth_m=0.02), V.Geometry(LENGTHS, AREAS))
