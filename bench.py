@@ -74,10 +74,12 @@ def hbm_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(cells: int, shape: int, fast: int):
-    """DRAM bytes (read + write) per step-kernel launch from the committed ncu summary of the
-    same kernel (launch shape and arithmetic) on this same workload (same interior cell
-    count); else None."""
+def profiled_kernel(cells: int, shape: int, fast: int) -> dict:
+    """DRAM bytes (read + write) per step-kernel launch and the issue-active
+    percentage from the committed ncu summary of the same kernel (launch shape
+    and arithmetic) on this same workload (same interior cell count); None
+    where no summary matches."""
+    out = {"traffic": None, "issue_active_pct": None}
     for name in ("quad2_kernel_fast_batch256.json", "quad_kernel_fast_batch256.json", "strip_kernel_batch256.json"):
         f = REPO / "profiles" / name
         if not f.exists():
@@ -87,10 +89,15 @@ def profiled_traffic(cells: int, shape: int, fast: int):
             continue
         by_shape = d.get("traffic_by_shape", {})
         if str(shape) in by_shape:
-            return int(by_shape[str(shape)]["dram_bytes_per_launch"])
-        if int(d.get("shape", -1)) == int(shape):
-            return int(d["dram_bytes_per_launch"])
-    return None
+            out["traffic"] = int(by_shape[str(shape)]["dram_bytes_per_launch"])
+        elif int(d.get("shape", -1)) == int(shape):
+            out["traffic"] = int(d["dram_bytes_per_launch"])
+        else:
+            continue
+        if int(d.get("shape", -1)) == int(shape) and "smsp_issue_active_pct" in d:
+            out["issue_active_pct"] = float(d["smsp_issue_active_pct"])
+        return out
+    return out
 
 
 class ClockSampler:
@@ -362,8 +369,11 @@ def run_b200(args, rank, world):
     step_launches = sim_steps // per_launch + sim_steps % per_launch
     launches_per_forward = step_launches + math.ceil(sim_steps / 128)
     launch_ms = ms_step / step_launches        # average per step-kernel launch incl. graph gaps
-    achieved_gbs = BYTES_PER_CELL_UPDATE * cells / (launch_ms / 1e3) / 1e9
+    # algorithmic bytes per launch = 37 B per cell-update x the cell-updates one
+    # launch performs (cells x time steps per launch)
+    achieved_gbs = BYTES_PER_CELL_UPDATE * cells * per_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
+    prof = profiled_kernel(cells, tile, fast)
 
     # ---- e2e: public API with host buffers: build + upload maps, run, download traces
     e2e = None
@@ -440,14 +450,19 @@ def run_b200(args, rank, world):
                    "arithmetic": "reciprocal form (fast_math=1)" if fast else "reference rounding (fast_math=0)",
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved_gbs / peak, 4), "traffic": profiled_traffic(cells, tile, fast),
+                     "frac": round(achieved_gbs / peak, 4), "traffic": prof["traffic"],
+                     # DRAM bytes the launch really moves (ncu, same kernel and workload) per
+                     # launch time: the two-step kernel moves the planes once per two steps
+                     "dram_frac": (round(prof["traffic"] / (launch_ms / 1e3) / 1e9 / peak, 4)
+                                   if prof["traffic"] else None),
+                     "issue_active_pct": prof["issue_active_pct"],
                      # the metric's own form: Gcell-updates/s per GPU against the one-step
                      # roofline (37 B per cell-update moved once per step at the peak)
                      "gcell_roofline": round(peak / BYTES_PER_CELL_UPDATE, 1),
                      "gcell_frac": round(value / world / (peak / BYTES_PER_CELL_UPDATE), 4),
-                     "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell per launch x {cells} cells / "
-                             f"mean launch time {launch_ms * 1e3:.2f} us ({per_launch} time step(s) per launch); "
-                             f"peak {peak_kind}"},
+                     "note": f"{BYTES_PER_CELL_UPDATE} B algorithmic per cell-update x {cells} cells x {per_launch} "
+                             f"time step(s) per launch / mean launch time {launch_ms * 1e3:.2f} us; peak {peak_kind}; "
+                             f"dram_frac and issue_active_pct from the committed ncu summary of the same kernel"},
         "gpu_launches": args.steps * launches_per_forward,
         "clocks": clocks.summary(),
         "e2e": e2e,

@@ -329,13 +329,18 @@ int vs_batch_section_gradients(vs_batch* b, double* grad_width, double* grad_dep
  * `steps` floats.  The listener trace equals what vs_run gives for the same
  * tube.  Everything else lives in a 16 MiB static device array that every
  * GPU loading the library holds until exit; a frame larger than it (about
- * 37 bytes x H x roundup(W, 32)) is rejected with VS_ERR_INVALID_ARG.  The
- * call allocates nothing and returns once the work is queued on cuda_stream
- * (a cudaStream_t; NULL = default stream); synchronise the stream before
- * reading the trace.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress), so make it before any stream capture.
- * Calls share the array: it is re-initialised on every call, and calls whose
- * work overlaps on the GPU race on it. */
+ * 37 bytes x H x roundup(W, 32)) is rejected with VS_ERR_INVALID_ARG, and so
+ * are listener or excitation cells outside the frame's interior
+ * (1..W-2 x 1..H-2).  The maps stay on the device, so they are checked there:
+ * a cell_type outside 0..12 is run as a dead cell and the whole trace is
+ * returned as NaN.  The call allocates nothing and returns once the work is
+ * queued on cuda_stream (a cudaStream_t; NULL = default stream); synchronise
+ * the stream before reading the trace.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and keeps it for the
+ * life of the process, so make that call before any stream capture, and do
+ * not use this entry point across a cudaDeviceReset of that device.  Calls
+ * share the array: it is re-initialised on every call, and calls whose work
+ * overlaps on the GPU race on it. */
 int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int32_t* cell_type,
                    const float* depth_p, const float* depth_x, const float* depth_y,
                    const float* z_inv, const float* source, int64_t steps, float* trace,

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import importlib.util
+import os
 import sys
 from pathlib import Path
 
@@ -22,7 +23,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path("/root/reference")
+# the reference tree: VOCALSIM_REFERENCE, else the build recipe's default location
+REF = Path(os.environ.get("VOCALSIM_REFERENCE", "/root/reference"))
 sys.path.insert(0, str(REPO / "oracle"))
 
 import oracle as O  # noqa: E402  (only for the library path of the reference pieces)

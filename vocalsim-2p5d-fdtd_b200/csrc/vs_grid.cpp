@@ -65,6 +65,38 @@ int64_t float_step_count(float dur, float dt) {
     return n;
 }
 
+// Scalar constants and tables of one tube (SimulationParams.cu:7-34,
+// SolverParams.cu:5-76, FDTDSolver.cu:311-312): the single source of these
+// values for the map builder and for vs_run_noalloc.
+void fill_tables(const vs_params& p, const Physics& k, TubeGrid& T) {
+    // SolverParams::setBeta / setSigmaPrimeDt / setSourceDirection (SolverParams.cu:5-76)
+    static const float beta_fixed[13] = {0, 1, 0, 1, 1, 1, 1, 1, 1, 0, 0, 1, 0};
+    for (int i = 0; i < 13; ++i) T.beta[i] = beta_fixed[i];
+    const float dt = k.dt;
+    const float sig_fixed[13] = {dt, 0, dt, 0, 0, 0, 0, 0, 0, 0, 1000000.0f, 0, dt};
+    for (int i = 0; i < 13; ++i) T.sigma[i] = sig_fixed[i];
+    for (int l = 0; l < kPmlLayers; ++l)
+        T.sigma[VS_CELL_PML0 + l] = ((float)l / (float)(kPmlLayers - 1)) * k.max_sigma_dt;
+    T.dir[0] = 0; T.dir[1] = 0; T.dir[2] = 1; T.dir[3] = 0;
+    T.K1 = (k.kappa * k.dt) / k.ds;
+    T.K2 = k.kappa * k.dt;
+    T.bcoef = (1.0f * k.dt) / (k.rho * k.ds);   // (minBeta^2 dt)/(rho ds), minBeta = 1
+    T.dt = k.dt;
+    T.Mw = 21 * (kKg / (kMeter * kMeter));
+    T.Bw = 8000 * (kKg / (kMeter * kMeter * kSecond));
+    T.Kw = 845000 * (kKg / (kMeter * kMeter * kSecond * kSecond));
+    T.cpl = p.wall_coupling;
+    T.srate_mul = p.srate_mul;
+    T.dirichlet = p.mouth_radiation_cond != 0;
+    T.eigen = p.engine == VS_ENGINE_EIGEN;
+    T.tmm = p.source_type == VS_SRC_TMM;
+    T.wall_ode = p.fdtd_solver_type == 1 && p.wall_coupling != 0.0f;
+    vs_dims& d = T.dims;
+    d.dt = k.dt;
+    d.ds = k.ds;
+    d.num_steps = p.num_steps > 0 ? p.num_steps : float_step_count(p.audio_dur, k.dt);
+}
+
 [[noreturn]] void raise(int status, const char* what) { throw VsFailure{status, what}; }
 
 // One tube column: wall rows and the area-function segment it samples.
@@ -132,34 +164,7 @@ private:
         }
     }
 
-    void tables() {
-        // SolverParams::setBeta / setSigmaPrimeDt / setSourceDirection (SolverParams.cu:5-76)
-        static const float beta_fixed[13] = {0, 1, 0, 1, 1, 1, 1, 1, 1, 0, 0, 1, 0};
-        for (int i = 0; i < 13; ++i) T_.beta[i] = beta_fixed[i];
-        const float dt = k_.dt;
-        const float sig_fixed[13] = {dt, 0, dt, 0, 0, 0, 0, 0, 0, 0, 1000000.0f, 0, dt};
-        for (int i = 0; i < 13; ++i) T_.sigma[i] = sig_fixed[i];
-        for (int l = 0; l < kPmlLayers; ++l)
-            T_.sigma[VS_CELL_PML0 + l] = ((float)l / (float)(kPmlLayers - 1)) * k_.max_sigma_dt;
-        T_.dir[0] = 0; T_.dir[1] = 0; T_.dir[2] = 1; T_.dir[3] = 0;
-        T_.K1 = (k_.kappa * k_.dt) / k_.ds;
-        T_.K2 = k_.kappa * k_.dt;
-        T_.bcoef = (1.0f * k_.dt) / (k_.rho * k_.ds);   // (minBeta^2 dt)/(rho ds), minBeta = 1
-        T_.dt = k_.dt;
-        T_.Mw = 21 * (kKg / (kMeter * kMeter));
-        T_.Bw = 8000 * (kKg / (kMeter * kMeter * kSecond));
-        T_.Kw = 845000 * (kKg / (kMeter * kMeter * kSecond * kSecond));
-        T_.cpl = p_.wall_coupling;
-        T_.srate_mul = p_.srate_mul;
-        T_.dirichlet = p_.mouth_radiation_cond != 0;
-        T_.eigen = p_.engine == VS_ENGINE_EIGEN;
-        T_.tmm = p_.source_type == VS_SRC_TMM;
-        T_.wall_ode = p_.fdtd_solver_type == 1 && p_.wall_coupling != 0.0f;
-        vs_dims& d = T_.dims;
-        d.dt = k_.dt;
-        d.ds = k_.ds;
-        d.num_steps = p_.num_steps > 0 ? p_.num_steps : float_step_count(p_.audio_dur, k_.dt);
-    }
+    void tables() { fill_tables(p_, k_, T_); }
 
     void alloc_frame(int H, int W) {
         if (H < 3 || W < 3 || (int64_t)H * W > (int64_t)1 << 28) raise(VS_ERR_GEOMETRY, "frame size out of range");
@@ -606,15 +611,26 @@ static TmmConsts64 widen(const TmmConsts& c) {
             c.etah2, c.Ag01, c.Ag02, c.lg, c.r1o, c.r2o, c.r1c, c.r2c, c.A1, c.ps, c.srate};
 }
 
+static void fill_tmm(const vs_params* p, TubeGrid& out) {
+    out.tmmc = tmm_consts<float>(p->tmm_ps_pa, p->srate_mul);
+    out.tmm64 = p->source_type == VS_SRC_TMM && p->tmm_f64 != 0;
+    out.tmmd = out.tmm64 ? tmm_consts<double>(p->tmm_ps_pa, p->srate_mul) : widen(out.tmmc);
+}
+
 void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source) {
     if (!p) throw VsFailure{VS_ERR_INVALID_ARG, "null vs_params"};
     Builder(p, g, out).run();
     const int64_t n = steps_for_source > 0 ? steps_for_source : out.dims.num_steps;
     if (p->source_type == VS_SRC_TMM) out.source.clear();
     else build_source(p, out.dt, n, out.source);
-    out.tmmc = tmm_consts<float>(p->tmm_ps_pa, p->srate_mul);
-    out.tmm64 = p->source_type == VS_SRC_TMM && p->tmm_f64 != 0;
-    out.tmmd = out.tmm64 ? tmm_consts<double>(p->tmm_ps_pa, p->srate_mul) : widen(out.tmmc);
+    fill_tmm(p, out);
+}
+
+void solver_constants(const vs_params* p, TubeGrid& out) {
+    if (!p) throw VsFailure{VS_ERR_INVALID_ARG, "null vs_params"};
+    if (p->srate_mul < 1 || p->srate_mul > 64) throw VsFailure{VS_ERR_INVALID_ARG, "srate_mul must be in 1..64"};
+    fill_tables(*p, physics(p->srate_mul), out);
+    fill_tmm(p, out);
 }
 
 }  // namespace vsb

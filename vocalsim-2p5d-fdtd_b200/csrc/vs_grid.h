@@ -78,6 +78,12 @@ void default_params(vs_params* p);
 // `steps_for_source` > 0 sizes the source table; 0 uses dims.num_steps.
 void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source);
 
+// Only the scalar constants and tables of a tube (K1, K2, bcoef, dt, the wall
+// parameters, sigma/beta/direction tables, two-mass constants and the flags
+// derived from p), without building any map: what a caller that brings its
+// own maps needs.  Touches none of the vectors of `out`.
+void solver_constants(const vs_params* p, TubeGrid& out);
+
 // The per-step excitation table (GlottalExcitations::setExcitationVelocity).
 void build_source(const vs_params* p, float dt, int64_t n, std::vector<float>& out);
 

@@ -65,7 +65,8 @@ cudaError_t scratch_address(unsigned char** out) {
 __global__ void pack_maps(const int32_t* __restrict__ cell_type, const float* __restrict__ dp,
                           const float* __restrict__ dx, const float* __restrict__ dy,
                           const float* __restrict__ zinv, float* __restrict__ odp, float* __restrict__ odx,
-                          float* __restrict__ ody, uint8_t* __restrict__ ocode, int H, int W, int pitch) {
+                          float* __restrict__ ody, uint8_t* __restrict__ ocode, int H, int W, int pitch,
+                          int32_t* __restrict__ bad) {
     const int64_t n = (int64_t)H * pitch;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int r = (int)(i / pitch), c = (int)(i - (int64_t)r * pitch);
@@ -74,8 +75,15 @@ __global__ void pack_maps(const int32_t* __restrict__ cell_type, const float* __
             odp[i] = dp[s];
             odx[i] = dx[s];
             ody[i] = dy[s];
-            uint8_t k = (uint8_t)(cell_type[s] & CODE_TYPE_MASK);
-            if (zinv[s] != 0.0f) k |= CODE_ZINV_BIT;
+            const int32_t ty = cell_type[s];
+            uint8_t k;
+            if (ty < 0 || ty >= 13) {          // not a reference cell type: kept out of the tables
+                k = (uint8_t)VS_CELL_DEAD;
+                *bad = 1;
+            } else {
+                k = (uint8_t)ty;
+                if (zinv[s] != 0.0f) k |= CODE_ZINV_BIT;
+            }
             ocode[i] = k;
         } else {
             odp[i] = 0.0f;
@@ -86,21 +94,37 @@ __global__ void pack_maps(const int32_t* __restrict__ cell_type, const float* __
     }
 }
 
-// Strip work items of one tube, in the order vs_batch builds them.
-__global__ void make_strips(Tile* __restrict__ tiles, const int32_t* __restrict__ cell_type,
-                            const float* __restrict__ zinv, int H, int W, int rows, int nstrips, int nitems) {
+// Strip work items of one tube, in the order vs_batch builds them, classified
+// from the packed code bytes.
+__global__ void make_strips(Tile* __restrict__ tiles, const uint8_t* __restrict__ code, int H, int W, int pitch,
+                            int rows, int nstrips, int nitems) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nitems) return;
     Tile t{};
     t.tube = 0;
     t.r0 = 1 + (i / nstrips) * rows;
     t.c0 = -kStripLead + (i % nstrips) * kStripCommit;
-    auto code_at = [=](int r, int c) {
-        const int64_t s = (int64_t)r * W + c;
-        return (cell_type[s] & CODE_TYPE_MASK) | (zinv[s] != 0.0f ? CODE_ZINV_BIT : 0);
-    };
+    auto code_at = [=](int r, int c) { return (int)code[(int64_t)r * pitch + c]; };
     classify_strip(code_at, H, W, t.r0, rows, t.c0, t);
     tiles[i] = t;
+}
+
+// Descriptors of the run, passed by value (kernel parameters are copied at
+// launch, so no host buffer has to stay alive and nothing is staged through
+// pageable memory).
+__global__ void init_run(TubeDev t, RunState rs, TubeDev* __restrict__ dt, RunState* __restrict__ drs,
+                         int32_t* __restrict__ bad) {
+    *dt = t;
+    *drs = rs;
+    *bad = 0;
+}
+
+// A map with a cell type outside 0..12 has no defined update: its trace is
+// returned as NaN so the caller cannot mistake it for a result.
+__global__ void poison_trace(const int32_t* __restrict__ bad, float* __restrict__ trace, int64_t n) {
+    if (!*bad) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        trace[i] = __int_as_float(0x7fc00000);
 }
 
 int fail(int status, const char* msg) {
@@ -127,6 +151,11 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     if (p->fast_math) return fail(VS_ERR_UNSUPPORTED, "vs_run_noalloc runs the reference arithmetic only (fast_math = 0)");
     const int H = dims->frame_h, W = dims->frame_w;
     if (H < 3 || W < 3) return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: frame smaller than 3 x 3");
+    // the same ranges the map builder guarantees: interior cells only
+    if (dims->listener_x < 1 || dims->listener_x > W - 2 || dims->listener_y < 1 || dims->listener_y > H - 2)
+        return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: listener cell outside the frame's interior");
+    if (dims->excitation_x < 1 || dims->excitation_x > W - 2 || dims->excitation_y < 1 || dims->excitation_y > H - 2)
+        return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: excitation cell outside the frame's interior");
     const int pitch = (W + 31) / 32 * 32;
     const bool wall = p->fdtd_solver_type == 1 && p->wall_coupling != 0.0f;
     const size_t plane_bytes = up256((size_t)H * pitch * sizeof(float));
@@ -141,30 +170,34 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     const size_t off_tmm = off;               off += up256(2 * sizeof(TmmState)) + up256(2 * sizeof(TmmState64));
     const size_t off_tube = off;              off += up256(sizeof(TubeDev));
     const size_t off_rs = off;                off += up256(sizeof(RunState));
+    const size_t off_bad = off;               off += 256;
     const size_t off_tiles = off;             off += up256((size_t)nitems * sizeof(Tile));
     if (off > kScratchBytes)
         return fail(VS_ERR_INVALID_ARG, "vs_run_noalloc: frame too large for the 16 MiB static scratch");
+
+    // K1, K2, bcoef, dt, wall parameters, sigma table and two-mass constants
+    // from the map builder's own source of them
+    TubeGrid k;
+    try {
+        solver_constants(p, k);
+    } catch (const VsFailure& f) {
+        return fail(f.status, f.what.c_str());
+    }
 
     unsigned char* base = nullptr;
     cudaError_t e = scratch_address(&base);
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
 
-    // constants of SimulationParams(srate_mul) / SolverParams / FDTDSolver.cu:311-312
-    const float c = 350.0f, rho = (float)((double)1.14f / std::pow(1.0, 3));
-    const float kappa = rho * c * c;
-    const float dt = 1.0f / (float)(44100 * p->srate_mul);
-    const float ds = dt * c * sqrtf(2.0f);
-
     TubeDev t;
     std::memset(&t, 0, sizeof(t));
     const size_t pe = plane_bytes / sizeof(float);
     float* s0 = reinterpret_cast<float*>(base + off_state);
-    for (int k = 0; k < 2; ++k) {
-        t.P[k] = s0 + k * pe;
-        t.Vx[k] = s0 + (2 + k) * pe;
-        t.Vy[k] = s0 + (4 + k) * pe;
-        if (wall) { t.w[k] = s0 + (6 + k) * pe; t.z[k] = s0 + (8 + k) * pe; }
+    for (int j = 0; j < 2; ++j) {
+        t.P[j] = s0 + j * pe;
+        t.Vx[j] = s0 + (2 + j) * pe;
+        t.Vy[j] = s0 + (4 + j) * pe;
+        if (wall) { t.w[j] = s0 + (6 + j) * pe; t.z[j] = s0 + (8 + j) * pe; }
     }
     float* d0 = reinterpret_cast<float*>(base + off_depth);
     t.dP = d0;
@@ -177,24 +210,17 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     t.tmm64 = reinterpret_cast<TmmState64*>(base + off_tmm + up256(2 * sizeof(TmmState)));
     t.plane = (int64_t)pe;
     t.H = H; t.W = W; t.pitch = pitch;
-    t.flags = (p->mouth_radiation_cond ? TUBE_DIRICHLET : 0) | (p->engine == VS_ENGINE_EIGEN ? TUBE_EIGEN : 0) |
-              (p->source_type == VS_SRC_TMM ? TUBE_TMM : 0) | (wall ? TUBE_WALL_ODE : 0) |
-              (p->source_type == VS_SRC_TMM && p->tmm_f64 ? TUBE_TMM64 : 0);
+    t.flags = (k.dirichlet ? TUBE_DIRICHLET : 0) | (k.eigen ? TUBE_EIGEN : 0) | (k.tmm ? TUBE_TMM : 0) |
+              (k.wall_ode ? TUBE_WALL_ODE : 0) | (k.tmm64 ? TUBE_TMM64 : 0);
     t.lis_x = dims->listener_x; t.lis_y = dims->listener_y;
     t.exc_x = dims->excitation_x; t.exc_y = dims->excitation_y;
-    t.K1 = (kappa * dt) / ds;
-    t.K2 = kappa * dt;
-    t.bcoef = (1.0f * dt) / (rho * ds);
+    t.K1 = k.K1; t.K2 = k.K2; t.bcoef = k.bcoef;
     t.zinv = dims->z_inv_val;
-    t.dt = dt;
-    t.Mw = 21.0f; t.Bw = 8000.0f; t.Kw = 845000.0f;
-    t.cpl = p->wall_coupling;
-    t.dir0 = 0.0f; t.dir1 = 0.0f; t.dir2 = 1.0f; t.dir3 = 0.0f;
-    const float sig[13] = {dt, 0, dt, 0, 0, 0, 0, 0, 0, 0, 1000000.0f, 0, dt};
-    for (int k = 0; k < 13; ++k) t.sigma[k] = sig[k];
-    for (int l = 0; l < 6; ++l) t.sigma[VS_CELL_PML0 + l] = ((float)l / (float)5) * 0.5f;
-    t.tmmc = tmm_consts<float>(p->tmm_ps_pa, p->srate_mul);
-    t.tmmd = tmm_consts<double>(p->tmm_ps_pa, p->srate_mul);
+    t.dt = k.dt; t.Mw = k.Mw; t.Bw = k.Bw; t.Kw = k.Kw; t.cpl = k.cpl;
+    t.dir0 = k.dir[0]; t.dir1 = k.dir[1]; t.dir2 = k.dir[2]; t.dir3 = k.dir[3];
+    for (int j = 0; j < 13; ++j) t.sigma[j] = k.sigma[j];
+    t.tmmc = k.tmmc;
+    t.tmmd = k.tmmd;
 
     RunState rs;
     std::memset(&rs, 0, sizeof(rs));
@@ -203,20 +229,24 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
 
     TubeDev* d_tube = reinterpret_cast<TubeDev*>(base + off_tube);
     RunState* d_rs = reinterpret_cast<RunState*>(base + off_rs);
+    int32_t* d_bad = reinterpret_cast<int32_t*>(base + off_bad);
     Tile* d_tiles = reinterpret_cast<Tile*>(base + off_tiles);
     // fields, wall state and the two-mass state restart at zero on every call
     e = cudaMemsetAsync(base + off_state, 0, plane_bytes * nstate, st);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(base + off_tmm, 0, up256(2 * sizeof(TmmState)) + up256(2 * sizeof(TmmState64)), st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_tube, &t, sizeof(t), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));
+    init_run<<<1, 1, 0, st>>>(t, rs, d_tube, d_rs, d_bad);
     pack_maps<<<592, 256, 0, st>>>(cell_type, depth_p, depth_x, depth_y, z_inv, d0, d0 + pe,
-                                   d0 + 2 * pe, base + off_code, H, W, pitch);
-    make_strips<<<(nitems + 127) / 128, 128, 0, st>>>(d_tiles, cell_type, z_inv, H, W, rows, nstrips, nitems);
+                                   d0 + 2 * pe, base + off_code, H, W, pitch, d_bad);
+    make_strips<<<(nitems + 127) / 128, 128, 0, st>>>(d_tiles, base + off_code, H, W, pitch, rows, nstrips, nitems);
     e = cudaGetLastError();
     for (int64_t i = 0; i < steps && e == cudaSuccess; ++i)
         e = launch_step(kShape, wall, false, d_tube, d_tiles, nitems, d_rs, (int)i, st, pitch);
+    if (e == cudaSuccess) {
+        poison_trace<<<64, 256, 0, st>>>(d_bad, trace, steps);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return fail(VS_ERR_CUDA, cudaGetErrorString(e));
     return VS_OK;
 }
