@@ -7,8 +7,12 @@ cpu_baseline / reference legs of bench.py, never by the solver package.
 from __future__ import annotations
 
 import ctypes as C
+import os
+import shutil
 import subprocess
 import sys
+import tempfile
+import time
 from pathlib import Path
 
 import numpy as np
@@ -20,7 +24,11 @@ from vocalsim_b200.abi import VsDims, VsGeometry, VsParams  # noqa: E402  (struc
 
 LIB = ORACLE_DIR / "_build" / "liboracle.so"
 REF_LIB = ORACLE_DIR / "_ref" / "libvsref.so"
-REFERENCE_TREE = Path("/root/reference")
+REF_ENGINE = ORACLE_DIR / "_ref" / "ref_engine"          # Release-like build of the reference's setup + engine
+REF_ENGINE_G = ORACLE_DIR / "_ref" / "ref_engine_g"      # the same with -G (the reference CMake's default)
+# Where oracle/Makefile.ref finds the reference sources: VOCALSIM_REFERENCE, else
+# the build recipe's default location.  Only build() reads it.
+REFERENCE_TREE = Path(os.environ.get("VOCALSIM_REFERENCE", "/root/reference"))
 
 _orc = None
 _ref = None
@@ -30,9 +38,9 @@ def build(force: bool = False) -> None:
     """Compile the oracle (and the reference pieces when the tree is present)."""
     if force or not LIB.exists():
         subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
-    if REFERENCE_TREE.exists() and (force or not REF_LIB.exists()):
+    if REFERENCE_TREE.exists() and (force or not (REF_LIB.exists() and REF_ENGINE.exists() and REF_ENGINE_G.exists())):
         subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "-f", "Makefile.ref",
-                        f"REF={REFERENCE_TREE}"], check=True)
+                        f"REF={REFERENCE_TREE}", "all"], check=True)
 
 
 def lib() -> C.CDLL:
@@ -230,3 +238,83 @@ def tables(srate_mul: int):
 
 def step_count(audio_dur: float, dt: float) -> int:
     return int(lib().orc_step_count(audio_dur, dt))
+
+
+# --------------------------------------------------------------------------- reference engine
+# vs_params fields whose values the reference hard-codes; a reference-engine
+# run is only a like-for-like check when they hold the defaults.
+_NATIVE_FIELDS = ("mu3d", "gauss_peak_s", "gauss_width_s", "gauss_amp", "sine_freq_hz", "sine_amp", "tmm_ps_pa",
+                  "wall_coupling", "uniform_depth_m", "listener_mode", "listener_x", "listener_y", "engine",
+                  "tmm_f64", "fast_math")
+
+
+def reference_native(p: VsParams) -> bool:
+    """True when every parameter the reference hard-codes has its reference value."""
+    d = params()
+    return all(getattr(p, k) == getattr(d, k) for k in _NATIVE_FIELDS if hasattr(d, k)) and p.source_type in (0, 1, 2)
+
+
+def _fmt32(x) -> str:
+    """Shortest decimal that reads back as the same float32 (strtof)."""
+    return np.format_float_positional(np.float32(x), unique=True, trim="-")
+
+
+def reference_engine(p: VsParams, g: Geometry | None, steps: int, debug_build: bool = False, with_maps: bool = True,
+                     timeout: float = 900.0) -> dict:
+    """Run the reference's own SimulationParams -> FDTDSolver::setupWaveSolver ->
+    FDTDEngineCPU::startSolverEngine (oracle/_ref/ref_engine, compiled from the
+    reference sources; the setup kernels need a CUDA device) for `steps` steps.
+    The area function is written in the reference's file format to the file
+    its constructor reads (TubeGeometry.cu:53-88) in a scratch tree.  Returns the
+    reference's maps, its 17 coefficient arrays, its excitation table, its
+    record_pressure and final fields, and the seconds its time loop took."""
+    exe = REF_ENGINE_G if debug_build else REF_ENGINE
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} is not built (oracle/Makefile.ref needs the reference tree)")
+    if not reference_native(p):
+        raise ValueError("the reference engine hard-codes mu3d, its sources and its wall and depth model: "
+                         "use reference defaults for those fields")
+    if g is None and p.source_type == 2:
+        # openSpaceSimulation never sets FDTDSolver::excitationX/Y (FDTDSolver.cu:530-531),
+        # which the two-mass source reads
+        raise ValueError("the reference's open-space domain has no excitation cell for the two-mass source")
+    root = Path(tempfile.mkdtemp(prefix="vs_refeng_"))
+    try:
+        (root / "data" / "tube-geometry").mkdir(parents=True)
+        (root / "results").mkdir()
+        (root / "a" / "b").mkdir(parents=True)
+        (root / "out").mkdir()
+        if g is not None:
+            lines = [f"{_fmt32(l)} {_fmt32(a)}" for l, a in zip(g.length, g.area)]
+            (root / "data" / "tube-geometry" / "vocaltract_a.txt").write_text("\n".join(lines) + "\n")
+        consts_ = consts(p.srate_mul)
+        dt = float(consts_[3])
+        audio_dur = (steps + 16) * dt * 1.01
+        args = [str(exe), f"solver={p.fdtd_solver_type}", f"sim={p.simulation_type}", "tube=1", "vowel=1",
+                f"shape={p.cross_sectional_shape if g is not None else -1}", f"mouth={p.mouth_radiation_cond}",
+                f"srate_mul={p.srate_mul}", f"audio_dur={audio_dur!r}", f"source={p.source_type}",
+                f"pml={p.pml_flag}", f"steps={steps}", f"out={root / 'out'}", f"maps={1 if with_maps else 0}"]
+        t0 = time.perf_counter()
+        r = subprocess.run(args, cwd=root / "a" / "b", capture_output=True, text=True, timeout=timeout)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_engine exited {r.returncode}: {r.stderr[-2000:]}")
+        out = root / "out"
+        meta = {}
+        for line in (out / "meta.txt").read_text().splitlines():
+            k, v = line.split()
+            meta[k] = float(v) if any(ch in v for ch in ".e") else int(v)
+        H, W = meta["frame_h"], meta["frame_w"]
+        rd = lambda name, dt_=np.float32: np.fromfile(out / name, dtype=dt_)  # noqa: E731
+        res = {"meta": meta, "trace": rd("trace.f32"), "excitation": rd("excitation.f32"),
+               "p": rd("p.f32").reshape(H, W), "vx": rd("vx.f32").reshape(H, W), "vy": rd("vy.f32").reshape(H, W),
+               "loop_s": meta["loop_s"], "wall_s": wall}
+        if with_maps:
+            res["cell_type"] = rd("cell_type.i32", np.int32).reshape(H, W)
+            for k in ("depth_p", "depth_x", "depth_y", "z_inv"):
+                res[k] = rd(k + ".f32").reshape(H, W)
+            res["coeffs"] = {k: rd(k + ".f32").reshape(H - 2, W - 2) for k in COEFF_NAMES}
+        return res
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
