@@ -56,11 +56,31 @@ def max_over_ranks(ms: float, world: int, device=None) -> float:
     return float(t.item())
 
 
-def workload_params(rank: int, n_tubes: int, fast_math: int = 1):
+def strong_seeds(rank: int, world: int, n_tubes: int) -> list[int]:
+    """Strong scaling: the fixed batch of seeds 0..n_tubes-1 split across the
+    ranks by LPT on each tube's interior cell count."""
+    from vocalsim_b200 import synthetic as S
+    import vocalsim_b200 as V
+    from vocalsim_b200.sharding import shard_batch
+    costs = [V.build_maps(V.params(cross_sectional_shape=2), V.Geometry(*S.batch_tube(sd)[:2]))["dims"]["interior_cells"]
+             for sd in range(n_tubes)]
+    return shard_batch(costs, rank, world)
+
+
+def sum_over_ranks(x: int, world: int, device=None) -> int:
+    if world <= 1:
+        return int(x)
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return int(t.item())
+
+
+def workload_params(rank: int, n_tubes: int, fast_math: int = 1, seeds=None):
     from vocalsim_b200 import synthetic as S
     import vocalsim_b200 as V
     ps, gs = [], []
-    for seed in rank_tube_seeds(rank, n_tubes):
+    for seed in (rank_tube_seeds(rank, n_tubes) if seeds is None else seeds):
         L, A, _, _ = S.batch_tube(seed)
         ps.append(V.params(cross_sectional_shape=2, num_steps=SIM_STEPS, fast_math=fast_math))
         gs.append(V.Geometry(L, A))
@@ -313,7 +333,8 @@ def run_b200(args, rank, world):
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream(dev)
     fast = 1 if args.arith == "fast" else 0
-    ps, gs = workload_params(rank, args.tubes, fast)
+    seeds = strong_seeds(rank, world, args.tubes) if args.strong else None
+    ps, gs = workload_params(rank, args.tubes, fast, seeds)
     batch = V.Batch(ps, gs)
     batch.set_stream(stream.cuda_stream)
     cells = batch.interior_cells
@@ -362,7 +383,10 @@ def run_b200(args, rank, world):
     ms_total = max_over_ranks(ms_total, world, dev)
     ms_step = ms_total / args.steps
     cell_updates_rank = cells * sim_steps
-    value = cell_updates_rank * world / (ms_step / 1e3) / 1e9
+    # whole-job cell-updates: every rank's own tubes (equal per rank under weak
+    # scaling; the LPT shares of the one batch under --strong)
+    job_cells = sum_over_ranks(cells, world, dev)
+    value = job_cells * sim_steps / (ms_step / 1e3) / 1e9
     # a two-step shape advances two time steps per launch and moves the state
     # planes once per launch: algorithmic bytes per launch = 37 B x cells
     per_launch = V.tile_shape_steps(tile)
@@ -395,7 +419,7 @@ def run_b200(args, rank, world):
         h2d = sum(d["frame_h"] * ((d["frame_w"] + 31) // 32 * 32) * 13 for d in batch.dims) + \
             sum(4 * sim_steps for _ in batch.dims)
         d2h = 4 * sim_steps * args.tubes
-        e2e = {"value": round(cell_updates_rank * world / (e2e_step / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
+        e2e = {"value": round(job_cells * sim_steps / (e2e_step / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_step, 2)}
 
     # ---- plain single-tube GPU path for the batched-vs-single ratio
@@ -441,12 +465,14 @@ def run_b200(args, rank, world):
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded area functions, no dataset)",
+        "higher_is_better": True, "scaling": "strong" if args.strong else "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded area functions, no dataset)",
         "config": {"workload": "batched forward, 256 tubes 12-20 cm x 2-4 cm, 3:1 elliptical, Gaussian, PML 6, "
                                "50 ms (33075 steps) at fs 661.5 kHz; one step = one full forward",
-                   "tubes_per_gpu": args.tubes, "interior_cells_per_gpu": cells, "sim_steps": sim_steps,
-                   "tile": list(V.tile_shapes()[tile]), "parallelism": f"tube sharding x{world} (no collective)",
+                   "tubes_per_gpu": len(ps), "interior_cells_per_gpu": cells, "sim_steps": sim_steps,
+                   "tile": list(V.tile_shapes()[tile]),
+                   "parallelism": (f"LPT tube sharding of one {args.tubes}-tube batch x{world} (no collective)"
+                                   if args.strong else f"tube sharding x{world} (no collective)"),
                    "arithmetic": "reciprocal form (fast_math=1)" if fast else "reference rounding (fast_math=0)",
                    "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
@@ -483,6 +509,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--tubes", type=int, default=N_TUBES)
+    ap.add_argument("--strong", action="store_true",
+                    help="split one batch of --tubes tubes across the ranks (LPT by cells) instead of one batch per rank")
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--profile-steps", type=int, default=0)
     ap.add_argument("--profile-adjoint", type=int, default=0,

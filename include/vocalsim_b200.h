@@ -235,20 +235,28 @@ int vs_batch_reset(vs_batch* b);
 int vs_batch_set_stream(vs_batch* b, void* cuda_stream);
 
 /* Select the tile shape used by the step kernel (index into the compiled
- * shape table, see vs_tile_shape) or -1 for the autotuned choice. */
+ * shape table, see vs_tile_shape) or -1 for the default choice.  The last
+ * shape of the table is the cluster kernel: a batch of one tube without the
+ * coupled wall oscillator keeps its state in the shared memory of one
+ * thread-block cluster (up to 16 CTAs, one band of rows each, halo rows
+ * exchanged through distributed shared memory) and runs every step of a
+ * vs_batch_run / vs_run call in one launch; it is the default for such
+ * batches when the band fits a CTA's shared memory. */
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
 
 /* Time every compiled tile shape on `steps` steps and keep the fastest.  The
  * state is reset afterwards.  best_index / best_ms may be NULL. */
 int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* best_ms);
 
-/* Number of compiled tile shapes, and the rows x cols of shape i. */
+/* Number of compiled tile shapes, and the rows x cols of shape i (0 x 0 for
+ * the cluster shape, the last one). */
 int vs_tile_shape_count(void);
 int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols);
 
 /* Time steps one kernel launch of shape i advances: 1, or 2 for the two-step
  * shapes (fast_math batches without the coupled wall; they keep a third set
- * of state planes and a third two-mass state slot beside the two parity sets). */
+ * of state planes and a third two-mass state slot beside the two parity sets),
+ * or 0 for the cluster shape (all the steps of a run in one launch). */
 int vs_tile_shape_steps(int32_t i, int32_t* steps_per_launch);
 
 void vs_batch_destroy(vs_batch* b);

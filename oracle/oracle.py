@@ -26,6 +26,7 @@ LIB = ORACLE_DIR / "_build" / "liboracle.so"
 REF_LIB = ORACLE_DIR / "_ref" / "libvsref.so"
 REF_ENGINE = ORACLE_DIR / "_ref" / "ref_engine"          # Release-like build of the reference's setup + engine
 REF_ENGINE_G = ORACLE_DIR / "_ref" / "ref_engine_g"      # the same with -G (the reference CMake's default)
+MAIN_ON_MIRROR = ORACLE_DIR / "_ref" / "main_on_mirror"  # the reference's main.cu against the C++ mirror headers
 # Where oracle/Makefile.ref finds the reference sources: VOCALSIM_REFERENCE, else
 # the build recipe's default location.  Only build() reads it.
 REFERENCE_TREE = Path(os.environ.get("VOCALSIM_REFERENCE", "/root/reference"))
@@ -41,6 +42,15 @@ def build(force: bool = False) -> None:
     if REFERENCE_TREE.exists() and (force or not (REF_LIB.exists() and REF_ENGINE.exists() and REF_ENGINE_G.exists())):
         subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "-f", "Makefile.ref",
                         f"REF={REFERENCE_TREE}", "all"], check=True)
+
+
+def build_main_on_mirror(force: bool = False) -> None:
+    """Compile the reference's own driver (src/main.cu, unchanged) against the
+    library's C++ mirror headers; needs the reference tree and the built
+    libvocalsim_b200.so."""
+    if REFERENCE_TREE.exists() and (force or not MAIN_ON_MIRROR.exists()):
+        subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "-f", "Makefile.ref", f"REF={REFERENCE_TREE}",
+                        "main_on_mirror"], check=True)
 
 
 def lib() -> C.CDLL:

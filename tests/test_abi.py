@@ -58,9 +58,12 @@ def test_source_table_matches_oracle(source):
 def test_tile_shapes_listed():
     shapes = V.tile_shapes()
     assert len(shapes) >= 4
-    assert all(r > 0 and c % 30 == 0 for r, c in shapes)     # strips commit 30 columns per warp
+    *strips, cluster = shapes
+    assert all(r > 0 and c % 30 == 0 for r, c in strips)     # strips commit 30 columns per warp
+    assert cluster == (0, 0)                                  # the last shape: one tube per cluster
     steps = [V.tile_shape_steps(i) for i in range(len(shapes))]
-    assert set(steps) == {1, 2} and steps.count(2) >= 8     # single-step and two-step shapes
+    assert set(steps[:-1]) == {1, 2} and steps.count(2) >= 8   # single-step and two-step shapes
+    assert steps[-1] == 0                                     # the cluster kernel runs a whole run per launch
     assert V.load_library().vs_tile_shape_steps(len(shapes), None) == 1
 
 

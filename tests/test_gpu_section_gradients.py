@@ -40,27 +40,36 @@ TWO_MASS = dict(source_type=V.SRC_TMM, tmm_ps_pa=800.0, tmm_f64=1)
 # the FP64 oracle only check gradients of a forward that tracks it.
 @pytest.mark.parametrize("seed,source", [(0, "gauss"), (1, "gauss"), (2, "two_mass")])
 def test_section_gradients_match_fd(seed, source, cuda_ok):
-    adj, fd = _directional(seed, 2000, TWO_MASS if source == "two_mass" else {})
+    adj, fd, _ = _directional(seed, 2000, TWO_MASS if source == "two_mass" else {})
     assert abs(adj - fd) <= TOL * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"
 
 
 # The 20 ms gradient workload (13230 steps, checkpoints every 512).  Over this
 # horizon the FP32 fields' rounding, fed back through the self-oscillating
-# two-mass source, moves the gradient of the FP32 system itself: central
-# differences of the FP32 oracle with h = 1e-2 .. 3e-4 scatter by about 2%
-# around the FP64 value.  The adjoint is checked against the FP64 central
-# difference with that bound.
-TOL_20MS = 2e-2
+# two-mass source, moves the gradient of the FP32 system itself.  The test
+# measures that floor: central differences of the FP32 oracle (the same
+# discrete system in the reference's FP32 arithmetic) at h = 1e-2 .. 3e-4
+# against the FP64 central difference.  Their largest relative distance is
+# the precision an FP32 forward can give this gradient; the adjoint (FP32
+# forward, FP64 accumulation) is held to it, and never to less than 1e-3.
+FD32_STEPS = (1e-2, 3e-3, 1e-3, 3e-4)
 
 
 def test_section_gradients_20ms_two_mass(cuda_ok):
-    adj, fd = _directional(3, 13230, TWO_MASS, every=512)
-    assert abs(adj - fd) <= TOL_20MS * abs(fd), f"adjoint {adj:.9e} vs finite difference {fd:.9e}"
+    adj, fd, fd32 = _directional(3, 13230, TWO_MASS, every=512, fd32_h=FD32_STEPS)
+    scatter = max(abs(v - fd) / abs(fd) for v in fd32.values())
+    # the floor is real: the FP32 system itself misses the 1e-3 gradient bound
+    assert scatter > TOL, (scatter, fd32, fd)
+    err = abs(adj - fd) / abs(fd)
+    assert err <= scatter, f"adjoint {adj:.9e} vs FP64 finite difference {fd:.9e}: {err:.3e} > FP32 floor {scatter:.3e}"
 
 
-def _directional(seed, steps, extra, every=256):
-    """(adjoint, FP64 central difference) of the spectral loss along a random
-    relative direction of the 44 widths, 44 depths and z_inv."""
+def _directional(seed, steps, extra, every=256, fd32_h=()):
+    """(adjoint, FP64 central difference, {h: FP32 central difference}) of the
+    spectral loss along a random relative direction of the 44 widths, 44
+    depths and z_inv.  The oracle runs go to host threads (ctypes releases
+    the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
     kw, L, A, p, g, M, target = _setup(steps, **extra)
     z0 = float(M.nominal["dims"]["z_inv_val"])
     w = M.width0.clone().requires_grad_(True)
@@ -80,12 +89,20 @@ def _directional(seed, steps, extra, every=256):
     adj = float((w.grad * M.width0 * dw).sum() + (d.grad * M.depth0 * dd).sum() + z.grad[0] * z0 * dz)
 
     po, go = O.params(**kw), O.Geometry(L, A)
+    with torch.no_grad():
+        maps = {h: [m.numpy() for m in M.maps(M.width0 * (1 + h * dw), M.depth0 * (1 + h * dd))]
+                for h in {H_REL, -H_REL, *fd32_h, *[-x for x in fd32_h]}}
 
-    def loss_at(h):
+    def loss_at(h, prec):
+        mp, mx, my = maps[h]
+        run = O.run_maps_f64 if prec == "f64" else O.run_maps_f32
+        t = run(po, go, steps, mp, mx, my, z0 * (1 + h * dz))
         with torch.no_grad():
-            mp, mx, my = M.maps(M.width0 * (1 + h * dw), M.depth0 * (1 + h * dd))
-            t = O.run_maps_f64(po, go, steps, mp.numpy(), mx.numpy(), my.numpy(), z0 * (1 + h * dz))
-            return float(spectral_loss(torch.from_numpy(t), target, FS))
+            return float(spectral_loss(torch.from_numpy(np.asarray(t, np.float64)), target, FS))
 
-    fd = (loss_at(H_REL) - loss_at(-H_REL)) / (2 * H_REL)
-    return adj, fd
+    jobs = [(H_REL, "f64"), (-H_REL, "f64")] + [(s * h, "f32") for h in fd32_h for s in (1, -1)]
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        vals = dict(zip(jobs, ex.map(lambda j: loss_at(*j), jobs)))
+    fd = (vals[(H_REL, "f64")] - vals[(-H_REL, "f64")]) / (2 * H_REL)
+    fd32 = {h: (vals[(h, "f32")] - vals[(-h, "f32")]) / (2 * h) for h in fd32_h}
+    return adj, fd, fd32

@@ -1,0 +1,16 @@
+// FDTDSolver.h -- the reference header of this name for code written against
+// the reference (its main.cu builds unchanged with this directory in place of
+// the reference's include/): the class of the C++ mirror over the C ABI of
+// libvocalsim_b200 (cpp/vocalsim_b200.hpp), in the global namespace.
+#pragma once
+
+#include "SimulationUnits.h"
+#include "../vocalsim_b200.hpp"
+
+using vsb::FDTDSolver;
+using vsb::TubeGeometry;
+using vsb::TubeDepth;
+using vsb::GlottalExcitations;
+
+#define SIMULATION_2D 0
+#define SIMULATION_2_5D 1

@@ -17,7 +17,12 @@
 // vs_status (the reference prints and continues, SimulationParams.h:17-24).
 #pragma once
 
+#include <chrono>
+#include <cmath>
 #include <cstdint>
+#include <fstream>
+#include <iostream>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -31,6 +36,7 @@ class Error : public std::runtime_error {
 public:
     Error(int status, const std::string& where)
         : std::runtime_error(where + ": " + vs_last_error()), status_(status) {}
+    Error(int status, const char* what) : std::runtime_error(what), status_(status) {}
     int status() const { return status_; }
 
 private:
@@ -89,6 +95,39 @@ public:
         if (len_.size() != area_.size()) throw std::invalid_argument("one area per segment length");
     }
 
+    // The file the reference's constructor picks (TubeGeometry.cu:57-74):
+    // with tube_geometry != 0, vowel 1 / 2 / 3 -> vocaltract_a / _i / _u.txt and
+    // any other vowel -> cylindrical-tube.txt (the reference's `else` binds to
+    // the inner if).  tube_geometry == 0 selects no file there; it is rejected.
+    static std::string data_file(int tube_geometry, int vowel_type) {
+        if (!tube_geometry)
+            throw Error(VS_ERR_INVALID_ARG, "tube_geometry 0 selects no area-function file (TubeGeometry.cu:60-74)");
+        switch (vowel_type) {
+            case 1: return "vocaltract_a.txt";
+            case 2: return "vocaltract_i.txt";
+            case 3: return "vocaltract_u.txt";
+            default: return "cylindrical-tube.txt";
+        }
+    }
+
+    // Whitespace-separated "segment_length_cm area_cm2" pairs, read with
+    // operator>> into floats as the reference does (TubeGeometry.cu:83-88).
+    static TubeGeometry from_file(const std::string& path) {
+        std::ifstream f(path);
+        if (!f.is_open()) throw Error(VS_ERR_INVALID_ARG, "cannot open area-function file " + path);
+        std::vector<float> len, area;
+        float l, a;
+        while (f >> l >> a) {
+            len.push_back(l);
+            area.push_back(a);
+        }
+        if (len.empty()) throw Error(VS_ERR_GEOMETRY, "no sections in " + path);
+        return TubeGeometry(std::move(len), std::move(area));
+    }
+
+    const std::vector<float>& segment_length_cm() const { return len_; }
+    const std::vector<float>& cross_sectional_area_cm2() const { return area_; }
+
     vs_geometry view() const {
         vs_geometry g{};
         g.n_sections = (int32_t)len_.size();
@@ -103,13 +142,23 @@ private:
 
 // FDTDSolver(SimulationParams) + setupWaveSolver() (FDTDSolver.cu:71-83,
 // 289-476): builds the maps on the host (bit-identical to the reference's)
-// and exposes the fields the engines read.
+// and exposes the fields the engines read.  Without an explicit geometry a
+// tube simulation reads the area function the way the reference does, from
+// data_dir + TubeGeometry::data_file(tube_geometry, vowel_type); data_dir
+// defaults to the reference's relative path ../../data/tube-geometry/.
 class FDTDSolver {
 public:
     FDTDSolver(const SimulationParams& params, const TubeGeometry* geometry = nullptr)
         : params_(params), geometry_(geometry) {}
 
+    std::string data_dir = "../../data/tube-geometry/";
+
     void setupWaveSolver() {
+        if (!geometry_ && params_.getSimulationType() == 1) {
+            owned_ = std::make_shared<TubeGeometry>(TubeGeometry::from_file(
+                data_dir + TubeGeometry::data_file(params_.getTubeGeometry(), params_.getVowelType())));
+            geometry_ = owned_.get();
+        }
         vs_geometry g{};
         const vs_geometry* gp = nullptr;
         if (geometry_) {
@@ -153,6 +202,48 @@ public:
 private:
     SimulationParams params_;
     const TubeGeometry* geometry_;
+    std::shared_ptr<TubeGeometry> owned_;     // the area function read in setupWaveSolver
+};
+
+// TubeDepth (TubeDepth.cu:82-265): the depth maps of a set-up solver.  The
+// reference computes them with its depth kernels inside setupWaveSolver; here
+// vs_build_maps has already produced the same maps, so setTubeDepth() copies
+// them out of the solver.
+class TubeDepth {
+public:
+    explicit TubeDepth(FDTDSolver& solver) : solver_(solver) {}
+
+    void setTubeDepth() {
+        if (solver_.depthP.empty()) solver_.setupWaveSolver();
+        depthP = solver_.depthP;
+        depthX = solver_.depthX;
+        depthY = solver_.depthY;
+    }
+
+    float min_depth = 0.001f;           // TubeDepth.cu:90
+    float open_space_depth = 0.50f;     // TubeDepth.cu:91
+    std::vector<float> depthP, depthX, depthY;
+
+private:
+    FDTDSolver& solver_;
+};
+
+// GlottalExcitations (GlottalExcitations.cu:9-52): the per-step source table
+// (0 sine, 1 Gaussian, 2 two-mass: zeros, the model runs in the engine).
+class GlottalExcitations {
+public:
+    void setExcitationVelocity(int source_type, int num_steps, double dt) {
+        vs_params p{};
+        check(vs_params_init(&p), "vs_params_init");
+        p.source_type = source_type;
+        p.srate_mul = (int)std::lround(1.0 / (dt * 44100.0));
+        excitation_.assign((size_t)std::max(num_steps, 0), 0.0f);
+        if (num_steps > 0) check(vs_source_table(&p, num_steps, excitation_.data()), "vs_source_table");
+    }
+    std::vector<float> getExcitationVelocity() const { return excitation_; }
+
+private:
+    std::vector<float> excitation_;
 };
 
 // Drop-in for FDTDEngineCPU / FDTDEngineEigen (FDTDEngineCPU.cpp:4-304,
@@ -189,9 +280,63 @@ public:
 
     std::vector<float> record_pressure;   // FDTDEngineCPU.h:69
 
+protected:
+    struct Arithmetic {
+        int engine;     // VS_ENGINE_CPU or VS_ENGINE_EIGEN
+    };
+    FDTDEngineB200(FDTDSolver& solver, Arithmetic a) : solver_(solver) {
+        vs_params p = solver.params().raw();
+        p.engine = a.engine;
+        vs_geometry g{};
+        const vs_geometry* gp = nullptr;
+        if (solver.geometry()) {
+            g = solver.geometry()->view();
+            gp = &g;
+        }
+        check(vs_create(&p, gp, &h_), "vs_create");
+    }
+
+    // startSolverEngine of the reference engines: run, print the loop time,
+    // write record_pressure one value per line to ../../results/
+    // (FDTDEngineCPU.cpp:290-303, 435-450).
+    void run_and_save(const std::string& results_path) {
+        const auto t0 = std::chrono::steady_clock::now();
+        startSolverEngine();
+        const std::chrono::duration<double> dt = std::chrono::steady_clock::now() - t0;
+        std::cout << "Elapsed time [in seconds]: " << dt.count() << " s" << std::endl;
+        std::ofstream out(results_path);
+        if (!out) throw Error(VS_ERR_INVALID_ARG, "cannot write " + results_path);
+        for (float v : record_pressure) out << v << "\n";
+    }
+
 private:
     FDTDSolver& solver_;
     vs_solver* h_ = nullptr;
+};
+
+// The reference's engine classes by name (FDTDEngineCPU.h, FDTDEngineEigen.h),
+// so its driver (main.cu:126-146) builds unchanged against the headers in
+// cpp/include: both run on the GPU, in the CPU engine's or the Eigen engine's
+// rounding, and save record_pressure where the reference does.
+class FDTDEngineCPU : public FDTDEngineB200 {
+public:
+    explicit FDTDEngineCPU(FDTDSolver& solver, bool validationFlag = false)
+        : FDTDEngineB200(solver, Arithmetic{VS_ENGINE_CPU}) {
+        (void)validationFlag;
+    }
+    void startSolverEngine() { run_and_save(results_path); }
+    std::string results_path = "../../results/recorded-pressure.txt";
+};
+
+class FDTDEngineEigen : public FDTDEngineB200 {
+public:
+    FDTDEngineEigen(FDTDEngineCPU& cpu, FDTDSolver& solver, bool validationFlag = false)
+        : FDTDEngineB200(solver, Arithmetic{VS_ENGINE_EIGEN}) {
+        (void)cpu;
+        (void)validationFlag;
+    }
+    void startSolverEngine() { run_and_save(results_path); }
+    std::string results_path = "../../results/recorded-pressure.txt";
 };
 
 }  // namespace vsb

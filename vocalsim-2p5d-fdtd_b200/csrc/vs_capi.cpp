@@ -117,6 +117,8 @@ struct vs_batch {
     bool wall = false;                     // some tube has the coupled wall oscillator
     bool fast = false;                     // reciprocal-form arithmetic (vs_params::fast_math)
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
+    int cluster_state = 0;                 // cluster shape: 0 = not checked, 1 = fits, -1 = does not
+    ClusterConfig cluster{};
     // adjoint: checkpoints of the last checkpointed forward, history, adjoint planes
     int64_t ck_steps = 0;                  // steps of the checkpointed forward (0 = none)
     int ck_every = 0;
@@ -252,8 +254,23 @@ size_t smem_optin_limit(int device) {
     return (size_t)v;
 }
 
+// The cluster shape runs one tube without the coupled wall oscillator whose
+// band of rows fits a CTA's shared memory.
+bool cluster_fits(const vs_batch* b) {
+    if (b->cluster_state == 0) {
+        vs_batch* m = const_cast<vs_batch*>(b);
+        m->cluster_state = -1;
+        if (b->grids.size() == 1 && !b->wall) {
+            const TubeGrid& g = b->grids[0];
+            if (cluster_config(g.H, g.W, g.pitch, b->fast, &m->cluster)) m->cluster_state = 1;
+        }
+    }
+    return b->cluster_state == 1;
+}
+
 bool shape_fits(const vs_batch* b, int shape) {
     const int kind = tile_shape(shape).kind;
+    if (kind == SHAPE_CLUSTER) return cluster_fits(b);
     if (b->wall && (kind == SHAPE_QUAD || kind == SHAPE_QUAD2)) return false;   // no wall-oscillator variant
     // two-step kernels: fast_math only
     if (kind == SHAPE_QUAD2 && !b->fast) return false;
@@ -272,6 +289,8 @@ int single_step_shape(const vs_batch* b) {
 }
 
 int default_shape(const vs_batch* b) {
+    // a single tube keeps its state on one thread-block cluster for the whole run
+    if (b->grids.size() == 1 && shape_fits(b, cluster_shape())) return cluster_shape();
     int64_t cells = 0;
     for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
     const int two = cells >= kSmallGridCells ? kTwoStepShape : kTwoStepSmallShape;
@@ -340,6 +359,7 @@ Tile* make_tiles(vs_batch* b, int shape, int* n) {
 }
 
 void build_tiles(vs_batch* b, int shape) {
+    if (tile_shape(shape).kind == SHAPE_CLUSTER) return;     // the cluster kernel needs no tile list
     if (b->tiles_shape == shape && b->d_tiles) return;
     int n = 0;
     Tile* d = make_tiles(b, shape, &n);
@@ -645,6 +665,10 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
 // count ends with one launch of the batch's single-step shape, so the state
 // of the final step is in its parity set (bsel = 0) when the call returns.
 void issue_steps(vs_batch* b, int64_t count) {
+    if (tile_shape(b->shape).kind == SHAPE_CLUSTER) {
+        ck(launch_cluster_run(b->d_tubes, b->d_rs, count, b->fast, b->cluster, b->stream), "cluster launch");
+        return;
+    }
     const bool two = tile_shape(b->shape).kind == SHAPE_QUAD2;
     int64_t done = 0;
     if (count >= kChunk) {
@@ -1404,7 +1428,8 @@ int vs_tile_shape(int32_t i, int32_t* rows, int32_t* cols) {
 int vs_tile_shape_steps(int32_t i, int32_t* steps_per_launch) {
     if (i < 0 || i >= tile_shape_count() || !steps_per_launch)
         return set_error(VS_ERR_INVALID_ARG, "vs_tile_shape_steps arguments");
-    *steps_per_launch = tile_shape(i).kind == SHAPE_QUAD2 ? 2 : 1;
+    const int kind = tile_shape(i).kind;
+    *steps_per_launch = kind == SHAPE_QUAD2 ? 2 : kind == SHAPE_CLUSTER ? 0 : 1;
     return VS_OK;
 }
 

@@ -1,0 +1,382 @@
+// vs_cluster.cu -- one tube on one thread-block cluster, a whole run per launch.
+//
+// A single tube is too small to fill the GPU with one launch per step: the
+// graph-replayed step kernels spend most of each step in launch and memory
+// latency.  This kernel keeps the tube's state on chip for the whole run.
+// The interior rows are split into C contiguous bands, one CTA of a cluster
+// of C (up to 16) per band; each CTA holds in shared memory the P, Vx and Vy
+// of its rows, the maps and codes it needs, and two ghost rows:
+//   top    (row r0 - 1): P, Vx, Vy; its P' is recomputed locally each step
+//          with the same inputs and expressions as its owner uses, so only
+//          its velocities arrive from the CTA above
+//   bottom (row r1 + 1): Vy, from the CTA below
+// One step of the reference loop (FDTDEngineCPU.cpp:257-288):
+//   P' of rows r0 - 1 .. r1 (in place; the listener sample is stored)
+//   __syncthreads
+//   V' of rows r0 .. r1 (in place); the threads of the first and last row
+//   store their new velocities into the neighbours' ghost rows (distributed
+//   shared memory); the excitation velocity of the next step is prepared
+//   (table value, or the two-mass step on the new pressure, computed by one
+//   thread of the CTA that owns the excitation cell and sent to every CTA)
+//   cluster barrier (arrive.release / wait.acquire)
+// Ghost rows and the excitation slot are double-buffered by step parity, so a
+// CTA that runs ahead into the next step never overwrites values a neighbour
+// still reads.  At the end every CTA writes its rows back to the parity set
+// of the final step; the other set is not touched.
+//
+// Arithmetic per cell is that of the strip and quad-strip kernels
+// (vs_cellmath.cuh): reference rounding (fast_math = 0), or the reciprocal
+// form with the per-cell descriptor tables (fast_math = 1).  The row masks of
+// the strip kernels are replaced by each cell's own velocity class; where a
+// strip kernel applies a shortened or a full form, both give the same value
+// (they differ only by operations with exact 0 / 1 operands).
+//
+// No wall oscillator and no history capture (those runs use the step
+// kernels).  Every thread executes the same barrier sequence; there are no
+// spin waits.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "vs_cellmath.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace vsb {
+namespace {
+
+// Shared-memory layout of one CTA (rows of `pitch` elements).
+struct ClusterLayout {
+    int pitch, R;           // R = rows of the tallest band
+    // float row offsets
+    int P, Vx, gVx, Vy, gVyT, gVyB, dP, dX, dY;
+    int nfloat_rows;
+    // byte rows: code, velocity class, descriptor (fast_math)
+    int nbyte_rows;
+    size_t bytes;
+};
+
+__host__ __device__ inline ClusterLayout cluster_layout(int pitch, int R, bool fast) {
+    ClusterLayout L{};
+    L.pitch = pitch;
+    L.R = R;
+    int o = 0;
+    L.P = o;    o += R + 1;     // rows r0-1 .. r1
+    L.Vx = o;   o += R;         // rows r0 .. r1
+    L.gVx = o;  o += 2;         // ghost top row, two slots
+    L.Vy = o;   o += R;
+    L.gVyT = o; o += 2;
+    L.gVyB = o; o += 2;         // ghost bottom row, two slots
+    L.dP = o;   o += R + 1;     // rows r0-1 .. r1
+    L.dX = o;   o += R + 1;
+    L.dY = o;   o += R + 2;     // rows r0-1 .. r1+1
+    L.nfloat_rows = o;
+    L.nbyte_rows = 3 * (R + 1);
+    // floats, then 2 x 256 float4 descriptor tables (fast_math), sigma[16],
+    // the two excitation slots, then the byte rows
+    size_t b = (size_t)o * pitch * sizeof(float);
+    b += fast ? 2 * kDescEntries * sizeof(float4) : 0;
+    b += 16 * sizeof(float) + 2 * sizeof(float) + 8;
+    b += (size_t)L.nbyte_rows * pitch;
+    L.bytes = (b + 127) / 128 * 128;
+    return L;
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(512, 1)
+cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_t nsteps, int R) {
+    extern __shared__ __align__(16) unsigned char c_smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int k = (int)cluster.block_rank();
+    const TubeDev* __restrict__ T = Tp;
+    const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
+    const ClusterLayout L = cluster_layout(pitch, R, FAST);
+    float* sf = reinterpret_cast<float*>(c_smem);
+    float4* tabA = reinterpret_cast<float4*>(sf + (size_t)L.nfloat_rows * pitch);
+    float4* tabB = tabA + (FAST ? kDescEntries : 0);
+    float* sSig = reinterpret_cast<float*>(tabB + (FAST ? kDescEntries : 0));
+    float* sExe = sSig + 16;
+    unsigned char* sb = reinterpret_cast<unsigned char*>(sExe + 4);
+    auto row = [&](int base, int i) { return sf + (size_t)(base + i) * pitch; };
+    unsigned char* sCode = sb;                          // rows i = 0..R (r0-1 .. r1)
+    unsigned char* sCls = sb + (size_t)(R + 1) * pitch;
+    unsigned char* sDesc = sb + (size_t)2 * (R + 1) * pitch;
+
+    // band of this CTA
+    const int NR = H - 2;
+    const int r0 = 1 + (int)(((int64_t)k * NR) / C);
+    const int r1 = (int)(((int64_t)(k + 1) * NR) / C);      // inclusive
+    const int Rk = r1 - r0 + 1;
+    const int64_t n0 = rs->step;
+    const int64_t run_start = rs->run_start;
+    float* __restrict__ trace = rs->trace;
+    const int par0 = (int)(n0 & 1);
+    const int64_t pl = T->plane;
+    const float* __restrict__ gP = T->P[0] + par0 * pl;
+    const float* __restrict__ gVx = gP + 2 * pl;
+    const float* __restrict__ gVy = gP + 4 * pl;
+    const float* __restrict__ gdP = T->dP;
+    const float* __restrict__ gdX = gdP + pl;
+    const float* __restrict__ gdY = gdP + 2 * pl;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+
+    // ---- load the band, its ghost rows and the maps
+    for (int c = tid; c < pitch; c += nthr) {
+        for (int i = 0; i <= Rk + 1; ++i) {
+            const int r = r0 - 1 + i;                     // 0 .. H-1
+            const int64_t o = (int64_t)r * pitch + c;
+            const float p = gP[o], vx = gVx[o], vy = gVy[o];
+            if (i <= Rk) {
+                row(L.P, i)[c] = p;
+                row(L.dP, i)[c] = gdP[o];
+                row(L.dX, i)[c] = gdX[o];
+                const int kc = T->code[o];
+                sCode[(size_t)i * pitch + c] = (unsigned char)kc;
+                if (FAST) sDesc[(size_t)i * pitch + c] = T->desc[o];
+                const int kr = c + 1 < pitch ? T->code[o + 1] : VS_CELL_DEAD;
+                const int kt = r >= 1 ? T->code[o - pitch] : VS_CELL_DEAD;
+                sCls[(size_t)i * pitch + c] = (unsigned char)velocity_class(kc, kr, kt);
+            }
+            row(L.dY, i)[c] = gdY[o];
+            if (i == 0) {
+                row(L.gVx, par0)[c] = vx;
+                row(L.gVyT, par0)[c] = vy;
+                row(L.gVx, par0 ^ 1)[c] = 0.0f;
+                row(L.gVyT, par0 ^ 1)[c] = 0.0f;
+            } else if (i <= Rk) {
+                row(L.Vx, i - 1)[c] = vx;
+                row(L.Vy, i - 1)[c] = vy;
+            } else {
+                row(L.gVyB, par0)[c] = vy;
+                row(L.gVyB, par0 ^ 1)[c] = 0.0f;
+            }
+        }
+    }
+    if (FAST)
+        for (int j = tid; j < 2 * kDescEntries; j += nthr) tabA[j] = T->desc_a[j];   // desc_b = desc_a + 256
+    if (tid < 16) sSig[tid] = tid < 13 ? T->sigma[tid] : 0.0f;
+
+    const bool tmm = flags & TUBE_TMM, tmm64 = flags & TUBE_TMM64;
+    const bool exc_owner = tmm && T->exc_y >= r0 && T->exc_y <= r1;
+    const int exc_i = T->exc_y - (r0 - 1), exc_x = T->exc_x;
+    TmmState s32{};
+    TmmState64 s64{};
+    if (exc_owner && tid == 0) {
+        if (tmm64) s64 = T->tmm64[par0];
+        else s32 = T->tmm[par0];
+    }
+    auto tmm_next = [&](float p1) -> float {
+        return tmm64 ? tmm_step64(T->tmmd, s64, p1) : tmm_step(T->tmmc, s32, p1);
+    };
+    auto send_exe = [&](int slot, float e) {
+        for (int q = 0; q < C; ++q) *cluster.map_shared_rank(sExe + slot, q) = e;
+    };
+    __syncthreads();
+    cluster.sync();                                       // every CTA of the cluster is running
+    if (tid == 0) {
+        if (tmm) {
+            if (exc_owner) send_exe(par0, tmm_next(row(L.P, exc_i)[exc_x]));
+        } else {
+            sExe[par0] = n0 < T->src_len ? T->src[n0] : 0.0f;
+        }
+    }
+    cluster.sync();
+
+    // neighbours' ghost rows (distributed shared memory)
+    float* up_gVyB = k > 0 ? cluster.map_shared_rank(row(L.gVyB, 0), k - 1) : nullptr;
+    float* dn_gVx = k + 1 < C ? cluster.map_shared_rank(row(L.gVx, 0), k + 1) : nullptr;
+    float* dn_gVyT = k + 1 < C ? cluster.map_shared_rank(row(L.gVyT, 0), k + 1) : nullptr;
+
+    const float K1 = T->K1, bco = T->bcoef;
+    const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
+    const float zval = T->zinv, dir0 = T->dir0, dir1 = T->dir1, dir2 = T->dir2, dir3 = T->dir3;
+    const int lis_y = T->lis_y, lis_x = T->lis_x;
+    const bool lis_here = lis_y >= r0 && lis_y <= r1;
+    const int64_t n_end = n0 + nsteps;
+
+    for (int64_t n = n0; n < n_end; ++n) {
+        const int p = (int)(n & 1), q = p ^ 1;
+        // ---- P' of rows r0-1 .. r1 (FDTDEngineCPU.cpp:316-339)
+        for (int c = 1 + tid; c <= W - 2; c += nthr) {
+            for (int i = (r0 == 1 ? 1 : 0); i <= Rk; ++i) {
+                const float vx = i == 0 ? row(L.gVx, p)[c] : row(L.Vx, i - 1)[c];
+                const float vxl = i == 0 ? row(L.gVx, p)[c - 1] : row(L.Vx, i - 1)[c - 1];
+                const float vy = i == 0 ? row(L.gVyT, p)[c] : row(L.Vy, i - 1)[c];
+                const float vyb = i == Rk ? row(L.gVyB, p)[c] : row(L.Vy, i)[c];
+                const float* dXr = row(L.dX, i);
+                const float ux = fmul(vx, dXr[c]), uxl = fmul(vxl, dXr[c - 1]);
+                const float uy = fmul(vy, row(L.dY, i)[c]), uyb = fmul(vyb, row(L.dY, i + 1)[c]);
+                const float dp = row(L.dP, i)[c];
+                float* Pr = row(L.P, i);
+                float pn;
+                if constexpr (FAST) {
+                    // (P dP - K1 S) / ((1 + s) dP) = (P - K1 S / dP) g
+                    const float ks = fmul(K1, fadd(fsub(ux, uxl), fsub(uy, uyb)));
+                    pn = __fmaf_rn(-ks, rcp_approx(dp), Pr[c]);
+                    const int d = sDesc[(size_t)i * pitch + c];
+                    if (d) pn = fmul(pn, tabA[d].z);
+                } else {
+                    const float num = fsub(fmul(Pr[c], dp), fmul(K1, fadd(fsub(ux, uxl), fsub(uy, uyb))));
+                    const int tc = sCode[(size_t)i * pitch + c] & CODE_TYPE_MASK;
+                    float den = dp;                       // sigma = 0: (1 + 0) dP == dP
+                    if (tc != VS_CELL_AIR) {
+                        const float s = sSig[tc];
+                        den = eigen ? fadd(fmul(s, dp), dp) : fmul(fadd(1.0f, s), dp);
+                    }
+                    pn = fdiv_z(num, den);
+                    if (dirichlet && tc == VS_CELL_NOPRESSURE) pn = 0.0f;
+                }
+                Pr[c] = pn;
+                if (i >= 1 && lis_here && r0 - 1 + i == lis_y && c == lis_x) trace[n - run_start] = pn;
+            }
+        }
+        __syncthreads();
+        // ---- excitation velocity of the next step
+        if (tid == 0 && n + 1 < n_end) {
+            if (tmm) {
+                if (exc_owner) send_exe(q, tmm_next(row(L.P, exc_i)[exc_x]));
+            } else {
+                sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+            }
+        }
+        const float exeV = sExe[p];
+        // ---- V' of rows r0 .. r1 (FDTDEngineCPU.cpp:364-410)
+        for (int c = 1 + tid; c <= W - 2; c += nthr) {
+            for (int i = 1; i <= Rk; ++i) {
+                const float* Pr = row(L.P, i);
+                const float pc = Pr[c], pr = Pr[c + 1], pt = row(L.P, i - 1)[c];
+                float* Vxr = row(L.Vx, i - 1);
+                float* Vyr = row(L.Vy, i - 1);
+                float vx = Vxr[c], vy = Vyr[c];
+                const int cls = sCls[(size_t)i * pitch + c];
+                if constexpr (FAST) {
+                    // V' = al (V - bco (P'n - P'c)) + zo P'c - zi P'n + ce exeV
+                    vx = fsub(vx, fmul(bco, fsub(pr, pc)));
+                    vy = fsub(vy, fmul(bco, fsub(pt, pc)));
+                    const int d = sDesc[(size_t)i * pitch + c];
+                    if (d) {
+                        const float4 da = tabA[d];
+                        vx = fmul(vx, da.x);
+                        vy = fmul(vy, da.y);
+                        if (cls == V_GENERIC) {
+                            const float4 db = tabB[d];
+                            vx = __fmaf_rn(da.w, exeV, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pc, vx)));
+                            vy = __fmaf_rn(-db.w, pt, __fmaf_rn(db.z, pc, vy));
+                        }
+                    }
+                } else if (cls == V_GENERIC) {
+                    const int kc = sCode[(size_t)i * pitch + c], kr = sCode[(size_t)i * pitch + c + 1];
+                    const int kt = sCode[(size_t)(i - 1) * pitch + c];
+                    const VelocityOut v = velocity_generic(kc, kr, kt, pc, pr, pt, vx, vy, exeV, sSig, zval, bco,
+                                                           dir0, dir1, dir2, dir3);
+                    vx = v.vx;
+                    vy = v.vy;
+                } else {
+                    vx = fsub(vx, fmul(bco, fsub(pr, pc)));
+                    vy = fsub(vy, fmul(bco, fsub(pt, pc)));
+                    if (cls == V_BETA1) {
+                        const float sc = sSig[sCode[(size_t)i * pitch + c] & CODE_TYPE_MASK];
+                        vx = fdiv_z(vx, fadd(1.0f, fmaxf(sc, sSig[sCode[(size_t)i * pitch + c + 1] & CODE_TYPE_MASK])));
+                        vy = fdiv_z(vy, fadd(1.0f, fmaxf(sc, sSig[sCode[(size_t)(i - 1) * pitch + c] & CODE_TYPE_MASK])));
+                    }
+                }
+                Vxr[c] = vx;
+                Vyr[c] = vy;
+                if (i == Rk && dn_gVx) {
+                    dn_gVx[(size_t)q * pitch + c] = vx;
+                    dn_gVyT[(size_t)q * pitch + c] = vy;
+                }
+                if (i == 1 && up_gVyB) up_gVyB[(size_t)q * pitch + c] = vy;
+            }
+        }
+        cluster.sync();
+    }
+
+    // ---- the state of step n_end back to its parity set
+    const int pe = (int)(n_end & 1);
+    float* __restrict__ oP = T->P[0] + pe * pl;
+    float* __restrict__ oVx = oP + 2 * pl;
+    float* __restrict__ oVy = oP + 4 * pl;
+    for (int c = 1 + tid; c <= W - 2; c += nthr)
+        for (int i = 1; i <= Rk; ++i) {
+            const int64_t o = (int64_t)(r0 - 1 + i) * pitch + c;
+            oP[o] = row(L.P, i)[c];
+            oVx[o] = row(L.Vx, i - 1)[c];
+            oVy[o] = row(L.Vy, i - 1)[c];
+        }
+    if (exc_owner && tid == 0) {
+        if (tmm64) T->tmm64[pe] = s64;
+        else T->tmm[pe] = s32;
+    }
+    if (k == 0 && tid == 0) rs->step = n_end;    // every CTA read rs->step before the first cluster barrier
+}
+
+}  // namespace
+
+size_t cluster_smem_bytes(int pitch, int rows_max, bool fast) { return cluster_layout(pitch, rows_max, fast).bytes; }
+
+// Cluster size, threads and shared memory for one tube of H x W (pitch), or
+// false when no cluster of at least 4 CTAs fits on this device.
+bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out) {
+    const int NR = H - 2;
+    if (NR < 4) return false;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    const void* fn = fast ? (const void*)cluster_kernel<true> : (const void*)cluster_kernel<false>;
+    const int threads = std::min(512, (W + 31) / 32 * 32);
+    for (int C : {16, 8, 4}) {
+        if (C > NR) continue;
+        const int R = (NR + C - 1) / C;
+        const size_t smem = cluster_layout(pitch, R, fast).bytes;
+        if (smem > (size_t)optin) continue;
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) continue;
+        if (C > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+            continue;
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(C);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) != cudaSuccess || nclusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        out->ctas = C;
+        out->threads = threads;
+        out->rows_max = R;
+        out->smem = smem;
+        return true;
+    }
+    cudaGetLastError();
+    return false;
+}
+
+cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps, bool fast, const ClusterConfig& c,
+                               cudaStream_t stream) {
+    if (steps <= 0) return cudaSuccess;
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c.ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(c.ctas);
+    cfg.blockDim = dim3(c.threads);
+    cfg.dynamicSmemBytes = c.smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (fast) return cudaLaunchKernelEx(&cfg, cluster_kernel<true>, tube, rs, steps, c.rows_max);
+    return cudaLaunchKernelEx(&cfg, cluster_kernel<false>, tube, rs, steps, c.rows_max);
+}
+
+}  // namespace vsb

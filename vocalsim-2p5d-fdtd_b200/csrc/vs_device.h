@@ -157,7 +157,7 @@ __host__ __device__ inline void classify_strip(CodeAt code, int H, int W, int r0
 // rows per strip, committed columns per strip, warps per CTA.  Bands: rows
 // per band (a band spans the full frame width; cols = 0), warps per CTA.
 // Quad strips have no wall-oscillator variant.
-enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1, SHAPE_QUAD = 2, SHAPE_QUAD2 = 3 };
+enum : int { SHAPE_STRIP = 0, SHAPE_BAND = 1, SHAPE_QUAD = 2, SHAPE_QUAD2 = 3, SHAPE_CLUSTER = 4 };
 
 // Two-step quad strips of NC columns per lane start at c0 = 30 NC k - NC,
 // commit columns c0 + NC .. c0 + 31 NC - 1 and classify an extended region:
@@ -170,6 +170,24 @@ struct TileShape {
 
 int tile_shape_count();
 TileShape tile_shape(int i);
+// Index of the cluster shape (the last one): a single tube on one
+// thread-block cluster, every step of a run in one launch (vs_cluster.cu).
+int cluster_shape();
+
+// Launch configuration of the cluster kernel for one tube.
+struct ClusterConfig {
+    int ctas = 0, threads = 0, rows_max = 0;
+    size_t smem = 0;
+};
+// Cluster size (16, 8 or 4 CTAs), threads and shared memory for a tube of
+// H x W cells (row pitch `pitch`) on the current device, or false when none
+// fits; sets the kernel attributes it needs.
+bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out);
+// `steps` time steps of the tube at `tube` (device) from RunState::step, in
+// one launch; RunState::step advances by `steps`.  The state must be in its
+// parity set (bsel = 0) and stays there.
+cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps, bool fast, const ClusterConfig& c,
+                               cudaStream_t stream);
 
 // Launch one time step (local index `local` after RunState::step) of every
 // strip or band in `tiles` with the compiled shape `shape`; `wall` selects

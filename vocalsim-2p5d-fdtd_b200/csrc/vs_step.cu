@@ -27,279 +27,11 @@
 
 #include "vs_device.h"
 
+#include "vs_cellmath.cuh"
+
 namespace vsb {
 namespace {
 
-__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
-__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double dsub(double a, double b) { return __dadd_rn(a, -b); }
-__device__ __forceinline__ double dd(float a) { return (double)a; }
-__device__ __forceinline__ float tof(double a) { return __double2float_rn(a); }
-
-constexpr unsigned kFull = 0xffffffffu;
-
-// One step of the Ishizaka-Flanagan two-mass model, TwoMassModel.cpp:90-232,
-// in the reference's mixed float/double precision and operand order.  The
-// reference's host build (g++) forms (rho/2)*fabs(ug) in double.
-__device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1) {
-    const float srate = k.srate;
-    const float two_lg = fmul(2.0f, k.lg);
-    float Ag1 = fadd(k.Ag01, fmul(two_lg, s.x1_curr));
-    float Ag2 = fadd(k.Ag02, fmul(two_lg, s.x2_curr));
-    const float mu12lglg = fmul(fmul(fmul(12.0f, k.mu), k.lg), k.lg);
-    const float Rv1 = fdiv(fmul(mu12lglg, k.d1), fmul(fmul(Ag1, Ag1), Ag1));
-    const float Lg1 = fdiv(fmul(k.rho, k.d1), Ag1);
-    const float Rv2 = fdiv(fmul(mu12lglg, k.d2), fmul(fmul(Ag2, Ag2), Ag2));
-    const float Lg2 = fdiv(fmul(k.rho, k.d2), Ag2);
-    const float thr1 = fdiv(-k.Ag01, two_lg);
-    const float thr2 = fdiv(-k.Ag02, two_lg);
-    const float ug = s.ug_curr, ugo = s.ug_old;
-    const float dug = fsub(ug, ugo);
-    const float half_rho = fdiv(k.rho, 2.0f);
-    float pm1, pm2;
-    if (s.x1_curr > thr1 && s.x2_curr > thr2) {
-        const float q = fdiv(ug, Ag1);
-        const double a = dmul(dmul(dmul(1.37, dd(half_rho)), dd(q)), dd(q));
-        const double b = dmul(0.5, dd(fadd(fmul(Rv1, ug), fmul(fmul(Lg1, srate), dug))));
-        pm1 = tof(dsub(dsub(dd(k.ps), a), b));
-    } else {
-        pm1 = k.ps;
-    }
-    const float fm1 = fmul(fmul(pm1, k.d1), k.lg);
-    if (s.x1_curr > thr1) {
-        if (s.x2_curr > thr2) {
-            const double u = dadd(dmul(dmul(0.5, dd(fadd(Rv1, Rv2))), dd(ug)),
-                                  dd(fmul(fmul(fadd(Lg1, Lg2), dug), srate)));
-            const float v = fmul(fmul(fmul(half_rho, ug), ug),
-                                 fsub(fdiv(1.0f, fmul(Ag2, Ag2)), fdiv(1.0f, fmul(Ag1, Ag1))));
-            pm2 = tof(dsub(dsub(dd(pm1), u), dd(v)));
-        } else {
-            pm2 = k.ps;
-        }
-    } else {
-        pm2 = 0.0f;
-    }
-    const float fm2 = fmul(fmul(pm2, k.d2), k.lg);
-    const float g1 = fdiv(k.Ag01, two_lg), g2 = fdiv(k.Ag02, two_lg);
-    float h1u, r1u, h2u, r2u;
-    if (fadd(s.x1_curr, g1) < 0.0f) { h1u = k.h1; r1u = k.r1c; } else { h1u = 0.0f; r1u = k.r1o; }
-    if (fadd(s.x2_curr, g2) < 0.0f) { h2u = k.h2; r2u = k.r2c; } else { h2u = 0.0f; r2u = k.r2o; }
-    const float s2 = fmul(srate, srate);
-    const float a11 = fadd(fadd(fdiv(fadd(fadd(k.k1, h1u), k.kc), s2), fdiv(r1u, srate)), k.m1);
-    const float a12 = fdiv(-k.kc, s2);
-    const float a21 = a12;
-    const float a22 = fadd(fadd(fdiv(fadd(fadd(k.k2, h2u), k.kc), s2), fdiv(r2u, srate)), k.m2);
-    const float x1 = s.x1_curr, x2 = s.x2_curr;
-    const float e1 = fadd(g1, x1), e2 = fadd(g2, x2);
-    const float sp1 = fadd(fmul(fmul(fmul(fmul(k.k1, k.etak1), x1), x1), x1),
-                           fmul(h1u, fadd(g1, fmul(fmul(fmul(k.etah1, e1), e1), e1))));
-    const float sp2 = fadd(fmul(fmul(fmul(fmul(k.k2, k.etak2), x2), x2), x2),
-                           fmul(h2u, fadd(g2, fmul(fmul(fmul(k.etah2, e2), e2), e2))));
-    const float b1 = fadd(fsub(fsub(fmul(fadd(fmul(2.0f, k.m1), fdiv(r1u, srate)), x1), fmul(k.m1, s.x1_old)),
-                               fdiv(sp1, s2)), fdiv(fm1, s2));
-    const float b2 = fadd(fsub(fsub(fmul(fadd(fmul(2.0f, k.m2), fdiv(r2u, srate)), x2), fmul(k.m2, s.x2_old)),
-                               fdiv(sp2, s2)), fdiv(fm2, s2));
-    float det = fsub(fmul(a11, a22), fmul(a21, a12));
-    if (det == 0.0f) det = 1.0f;
-    const float x1n = fdiv(fsub(fmul(a22, b1), fmul(a12, b2)), det);
-    const float x2n = fdiv(fsub(fmul(a11, b2), fmul(a21, b1)), det);
-    s.x1_old = x1; s.x1_curr = x1n;
-    s.x2_old = x2; s.x2_curr = x2n;
-    Ag1 = fadd(k.Ag01, fmul(two_lg, x1n));
-    Ag2 = fadd(k.Ag02, fmul(two_lg, x2n));
-    float ugn;
-    if (Ag1 < 0.0f || Ag2 < 0.0f) {
-        ugn = 0.0f;
-    } else {
-        const float r = fdiv(Ag2, k.A1);
-        const float f = fdiv(fsub(1.0f, fmul(fmul(2.0f, r), fsub(1.0f, r))), fmul(Ag2, Ag2));
-        const double t1 = dmul(dmul(dd(half_rho), fabs(dd(ug))),
-                               dadd(__ddiv_rn(0.37, dd(fmul(Ag1, Ag1))), dd(f)));
-        const float t2 = fmul(mu12lglg, fadd(fdiv(k.d1, fmul(fmul(Ag1, Ag1), Ag1)),
-                                             fdiv(k.d2, fmul(fmul(Ag2, Ag2), Ag2))));
-        const float Rtot = tof(dadd(t1, dd(t2)));
-        const float Ltot = fmul(k.rho, fadd(fdiv(k.d1, Ag1), fdiv(k.d2, Ag2)));
-        ugn = fdiv(fadd(fdiv(fsub(k.ps, p1), srate), fmul(Ltot, ug)), fadd(fdiv(Rtot, srate), Ltot));
-    }
-    s.ug_old = ug;
-    s.ug_curr = ugn;
-    return ugn;
-}
-
-// The same model step with every quantity in double (tmm_f64), following
-// TwoMassModel.cpp:90-232 operation by operation; the caller's pressure is
-// widened and the flow rounded to float for the field update.
-__device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, float p1f) {
-    const double srate = k.srate, ss = srate * srate;
-    const double p1 = (double)p1f;
-    const double x1c = s.x1_curr, x2c = s.x2_curr, ug = s.ug_curr, ugo = s.ug_old;
-    double Ag1 = k.Ag01 + 2 * k.lg * x1c;
-    double Ag2 = k.Ag02 + 2 * k.lg * x2c;
-    const double Rv1 = (12 * k.mu * k.lg * k.lg * k.d1) / (Ag1 * Ag1 * Ag1);
-    const double Lg1 = (k.rho * k.d1) / Ag1;
-    const double Rv2 = (12 * k.mu * k.lg * k.lg * k.d2) / (Ag2 * Ag2 * Ag2);
-    const double Lg2 = (k.rho * k.d2) / Ag2;
-    double pm1, pm2;
-    if (x1c > -k.Ag01 / (2 * k.lg) && x2c > -k.Ag02 / (2 * k.lg))
-        pm1 = k.ps - 1.37 * (k.rho / 2) * (ug / Ag1) * (ug / Ag1) - 0.5 * (Rv1 * ug + Lg1 * srate * (ug - ugo));
-    else
-        pm1 = k.ps;
-    const double fm1 = pm1 * k.d1 * k.lg;
-    if (x1c > -k.Ag01 / (2 * k.lg)) {
-        if (x2c > -k.Ag02 / (2 * k.lg))
-            pm2 = pm1 - (0.5 * (Rv1 + Rv2) * ug + (Lg1 + Lg2) * (ug - ugo) * srate) -
-                  (k.rho / 2 * ug * ug) * (1 / (Ag2 * Ag2) - 1 / (Ag1 * Ag1));
-        else
-            pm2 = k.ps;
-    } else {
-        pm2 = 0;
-    }
-    const double fm2 = pm2 * k.d2 * k.lg;
-    double h1u, r1u, h2u, r2u;
-    if (x1c + k.Ag01 / (2 * k.lg) < 0) { h1u = k.h1; r1u = k.r1c; } else { h1u = 0; r1u = k.r1o; }
-    if (x2c + k.Ag02 / (2 * k.lg) < 0) { h2u = k.h2; r2u = k.r2c; } else { h2u = 0; r2u = k.r2o; }
-    const double a11 = (k.k1 + h1u + k.kc) / ss + r1u / srate + k.m1;
-    const double a12 = -k.kc / ss;
-    const double a21 = a12;
-    const double a22 = (k.k2 + h2u + k.kc) / ss + r2u / srate + k.m2;
-    const double g1 = k.Ag01 / (2 * k.lg), g2 = k.Ag02 / (2 * k.lg);
-    const double s1 = k.k1 * k.etak1 * x1c * x1c * x1c + h1u * (g1 + k.etah1 * (g1 + x1c) * (g1 + x1c) * (g1 + x1c));
-    const double s2 = k.k2 * k.etak2 * x2c * x2c * x2c + h2u * (g2 + k.etah2 * (g2 + x2c) * (g2 + x2c) * (g2 + x2c));
-    const double b1 = (2 * k.m1 + r1u / srate) * x1c - k.m1 * s.x1_old - s1 / ss + fm1 / ss;
-    const double b2 = (2 * k.m2 + r2u / srate) * x2c - k.m2 * s.x2_old - s2 / ss + fm2 / ss;
-    double det = a11 * a22 - a21 * a12;
-    if (det == 0) det = 1;
-    const double x1n = (a22 * b1 - a12 * b2) / det;
-    const double x2n = (a11 * b2 - a21 * b1) / det;
-    s.x1_old = x1c; s.x1_curr = x1n;
-    s.x2_old = x2c; s.x2_curr = x2n;
-    Ag1 = k.Ag01 + 2 * k.lg * x1n;
-    Ag2 = k.Ag02 + 2 * k.lg * x2n;
-    double ugn;
-    if (Ag1 < 0 || Ag2 < 0) {
-        ugn = 0;
-    } else {
-        const double Rtot = (k.rho / 2) * fabs(ug) *
-                                ((0.37 / (Ag1 * Ag1)) + (1 - 2 * (Ag2 / k.A1) * (1 - Ag2 / k.A1)) / (Ag2 * Ag2)) +
-                            (12 * k.mu * k.lg * k.lg * (k.d1 / (Ag1 * Ag1 * Ag1) + k.d2 / (Ag2 * Ag2 * Ag2)));
-        const double Ltot = k.rho * (k.d1 / Ag1 + k.d2 / Ag2);
-        ugn = ((k.ps - p1) / srate + Ltot * ug) / (Rtot / srate + Ltot);
-    }
-    s.ug_old = ug;
-    s.ug_curr = ugn;
-    return (float)ugn;
-}
-
-// One two-mass step of tube T from the state of parity par and the pressure
-// p1 at the excitation point; with `store` the new state is written to parity
-// par ^ 1 (and, when hist is given, as 6 doubles to hist).
-__device__ __noinline__ float glottal_step(const TubeDev* T, int par, float p1, bool store, double* hist) {
-    if (T->flags & TUBE_TMM64) {
-        TmmState64 s = T->tmm64[par];
-        const float e = tmm_step64(T->tmmd, s, p1);
-        if (store) {
-            T->tmm64[par ^ 1] = s;
-            if (hist) {
-                hist[0] = s.x1_old; hist[1] = s.x1_curr; hist[2] = s.x2_old;
-                hist[3] = s.x2_curr; hist[4] = s.ug_old; hist[5] = s.ug_curr;
-            }
-        }
-        return e;
-    }
-    TmmState s = T->tmm[par];
-    const float e = tmm_step(T->tmmc, s, p1);
-    if (store) {
-        T->tmm[par ^ 1] = s;
-        if (hist) {
-            hist[0] = s.x1_old; hist[1] = s.x1_curr; hist[2] = s.x2_old;
-            hist[3] = s.x2_curr; hist[4] = s.ug_old; hist[5] = s.ug_curr;
-        }
-    }
-    return e;
-}
-
-// Two-mass steps n and n+1 for the two-step kernels: the state of step n is
-// in the parity slot (from_x = false) or the third slot, that of step n+2
-// goes to the other one (stored by the owning strip only).
-__device__ __noinline__ float2 glottal_two_steps(const TubeDev* T, int par, bool from_x, float p1, float p2,
-                                                 bool store) {
-    float2 e;
-    if (T->flags & TUBE_TMM64) {
-        TmmState64 s = from_x ? *T->tmm64_x : T->tmm64[par];
-        e.x = tmm_step64(T->tmmd, s, p1);
-        e.y = tmm_step64(T->tmmd, s, p2);
-        if (store) *(from_x ? &T->tmm64[par] : T->tmm64_x) = s;
-    } else {
-        TmmState s = from_x ? *T->tmm_x : T->tmm[par];
-        e.x = tmm_step(T->tmmc, s, p1);
-        e.y = tmm_step(T->tmmc, s, p2);
-        if (store) *(from_x ? &T->tmm[par] : T->tmm_x) = s;
-    }
-    return e;
-}
-
-// a / b for b > 0 with the signed zero returned directly when a is zero:
-// the same value as the division, without sending the zero fields of a cold
-// start through the slow path of the IEEE divide.
-__device__ __forceinline__ float fdiv_z(float a, float b) { return a == 0.0f ? a : fdiv(a, b); }
-
-// Velocity update of one cell, FDTDEngineCPU.cpp:364-410, with the 17
-// coefficient arrays of calculateSolverCoefficients (FDTDSolver.cu:652-801)
-// derived from the cell codes of the cell, its right and its top neighbour.
-//
-// Every beta is 0 or 1, so minBeta, x1..x4, the no-excitation factors and
-// the excitation weights multiply by exact 0 / 1 and the normal components
-// are 1 or 0.707106 chosen by the neighbours' betas (betaLookUpTable,
-// FDTDSolver.cu:1047-1056, with the tables of DeviceSymbols.cu:20-21).  The reference expression
-//   V' = ((mB V - bX dP) + exeV ew mS + mS zinv n (x2 Pc Nout - x1 Pn Nin)) / (mB + mS)
-// is evaluated here with those exact factors resolved by selects: the
-// remaining products, sums and the division are the reference's, in its
-// order, so the values are equal (a dropped term only ever adds an exact 0).
-struct VelocityOut { float vx, vy; };
-
-// beta per cell type (SolverParams::setBeta, SolverParams.cu:5-27): 1 for
-// air, PML 0..5 and no-pressure cells, 0 otherwise
-constexpr uint32_t kBetaMask = 0x9FAu;
-
-__device__ __forceinline__ bool beta_bit(int t) { return (kBetaMask >> t) & 1u; }
-
-__device__ __forceinline__ float velocity_dir(bool bc, bool bn, bool bo, bool ec, bool en, float dirc, float dirn,
-                                              float v0, float pc, float pn, float exeV, float mS, float zinv,
-                                              float bco) {
-    const bool mB = bc && bn;
-    float v = mB ? fsub(v0, fmul(bco, fsub(pn, pc))) : 0.0f;
-    if (ec || en) v = fadd(v, fmul(fmul(exeV, fadd(fmul((float)ec, dirc), fmul((float)en, dirn))), mS));
-    if (zinv != 0.0f && !(ec || en) && bc != bn) {
-        // x2 = bc (1 - bn): Pc * Nout, Nout = 1/sqrt(2) when the other neighbour is
-        // a wall (beta 0), else 1; x1 = bn (1 - bc): -Pn * Nin with Nin = 1
-        const float vb = bc ? fmul(pc, bo ? 1.0f : 0.707106f) : -pn;
-        v = fadd(v, fmul(mS, fmul(vb, zinv)));
-    }
-    return fdiv_z(v, fadd(mB ? 1.0f : 0.0f, mS));
-}
-
-__device__ __forceinline__ VelocityOut velocity_generic(
-        int kc, int kr, int kt, float pc, float pr, float pt, float vx0, float vy0, float exeV,
-        const float* __restrict__ sig, float zval, float bco, float dir0, float dir1, float dir2, float dir3) {
-    const int tc = kc & CODE_TYPE_MASK, tr = kr & CODE_TYPE_MASK, tt = kt & CODE_TYPE_MASK;
-    const bool bc = beta_bit(tc), br = beta_bit(tr), bt = beta_bit(tt);
-    const bool ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
-    const float sc = sig[tc];
-    const float zinv = (kc & CODE_ZINV_BIT) ? zval : 0.0f;
-    return {velocity_dir(bc, br, bt, ec, er, dir2, dir0, vx0, pc, pr, exeV, fmaxf(sc, sig[tr]), zinv, bco),
-            velocity_dir(bc, bt, br, ec, et, dir3, dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco)};
-}
-
-// Approximate reciprocal (PTX rcp.approx.f32, at most 1 ulp from 1/x).
-__device__ __forceinline__ float rcp_approx(float x) {
-    float r;
-    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
 
 // Row-marching strip kernel.  One warp owns a strip of 32 columns x TR rows:
 // lane i holds column c0 + i, strips overlap by two columns (stride 30), so
@@ -1466,9 +1198,12 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 }  // namespace
 
-int tile_shape_count() { return kNumShapes; }
+int tile_shape_count() { return kNumShapes + 1; }
+
+int cluster_shape() { return kNumShapes; }
 
 TileShape tile_shape(int i) {
+    if (i == kNumShapes) return {0, 0, 0, SHAPE_CLUSTER, 0};
     const ShapeEntry& e = kShapes[i];
     const int cols = e.kind == SHAPE_STRIP ? kStripCommit
                      : e.kind == SHAPE_BAND ? 0
@@ -1496,7 +1231,9 @@ cudaError_t prepare_shape(int shape, int max_pitch) {
     return e;
 }
 
-bool shape_has_fast(int shape) { return shape >= 0 && shape < kNumShapes && kShapes[shape].fast != nullptr; }
+bool shape_has_fast(int shape) {
+    return shape == kNumShapes || (shape >= 0 && shape < kNumShapes && kShapes[shape].fast != nullptr);
+}
 
 cudaError_t launch_step(int shape, bool wall, bool fast, const TubeDev* tubes, const Tile* tiles, int ntiles,
                         RunState* rs, int local, cudaStream_t stream, int max_pitch) {
