@@ -244,6 +244,14 @@ int vs_batch_set_stream(vs_batch* b, void* cuda_stream);
  * batches when the band fits a CTA's shared memory. */
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
 
+/* Failure-path hook, no counterpart in the reference: the number of polls a
+ * kernel's wait for its bulk row copies (band and staged quad-strip shapes)
+ * makes before it gives up, and the run returns VS_ERR_TIMEOUT with the
+ * state not valid; 0 restores the default (2^22).  A kernel that gives up
+ * still waits, with the default limit, for its own copies in flight before it
+ * exits.  Tests lower it to drive the timeout path without a fault. */
+int vs_batch_set_wait_limit(vs_batch* b, uint32_t polls);
+
 /* Time every compiled tile shape on `steps` steps and keep the fastest.  The
  * state is reset afterwards.  best_index / best_ms may be NULL. */
 int vs_batch_autotune(vs_batch* b, int64_t steps, int32_t* best_index, float* best_ms);

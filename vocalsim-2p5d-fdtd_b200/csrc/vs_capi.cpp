@@ -118,6 +118,7 @@ struct vs_batch {
     bool fast = false;                     // reciprocal-form arithmetic (vs_params::fast_math)
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
     int cluster_state = 0;                 // cluster shape: 0 = not checked, 1 = fits, -1 = does not
+    uint32_t wait_polls = 0;               // RunState::wait_polls of every run (0 = the default limit)
     ClusterConfig cluster{};
     // adjoint: checkpoints of the last checkpointed forward, history, adjoint planes
     int64_t ck_steps = 0;                  // steps of the checkpointed forward (0 = none)
@@ -564,6 +565,7 @@ void reset_state(vs_batch* b) {
     // the two-step kernels' third set: its ring cells must read as zero
     if (b->x_mem) ck(cudaMemsetAsync(b->x_mem, 0, b->x_bytes, b->stream), "zero third state set");
     RunState rs{};
+    rs.wait_polls = b->wait_polls;
     ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "reset run state");
     ck(cudaStreamSynchronize(b->stream), "reset sync");
     b->step = 0;
@@ -717,6 +719,7 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
         b->trace_cap = need;
     }
     RunState rs{};
+    rs.wait_polls = b->wait_polls;
     rs.step = b->step;
     rs.run_start = b->step;
     rs.trace = b->d_trace;
@@ -732,6 +735,7 @@ void run_batch(vs_batch* b, int64_t steps, float* traces, int on_device) {
     ck(cudaStreamSynchronize(b->stream), "run sync");
     int32_t dev_error = 0;
     ck(cudaMemcpy(&dev_error, &b->d_rs->error, sizeof(dev_error), cudaMemcpyDeviceToHost), "read run status");
+    if (dev_error == VS_ERR_NONFINITE) throw VsFailure{dev_error, "non-finite listener pressure"};
     if (dev_error != 0) throw VsFailure{dev_error, "a bounded device wait gave up; the state is not valid"};
     if (traces && !on_device) {
         for (int64_t i = 0; i < need; ++i)
@@ -779,6 +783,7 @@ void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces) 
     ck(cudaMalloc(&b->ckpt, stride * count), "cudaMalloc(checkpoints)");
     b->ckpt_stride = stride;
     RunState rs{};
+    rs.wait_polls = b->wait_polls;
     rs.trace = b->d_trace;
     rs.trace_stride = steps;
     ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
@@ -1042,6 +1047,7 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         const int len = (int)std::min<int64_t>(K, steps - start);
         copy_state(b, k, false);
         RunState rs{};
+        rs.wait_polls = b->wait_polls;
         rs.step = start;
         rs.run_start = start;
         rs.trace = b->d_trace;
@@ -1356,6 +1362,12 @@ int vs_batch_set_tile(vs_batch* b, int32_t tile_index) {
     const int s = tile_index < 0 ? default_shape(b) : tile_index;
     if (!shape_fits(b, s)) return set_error(VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)");
     b->shape = s;
+    return VS_OK;
+}
+
+int vs_batch_set_wait_limit(vs_batch* b, uint32_t polls) {
+    if (!b) return set_error(VS_ERR_INVALID_ARG, "null batch");
+    b->wait_polls = polls;
     return VS_OK;
 }
 

@@ -276,6 +276,14 @@ __device__ __forceinline__ VelocityOut velocity_generic(
             velocity_dir(bc, bt, br, ec, et, dir3, dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco)};
 }
 
+// Listener sample of a step; a non-finite value (an unstable tube) also
+// raises the run's sticky error word, so runs that keep their traces on the
+// device report VS_ERR_NONFINITE too.
+__device__ __forceinline__ void store_trace(RunState* rs, float* dst, float v) {
+    *dst = v;
+    if (!isfinite(v)) atomicExch(&rs->error, VS_ERR_NONFINITE);
+}
+
 // Approximate reciprocal (PTX rcp.approx.f32, at most 1 ulp from 1/x).
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;

@@ -228,7 +228,7 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
                     if (dirichlet && tc == VS_CELL_NOPRESSURE) pn = 0.0f;
                 }
                 Pr[c] = pn;
-                if (i >= 1 && lis_here && r0 - 1 + i == lis_y && c == lis_x) trace[n - run_start] = pn;
+                if (i >= 1 && lis_here && r0 - 1 + i == lis_y && c == lis_x) store_trace(rs, trace + (n - run_start), pn);
             }
         }
         __syncthreads();

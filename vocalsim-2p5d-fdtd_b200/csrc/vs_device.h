@@ -75,8 +75,10 @@ struct RunState {
     int64_t run_start;    // global step that lands in trace column 0
     float* trace;         // device trace buffer, [ntubes][trace_stride]
     int64_t trace_stride;
-    int32_t error;        // sticky device error word (0 = ok)
+    int32_t error;        // sticky device error word (0 = ok): VS_ERR_TIMEOUT, VS_ERR_NONFINITE
     int32_t bsel;         // two-step kernels: 1 = the state of `step` is in TubeDev::X
+    uint32_t wait_polls;  // polls of a row-copy wait before it gives up (0 = kWaitPolls);
+                          // the drain after a timeout always uses kWaitPolls
 };
 
 // Strip geometry of the step kernel: lane i of a warp holds column c0 + i;

@@ -177,7 +177,7 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             if (lane_commit) {
                 Pout[o] = pn;
                 if (r == lis_y && x == lis_x)
-                    rs->trace[(int64_t)it.tube * rs->trace_stride + (n - rs->run_start)] = pn;
+                    store_trace(rs, rs->trace + (int64_t)it.tube * rs->trace_stride + (n - rs->run_start), pn);
                 if (WALL) {
                     // wall oscillator, FDTDEngineCPU.cpp:345-361
                     const float dt = T->dt;
@@ -274,6 +274,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit)
 }
 
 constexpr uint32_t kWaitPolls = 1u << 22;
+
+// Poll limit of the waits whose expiry ends the launch with VS_ERR_TIMEOUT.
+__device__ __forceinline__ uint32_t first_wait_limit(const RunState* rs) {
+    const uint32_t w = rs->wait_polls;
+    return w ? w : kWaitPolls;
+}
 
 // Bounded wait on the phase with the given parity.
 __device__ __forceinline__ bool mbar_wait_parity_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
@@ -434,7 +440,7 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
         bulk_g2s(st + 6 * kQSeg, code + (off & ~(int64_t)15), kQCode, bar);
     };
     auto wait_row = [&](int i) -> bool {
-        const bool ok = mbar_wait_parity_bounded(bars + i % kS, (uint32_t)(i / kS) & 1u, kWaitPolls);
+        const bool ok = mbar_wait_parity_bounded(bars + i % kS, (uint32_t)(i / kS) & 1u, first_wait_limit(rs));
         return __all_sync(kFull, ok);
     };
     auto drain = [&](int from, int issued) {            // after a timeout: bounded wait for copies in flight
@@ -591,7 +597,7 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
                 float pv = pn[0];
 #pragma unroll
                 for (int q = 1; q < 4; ++q) if (lis_q == q) pv = pn[q];
-                rs->trace[(int64_t)it.tube * rs->trace_stride + (n - rs->run_start)] = pv;
+                store_trace(rs, rs->trace + (int64_t)it.tube * rs->trace_stride + (n - rs->run_start), pv);
             }
             float vx[4], vy[4];
             if constexpr (FAST) {
@@ -874,7 +880,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             float pv = pn1[0];
 #pragma unroll
             for (int q = 1; q < NC; ++q) if (lis_q == q) pv = pn1[q];
-            trace[0] = pv;
+            store_trace(rs, trace, pv);
         }
 
         // ---- step n+1 at row s = r - 1
@@ -918,7 +924,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                     float pv = pn2[0];
 #pragma unroll
                     for (int q = 1; q < NC; ++q) if (lis_q == q) pv = pn2[q];
-                    trace[1] = pv;
+                    store_trace(rs, trace + 1, pv);
                 }
             }
 #pragma unroll
@@ -1057,12 +1063,20 @@ band_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ bands, i
         }
         s_exe = e;
     }
-    if (!mbar_wait_bounded(&bar, kWaitPolls)) {
-        // the copies did not land: flag the run, let them finish, and leave
-        if (threadIdx.x == 0) atomicExch(&rs->error, VS_ERR_TIMEOUT);
-        mbar_wait_bounded(&bar, kWaitPolls);
+    // one thread decides whether the copies landed, so the whole CTA leaves or
+    // stays together; the others then observe the completed phase themselves
+    __shared__ int s_landed;
+    if (threadIdx.x == 0) s_landed = mbar_wait_bounded(&bar, first_wait_limit(rs)) ? 1 : 0;
+    __syncthreads();
+    if (!s_landed) {
+        // the copies did not land in time: flag the run, let them finish, and leave
+        if (threadIdx.x == 0) {
+            atomicExch(&rs->error, VS_ERR_TIMEOUT);
+            mbar_wait_bounded(&bar, kWaitPolls);
+        }
         return;
     }
+    mbar_wait_bounded(&bar, kWaitPolls);       // completed: returns on the first poll
     __syncthreads();
     const float exeV = s_exe;
     const float* __restrict__ sig = T->sigma;
@@ -1101,7 +1115,7 @@ band_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ bands, i
             if (r >= r0) {
                 Pout[o] = pn;
                 if (r == T->lis_y && c == T->lis_x)
-                    rs->trace[(int64_t)bd.tube * rs->trace_stride + (n - rs->run_start)] = pn;
+                    store_trace(rs, rs->trace + (int64_t)bd.tube * rs->trace_stride + (n - rs->run_start), pn);
                 if (WALL) {
                     // wall oscillator, FDTDEngineCPU.cpp:345-361
                     const float dt = T->dt;

@@ -157,6 +157,10 @@ class Batch:
     def set_tile(self, index: int) -> None:
         check(self.lib, self.lib.vs_batch_set_tile(self.h, index), "vs_batch_set_tile")
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of a row-copy wait before the run gives up with VS_ERR_TIMEOUT (0 = default)."""
+        check(self.lib, self.lib.vs_batch_set_wait_limit(self.h, polls), "vs_batch_set_wait_limit")
+
     def set_maps(self, tube: int, depth_p=None, depth_x=None, depth_y=None, z_inv: float = 0.0) -> None:
         """Replace tube `tube`'s depth maps (frame-shaped float32) and z_inv value."""
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32) for a in (depth_p, depth_x, depth_y)]
