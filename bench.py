@@ -8,9 +8,11 @@ one interior cell advanced one full step (P and V).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
---impl reference times the reference's CPU engine (the oracle's restatement of
-FDTDEngineCPU; the reference engine itself does not build here) on the host
-cores over a bounded sample of the same workload.
+--impl reference times the reference's CPU engine on the host cores over a
+bounded sample of the same workload: its own FDTDEngineCPU compiled from the
+reference sources (oracle/_ref/ref_engine; the grid setup runs on the GPU,
+only the time loop is timed), or the oracle's FP32 restatement of it where
+that binary is not built.
 --profile-steps S builds the batch and runs S time steps, untimed, for ncu.
 Under torchrun every rank runs its own 256-tube batch (weak scaling; no
 collective on the data path) and rank 0 prints one JSON line.
@@ -39,6 +41,13 @@ BYTES_PER_CELL_UPDATE = 37             # P,Vx,Vy read+write (24) + dP,dX,dY (12)
 METRIC = "Gcell-updates/s"
 PEAKS = REPO / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_config(n_tubes: int = N_TUBES, sim_steps: int = SIM_STEPS) -> dict:
+    """The workload both arms measure."""
+    return {"workload": f"batched forward, {n_tubes} seeded tubes 12-20 cm x 2-4 cm, 3:1 elliptical, Gaussian, PML 6, "
+                        f"{sim_steps} steps (50 ms) at fs 661.5 kHz; one step = one full forward",
+            "tubes": n_tubes, "sim_steps": sim_steps}
 
 
 def rank_tube_seeds(rank: int, n_tubes: int) -> list[int]:
@@ -203,6 +212,40 @@ def cpu_reference(n_tubes: int, steps_per_tube: int, procs: int):
     return cell_updates / wall / 1e9, wall, cell_updates
 
 
+def ref_engine_available() -> bool:
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    return O.REF_ENGINE.exists()
+
+
+def ref_engine_throughput(n_sample: int, steps: int, procs: int):
+    """Throughput of the reference's own FDTDEngineCPU (oracle/_ref/ref_engine:
+    its SimulationParams -> FDTDSolver::setupWaveSolver -> startSolverEngine
+    compiled from the reference sources) on batch tubes 0..n_sample-1, `procs`
+    processes at a time, one tube each.  Work = interior cells x steps; time =
+    from the first loop's start to the last loop's end (monotonic clock), so
+    set-up and process start-up are outside it."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    from concurrent.futures import ThreadPoolExecutor
+    from vocalsim_b200 import synthetic as S
+
+    def one(seed):
+        L, A = S.batch_tube(seed)[:2]
+        r = O.reference_engine(O.params(cross_sectional_shape=2), O.Geometry(L, A), steps, with_maps=False)
+        m = r["meta"]
+        return (m["frame_h"] - 2) * (m["frame_w"] - 2) * steps, m["loop_t0"], m["loop_t1"]
+
+    with ThreadPoolExecutor(procs) as ex:
+        res = list(ex.map(one, range(n_sample)))
+    work = sum(x[0] for x in res)
+    span = max(x[2] for x in res) - min(x[1] for x in res)
+    return work / span / 1e9, span, work
+
+
+REF_ENGINE_STEPS = 1500
+
+
 def host_cores() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -219,26 +262,42 @@ def run_reference(args, rank):
     if rank != 0:
         return None
     procs = host_cores()
-    n_sample = min(N_TUBES, max(procs, 16))
-    steps = cpu_sample_steps(n_sample)
     per_step = []
-    for _ in range(args.warmup):
-        cpu_reference(procs, 50, procs)
-    for _ in range(args.steps):
-        g, wall, cu = cpu_reference(n_sample, steps, procs)
-        per_step.append((g, wall))
+    if ref_engine_available():
+        # the reference's own engine, compiled from its sources
+        kind = "reference"
+        n_sample = min(N_TUBES, procs)
+        steps = REF_ENGINE_STEPS
+        for _ in range(min(args.warmup, 1)):
+            ref_engine_throughput(min(procs, 4), 50, procs)
+        for _ in range(args.steps):
+            g, wall, _ = ref_engine_throughput(n_sample, steps, procs)
+            per_step.append((g, wall))
+        sample = (f"{n_sample} of the {N_TUBES} batch tubes x {steps} of {SIM_STEPS} time steps per bench step: the "
+                  f"reference's FDTDEngineCPU built from its sources (setup on the GPU, loop timed), one process "
+                  f"per host core")
+    else:
+        kind = "port"
+        n_sample = min(N_TUBES, max(procs, 16))
+        steps = cpu_sample_steps(n_sample)
+        for _ in range(args.warmup):
+            cpu_reference(procs, 50, procs)
+        for _ in range(args.steps):
+            g, wall, cu = cpu_reference(n_sample, steps, procs)
+            per_step.append((g, wall))
+        sample = (f"{n_sample} of the {N_TUBES} batch tubes x {steps} of {SIM_STEPS} time steps per bench step, "
+                  f"FP32 restatement of FDTDEngineCPU, one spawn process per host core")
     value = statistics.median(g for g, _ in per_step)
-    sample = (f"{n_sample} of the {N_TUBES} batch tubes x {steps} of {SIM_STEPS} time steps per bench step, "
-              f"one spawn process per host core")
     return {
         "metric": METRIC, "value": round(value, 4), "unit": "Gcell-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * statistics.median(w for _, w in per_step), 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded area functions)",
-        "config": {"workload": "batched forward, 256 tubes 12-20 cm x 2-4 cm, 50 ms (33075 steps), fs 661.5 kHz",
-                   "tubes": N_TUBES, "sim_steps": SIM_STEPS},
-        "cpu_baseline": {"value": round(value, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": "port",
+        "config": workload_config(N_TUBES),
+        "run": {"engine": "the reference's FDTDEngineCPU" if kind == "reference" else "FP32 port of FDTDEngineCPU",
+                "arithmetic": "reference rounding (FP32, host)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": kind,
                          "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -440,10 +499,58 @@ def run_b200(args, rank, world):
         b.record(stream)
         torch.cuda.synchronize()
         sms = a.elapsed_time(b)
-        single = {"workload": "uniform tube 17.5 x 3 cm, 57x253 frame, 33075 steps",
+        single = {"workload": "uniform tube 17.5 x 3 cm, 57x253 frame, 33075 steps (cluster kernel: one launch)",
                   "value": round(s.dims["interior_cells"] * SIM_STEPS / (sms / 1e3) / 1e9, 3),
                   "unit": "Gcell-updates/s", "ms": round(sms, 2)}
         s.close()
+        # the same tube on the graph-replayed step kernels (its best step shape)
+        bs = V.Batch([V.params(mu3d=0.005, uniform_depth_m=0.02, num_steps=SIM_STEPS, fast_math=fast)],
+                     [V.Geometry(L, A)])
+        bs.set_stream(stream.cuda_stream)
+        best_ms, best_k = None, None
+        for k in range(len(V.tile_shapes()) - 1):
+            try:
+                bs.set_tile(k)
+            except V.VsError:
+                continue
+            bs.reset()
+            bs.run_device(2048)
+            bs.reset()
+            a.record(stream)
+            bs.run_device(SIM_STEPS)
+            b.record(stream)
+            torch.cuda.synchronize()
+            t = a.elapsed_time(b)
+            if best_ms is None or t < best_ms:
+                best_ms, best_k = t, k
+        bs.close()
+        single["step_kernels_value"] = round(s.dims["interior_cells"] * SIM_STEPS / (best_ms / 1e3) / 1e9, 3)
+        single["step_kernels_ms"] = round(best_ms, 2)
+        single["step_kernels_shape"] = best_k
+        single["cluster_speedup"] = round(best_ms / sms, 2)
+
+    # ---- a 1 s vowel tube with the two-mass source (800 Pa)
+    config2 = None
+    if not args.no_single:
+        from vocalsim_b200 import synthetic as S
+        n2 = 661500
+        s2 = V.Solver(V.params(cross_sectional_shape=2, source_type=V.SRC_TMM, tmm_ps_pa=800.0, tmm_f64=1,
+                               num_steps=n2, fast_math=fast), V.Geometry(*S.vowel_tube(0)))
+        s2.set_stream(stream.cuda_stream)
+        d2 = torch.empty(n2, dtype=torch.float32, device=dev)
+        s2.run_device(2000, d2.data_ptr())
+        s2.reset()
+        a.record(stream)
+        s2.run_device(n2, d2.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms2 = a.elapsed_time(b)
+        config2 = {"workload": "vowel tube (seed 0, 44 sections, 3:1 elliptical), two-mass source 800 Pa in double, "
+                               f"1 s simulated ({n2} steps), one cluster-kernel launch",
+                   "interior_cells": s2.dims["interior_cells"],
+                   "value": round(s2.dims["interior_cells"] * n2 / (ms2 / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
+                   "ms": round(ms2, 2), "s_per_simulated_s": round(ms2 / 1e3, 4)}
+        s2.close()
 
     grad = None
     if not args.no_grad:
@@ -455,26 +562,31 @@ def run_b200(args, rank, world):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         procs = host_cores()
-        n_sample = min(args.tubes, max(procs, 16))
-        csteps = cpu_sample_steps(n_sample)
-        g, wall, _ = cpu_reference(n_sample, csteps, procs)
-        cpu = {"value": round(g, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": "port",
-               "sample": f"{n_sample} batch tubes x {csteps} of {SIM_STEPS} steps, FP32 restatement of FDTDEngineCPU, "
-                         f"one process per core ({wall:.1f} s)"}
+        if ref_engine_available():
+            n_sample = min(args.tubes, procs)
+            g, wall, _ = ref_engine_throughput(n_sample, REF_ENGINE_STEPS, procs)
+            cpu = {"value": round(g, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": "reference",
+                   "sample": f"{n_sample} batch tubes x {REF_ENGINE_STEPS} of {SIM_STEPS} steps, the reference's "
+                             f"FDTDEngineCPU built from its sources, one process per core (loops {wall:.1f} s)"}
+        else:
+            n_sample = min(args.tubes, max(procs, 16))
+            csteps = cpu_sample_steps(n_sample)
+            g, wall, _ = cpu_reference(n_sample, csteps, procs)
+            cpu = {"value": round(g, 4), "unit": "Gcell-updates/s", "cores": procs, "kind": "port",
+                   "sample": f"{n_sample} batch tubes x {csteps} of {SIM_STEPS} steps, FP32 restatement of "
+                             f"FDTDEngineCPU, one process per core ({wall:.1f} s)"}
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
         "higher_is_better": True, "scaling": "strong" if args.strong else "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded area functions, no dataset)",
-        "config": {"workload": "batched forward, 256 tubes 12-20 cm x 2-4 cm, 3:1 elliptical, Gaussian, PML 6, "
-                               "50 ms (33075 steps) at fs 661.5 kHz; one step = one full forward",
-                   "tubes_per_gpu": len(ps), "interior_cells_per_gpu": cells, "sim_steps": sim_steps,
-                   "tile": list(V.tile_shapes()[tile]),
-                   "parallelism": (f"LPT tube sharding of one {args.tubes}-tube batch x{world} (no collective)"
-                                   if args.strong else f"tube sharding x{world} (no collective)"),
-                   "arithmetic": "reciprocal form (fast_math=1)" if fast else "reference rounding (fast_math=0)",
-                   "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
+        "config": workload_config(args.tubes, sim_steps),
+        "run": {"tubes_per_gpu": len(ps), "interior_cells_per_gpu": cells, "tile": list(V.tile_shapes()[tile]),
+                "parallelism": (f"LPT tube sharding of one {args.tubes}-tube batch x{world} (no collective)"
+                                if args.strong else f"tube sharding x{world} (no collective)"),
+                "arithmetic": "reciprocal form (fast_math=1)" if fast else "reference rounding (fast_math=0)",
+                "l2": "state + maps per GPU > 126 MB L2 and 33075 launches per timed step; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": prof["traffic"],
                      # DRAM bytes the launch really moves (ncu, same kernel and workload) per
@@ -494,7 +606,11 @@ def run_b200(args, rank, world):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "single_tube": single,
+        "config2": config2,
+        # against the library's default single-tube path (the cluster kernel), and
+        # against the same step kernels the batch uses, run on the one tube
         "batched_vs_single": round(value / world / single["value"], 2) if single else None,
+        "batched_vs_single_step_kernels": round(value / world / single["step_kernels_value"], 2) if single else None,
         "grad_fwd_ratio": grad["ratio"] if grad else None,
         "gradient": grad,
         "inversion": inversion,

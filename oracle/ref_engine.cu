@@ -136,6 +136,9 @@ int main(int argc, char** argv) {
     std::fprintf(m, "frame_h %d\nframe_w %d\nlistener_x %d\nlistener_y %d\nexcitation_x %d\nexcitation_y %d\n", H, W,
                  fdtd.listenerX, fdtd.listenerY, fdtd.excitationX, fdtd.excitationY);
     std::fprintf(m, "ref_steps %d\nsteps %d\nloop_s %.9f\n", ref_steps, steps, loop_s);
+    // the loop's start and end on the monotonic clock, comparable across processes
+    std::fprintf(m, "loop_t0 %.9f\nloop_t1 %.9f\n", std::chrono::duration<double>(t0.time_since_epoch()).count(),
+                 std::chrono::duration<double>(t1.time_since_epoch()).count());
     std::fprintf(m, "dt %.9e\nds %.9e\nkappa %.9e\n", fdtd.dt, fdtd.ds, fdtd.kappa);
     std::fclose(m);
 
