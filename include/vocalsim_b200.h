@@ -244,6 +244,12 @@ int vs_batch_set_stream(vs_batch* b, void* cuda_stream);
  * batches when the band fits a CTA's shared memory. */
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
 
+/* Kernel form of the reverse steps of vs_batch_adjoint, no counterpart in the
+ * reference: 0 = row-marching warp strips with four columns per lane (the
+ * default), 1 = 32 x 8 tiles with mu in shared memory.  Both compute the same
+ * transposed step; they differ only in float rounding. */
+int vs_batch_set_adjoint_form(vs_batch* b, int32_t form);
+
 /* Failure-path hook, no counterpart in the reference: the number of polls a
  * kernel's wait for its bulk row copies (band and staged quad-strip shapes)
  * makes before it gives up, and the run returns VS_ERR_TIMEOUT with the

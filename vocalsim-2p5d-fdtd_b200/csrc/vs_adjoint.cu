@@ -308,6 +308,224 @@ adjoint_step_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same reverse step in strip form: one warp per strip of TR rows x
+// 30 NC columns, NC consecutive columns per lane (one aligned NC-float load
+// per plane row), lanes 1..30 commit; strip k of a tube starts at column
+// c0 = 30 NC k - NC.  The warp marches down its rows: mu and q of row r come
+// from the row's own lambda' and that of the row below (kept one row ahead
+// in registers), the left neighbour's bx lambdaVx' and Vx dX by one shuffle;
+// the commit of row r takes q of the right neighbour by one shuffle and q of
+// the row above from the previous iteration (the row above the strip is
+// computed, not committed).  No shared memory and no block barrier.  The
+// per-cell gradient terms are formed in float and added to the double
+// accumulators; q = mu / D uses the fast division (the adjoint is not meant
+// to be bit-identical to anything).
+template <int NC>
+struct Row {
+    float v[NC];
+};
+
+template <int NC>
+__device__ __forceinline__ void ldrow(float (&d)[NC], const float* p, bool ok) {
+    if (!ok) {
+#pragma unroll
+        for (int q = 0; q < NC; ++q) d[q] = 0.0f;
+        return;
+    }
+    if constexpr (NC == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w;
+    } else if constexpr (NC == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        d[0] = t.x; d[1] = t.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < NC; ++q) d[q] = __ldg(p + q);
+    }
+}
+
+template <int NC>
+__device__ __forceinline__ uint32_t ldbytes(const uint8_t* p, bool ok) {
+    if (!ok) return 0u;
+    if constexpr (NC == 4) return __ldg(reinterpret_cast<const uint32_t*>(p));
+    else if constexpr (NC == 2) return (uint32_t)__ldg(reinterpret_cast<const uint16_t*>(p));
+    else return (uint32_t)__ldg(p);
+}
+
+__device__ __forceinline__ int byte_at(uint32_t k, int q) { return (int)((k >> (8 * q)) & 0xffu); }
+
+template <int NC, int TR, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+adjoint_strip_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
+                     const AdjRun* __restrict__ run, int local) {
+    const TubeDev& T = tubes[blockIdx.y];
+    const AdjTube& A = adj[blockIdx.y];
+    const AdjRun ar = *run;
+    const int64_t n = ar.start + ar.len - 1 - local;
+    const int64_t slot = n - ar.start;
+    const int par = ar.q0 ^ (local & 1);
+    const int nblk = (A.strips + WARPS - 1) / WARPS;
+    if ((int)blockIdx.x >= nblk) {
+        // the block after the last strip block reverses the two-mass step
+        if ((int)blockIdx.x == nblk && (T.flags & TUBE_TMM) && threadIdx.x < 32)
+            tmm_reverse(T, A, A.lam[par], par, slot);
+        return;
+    }
+    const int s = (int)blockIdx.x * WARPS + (int)(threadIdx.x >> 5);
+    if (s >= A.strips) return;
+    constexpr unsigned kAll = 0xffffffffu;
+    constexpr int kCommit = 30 * NC;
+    const int lane = threadIdx.x & 31;
+    const int W = T.W, H = T.H, pitch = T.pitch;
+    const int nsx = (W - 2) / kCommit + 1;
+    const int c0 = kCommit * (s % nsx) - NC;
+    const int r0 = 1 + (s / nsx) * TR;
+    const int rlast = min(r0 + TR - 1, H - 2);
+    const int x0 = c0 + NC * lane;
+    const bool ok = x0 >= 0 && x0 < pitch;          // the lane's NC columns lie in the pitched row
+    unsigned inter = 0, commit = 0;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const int x = x0 + q;
+        const bool in = x >= 1 && x <= W - 2;
+        inter |= (unsigned)in << q;
+        commit |= (unsigned)(in && lane >= 1 && lane <= 30) << q;
+    }
+    const int64_t pl = T.plane;
+    const float* __restrict__ lam = A.lam[par];
+    float* __restrict__ lout = A.lam[par ^ 1];
+    const float* __restrict__ s0 = T.hist + slot * 3 * pl;   // state before the step (P, Vx, Vy)
+    const float* __restrict__ s1 = s0 + 3 * pl;              // P' after it
+    const float* __restrict__ mP = T.dP;
+    const uint8_t* __restrict__ dsc = A.desc;
+    const uint8_t* __restrict__ code = T.code;
+    const float4* __restrict__ tab = A.tab;
+    const float K1 = T.K1;
+    const int lis_y = T.lis_y, lis_q = T.lis_x - x0;
+    const bool tmm = (T.flags & TUBE_TMM) != 0;
+    const int exc_y = T.exc_y, exc_q = T.exc_x - x0;
+    const float glis = (lis_y >= r0 - 1 && lis_y <= rlast && lis_q >= 0 && lis_q < NC) ? __ldg(A.gtrace + n) : 0.0f;
+    const float pend = (tmm && exc_y >= r0 - 1 && exc_y <= rlast && exc_q >= 0 && exc_q < NC)
+                           ? (float)A.lam_tmm[6 + par] : 0.0f;
+
+    // row r = r0 - 1 and the row below it
+    int r = r0 - 1;
+    int64_t o = (int64_t)r * pitch + x0;
+    float lP[NC], lX[NC], lY[NC], dp[NC], dx[NC], dy[NC], vx[NC], vy[NC];
+    float lYn[NC], dyn[NC], vyn[NC], qa[NC];
+    uint32_t d_c, d_n;
+    ldrow<NC>(lP, lam + o, ok);
+    ldrow<NC>(lX, lam + pl + o, ok);
+    ldrow<NC>(lY, lam + 2 * pl + o, ok);
+    ldrow<NC>(dp, mP + o, ok);
+    ldrow<NC>(dx, mP + pl + o, ok);
+    ldrow<NC>(dy, mP + 2 * pl + o, ok);
+    ldrow<NC>(vx, s0 + pl + o, ok);
+    ldrow<NC>(vy, s0 + 2 * pl + o, ok);
+    d_c = ldbytes<NC>(dsc + o, ok);
+    ldrow<NC>(lYn, lam + 2 * pl + o + pitch, ok);
+    ldrow<NC>(dyn, mP + 2 * pl + o + pitch, ok);
+    ldrow<NC>(vyn, s0 + 2 * pl + o + pitch, ok);
+    d_n = ldbytes<NC>(dsc + o + pitch, ok);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) qa[q] = 0.0f;
+
+    for (int j = 0; r <= rlast; ++j, ++r, o += pitch) {
+        // ---- loads for the next row: its own values and the row below it
+        const int64_t o1 = o + pitch;
+        const bool more = r + 1 <= rlast;
+        float lP1[NC], lX1[NC], dp1[NC], dx1[NC], vx1[NC], lY2[NC], dy2[NC], vy2[NC];
+        uint32_t d_2 = 0;
+        ldrow<NC>(lP1, lam + o1, ok && more);
+        ldrow<NC>(lX1, lam + pl + o1, ok && more);
+        ldrow<NC>(dp1, mP + o1, ok && more);
+        ldrow<NC>(dx1, mP + pl + o1, ok && more);
+        ldrow<NC>(vx1, s0 + pl + o1, ok && more);
+        ldrow<NC>(lY2, lam + 2 * pl + o1 + pitch, ok && more);
+        ldrow<NC>(dy2, mP + 2 * pl + o1 + pitch, ok && more);
+        ldrow<NC>(vy2, s0 + 2 * pl + o1 + pitch, ok && more);
+        d_2 = ldbytes<NC>(dsc + o1 + pitch, ok && more);
+
+        // ---- mu and q of row r
+        const unsigned rowm = r >= 1 ? inter : 0u;
+        float4 eb[NC];
+        float mu[NC], qc[NC], bxl[NC], ux[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            const float4 ea = __ldg(tab + 3 * byte_at(d_c, q));
+            eb[q] = __ldg(tab + 3 * byte_at(d_c, q) + 1);
+            const float byd = __ldg(tab + 3 * byte_at(d_n, q)).w;
+            bxl[q] = ea.z * lX[q];                 // this cell's bx lambdaVx', for its right neighbour
+            ux[q] = vx[q] * dx[q];                 // this cell's Vx dX, for its right neighbour
+            mu[q] = lP[q] + ea.x * lX[q] + ea.y * lY[q] - byd * lYn[q];
+        }
+        const float bx_in = __shfl_up_sync(kAll, bxl[NC - 1], 1);
+        const float ux_in = __shfl_up_sync(kAll, ux[NC - 1], 1);
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            mu[q] -= q > 0 ? bxl[q - 1] : bx_in;
+            if (r == lis_y && q == lis_q) mu[q] += glis;
+            if (tmm && r == exc_y && q == exc_q) mu[q] += pend;
+            if (!((rowm >> q) & 1u) || eb[q].w != 0.0f) mu[q] = 0.0f;   // ring / Dirichlet no-pressure
+            qc[q] = mu[q] == 0.0f ? 0.0f : __fdividef(mu[q], eb[q].z * dp[q]);
+        }
+        // ---- commit row r (FDTDEngineCPU.cpp:316-410 transposed)
+        if (j >= 1) {
+            const float q_in = __shfl_down_sync(kAll, qc[0], 1);
+            const uint32_t kc = ldbytes<NC>(code + o, ok);
+            float oP[NC], oX[NC], oY[NC];
+            float tP[NC], tX[NC], tY[NC];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                const float qr = q < NC - 1 ? qc[q + 1] : q_in;
+                const float lamU = K1 * (qr - qc[q]);
+                const float lamW = K1 * (qa[q] - qc[q]);
+                oP[q] = qc[q] * dp[q];
+                oX[q] = eb[q].x * lX[q] + dx[q] * lamU;
+                oY[q] = eb[q].y * lY[q] + dy[q] * lamW;
+                const float uxl = q > 0 ? ux[q - 1] : ux_in;
+                const float S = (ux[q] - uxl) + (vy[q] * dy[q] - vyn[q] * dyn[q]);
+                tP[q] = mu[q] != 0.0f ? qc[q] * K1 * S / dp[q] : 0.0f;
+                tX[q] = vx[q] * lamU;
+                tY[q] = vy[q] * lamW;
+            }
+            if (commit) {
+                const int64_t ob = o;
+#pragma unroll
+                for (int q = 0; q < NC; ++q) {
+                    if (!((commit >> q) & 1u)) continue;
+                    lout[ob + q] = oP[q];
+                    lout[pl + ob + q] = oX[q];
+                    lout[2 * pl + ob + q] = oY[q];
+                    if (tP[q] != 0.0f) A.gP[ob + q] += (double)tP[q];
+                    A.gX[ob + q] += (double)tX[q];
+                    A.gY[ob + q] += (double)tY[q];
+                    if (byte_at(kc, q) & CODE_ZINV_BIT) {
+                        const float4 ez = __ldg(tab + 3 * byte_at(d_c, q) + 2);
+                        const float pc = s1[ob + q], pr = s1[ob + q + 1], pt = s1[ob + q - pitch];
+                        A.gZ[ob + q] += (double)(ez.x * pc - ez.y * pr) * (double)lX[q] +
+                                        (double)(ez.z * pc - ez.w * pt) * (double)lY[q];
+                    }
+                }
+            }
+        }
+        // ---- shift the row pipeline
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            qa[q] = qc[q];
+            lP[q] = lP1[q]; lX[q] = lX1[q]; lY[q] = lYn[q];
+            dp[q] = dp1[q]; dx[q] = dx1[q]; dy[q] = dyn[q];
+            vx[q] = vx1[q]; vy[q] = vyn[q];
+            lYn[q] = lY2[q]; dyn[q] = dy2[q]; vyn[q] = vy2[q];
+        }
+        d_c = d_n;
+        d_n = d_2;
+    }
+}
+
+constexpr int kAdjNC = 2, kAdjTR = 16, kAdjWarps = 4;
+
 // Slot 0 of every tube's history = the state before the first step of a
 // segment (P, Vx, Vy of parity par).
 __global__ void history_seed_kernel(const TubeDev* __restrict__ tubes, int par) {
@@ -340,11 +558,18 @@ cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_
     return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_tiles,
-                                const AdjRun* run, int local, cudaStream_t stream) {
-    const dim3 grid(max_tiles, ntubes);
-    adjoint_step_kernel<<<grid, kAdjTileW * kAdjTileH, 0, stream>>>(tubes, adj, run, local);
+cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_blocks,
+                                const AdjRun* run, int local, cudaStream_t stream, int form) {
+    const dim3 grid(max_blocks, ntubes);
+    if (form == ADJ_FORM_TILES)
+        adjoint_step_kernel<<<grid, kAdjTileW * kAdjTileH, 0, stream>>>(tubes, adj, run, local);
+    else
+        adjoint_strip_kernel<kAdjNC, kAdjTR, kAdjWarps><<<grid, kAdjWarps * 32, 0, stream>>>(tubes, adj, run, local);
     return cudaGetLastError();
 }
+
+int adjoint_strips(int H, int W) { return ((W - 2) / (30 * kAdjNC) + 1) * ((H - 2 + kAdjTR - 1) / kAdjTR); }
+
+int adjoint_strip_blocks(int strips) { return (strips + kAdjWarps - 1) / kAdjWarps; }
 
 }  // namespace vsb

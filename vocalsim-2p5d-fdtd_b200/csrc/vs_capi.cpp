@@ -119,6 +119,7 @@ struct vs_batch {
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
     int cluster_state = 0;                 // cluster shape: 0 = not checked, 1 = fits, -1 = does not
     uint32_t wait_polls = 0;               // RunState::wait_polls of every run (0 = the default limit)
+    int adj_form = ADJ_FORM_STRIPS;        // reverse-step kernel form (vs_batch_set_adjoint_form)
     ClusterConfig cluster{};
     // adjoint: checkpoints of the last checkpointed forward, history, adjoint planes
     int64_t ck_steps = 0;                  // steps of the checkpointed forward (0 = none)
@@ -151,6 +152,7 @@ struct vs_batch {
     cudaGraphExec_t hist_graph = nullptr;  // ck_every history steps
     cudaGraphExec_t adj_graph = nullptr;   // ck_every reverse steps
     int adj_graph_len = 0;
+    int adj_graph_form = -1;
 
     ~vs_batch() { release(); }
 
@@ -935,7 +937,8 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         if (g.tmm) total += align_up((size_t)(K + 1) * 6 * sizeof(double)) + align_up(8 * sizeof(double));
         zero_len[i] = total - zero_off[i];
         const int tiles = ((g.W - 2 + kAdjTileW - 1) / kAdjTileW) * ((g.H - 2 + kAdjTileH - 1) / kAdjTileH);
-        max_tiles = std::max(max_tiles, tiles);
+        const int blocks = b->adj_form == ADJ_FORM_TILES ? tiles : adjoint_strip_blocks(adjoint_strips(g.H, g.W));
+        max_tiles = std::max(max_tiles, blocks);
         max_plane = std::max(max_plane, g.H * g.pitch);
     }
     if (total != b->adj_bytes) {
@@ -1018,7 +1021,9 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         adj[i].exc_coef = d_coef;
         adj[i].n_exc = (int32_t)nb;
         adj[i].tiles = ((g.W - 2 + kAdjTileW - 1) / kAdjTileW) * ((g.H - 2 + kAdjTileH - 1) / kAdjTileH);
-        if (g.tmm) max_tiles = std::max(max_tiles, adj[i].tiles + 1);
+        adj[i].strips = adjoint_strips(g.H, g.W);
+        const int blocks = b->adj_form == ADJ_FORM_TILES ? adj[i].tiles : adjoint_strip_blocks(adj[i].strips);
+        if (g.tmm) max_tiles = std::max(max_tiles, blocks + 1);
     }
     if (!b->d_adj) ck(cudaMalloc(&b->d_adj, n * sizeof(AdjTube)), "cudaMalloc(adjoint descriptors)");
     if (!b->d_adjrun) ck(cudaMalloc(&b->d_adjrun, sizeof(AdjRun)), "cudaMalloc(adjoint run state)");
@@ -1035,11 +1040,12 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         return launch_step_history(hshape, b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, j, b->stream);
     };
     auto adj_step = [&](int j) { return launch_adjoint_step(b->d_tubes, b->d_adj, n, max_tiles, b->d_adjrun, j,
-                                                            b->stream); };
-    if (b->adj_graph_len != K || !b->hist_graph || !b->adj_graph) {
+                                                            b->stream, b->adj_form); };
+    if (b->adj_graph_len != K || b->adj_graph_form != b->adj_form || !b->hist_graph || !b->adj_graph) {
         capture(b, &b->hist_graph, "capture history steps", hist_step, K);
         capture(b, &b->adj_graph, "capture reverse steps", adj_step, K);
         b->adj_graph_len = K;
+        b->adj_graph_form = b->adj_form;
     }
     int q = 0;                    // lambda parity holding the adjoint of the later state
     for (int k = b->ck_count - 1; k >= 0; --k) {
@@ -1362,6 +1368,13 @@ int vs_batch_set_tile(vs_batch* b, int32_t tile_index) {
     const int s = tile_index < 0 ? default_shape(b) : tile_index;
     if (!shape_fits(b, s)) return set_error(VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)");
     b->shape = s;
+    return VS_OK;
+}
+
+int vs_batch_set_adjoint_form(vs_batch* b, int32_t form) {
+    if (!b || (form != ADJ_FORM_STRIPS && form != ADJ_FORM_TILES))
+        return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_adjoint_form: form must be 0 (strips) or 1 (tiles)");
+    b->adj_form = form;
     return VS_OK;
 }
 

@@ -229,7 +229,8 @@ struct AdjTube {
     const int32_t* exc_off;
     const float* exc_coef;
     int32_t n_exc;
-    int32_t tiles;        // 32 x 8 cell tiles of the interior
+    int32_t tiles;        // 32 x 8 cell tiles of the interior (tile form)
+    int32_t strips;       // row-marching strips of the interior (strip form)
     // per-cell neighbourhood descriptors (H x pitch bytes) into a table of
     // three float4 per descriptor: (ax, ay, bx, by), (alx, aly, 1 + sigma,
     // Dirichlet no-pressure flag), (zc_out x, zc_in x, zc_out y, zc_in y)
@@ -255,8 +256,15 @@ constexpr int kAdjTileW = 32, kAdjTileH = 8;
 // and, for the two-mass source, its reverse step.  max_tiles = the largest
 // AdjTube::tiles of the batch, plus one when a tube has the two-mass source
 // (its reverse step runs in the block after the tiles).
-cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_tiles,
-                                const AdjRun* run, int local, cudaStream_t stream);
+// Two implementations of the same reverse step: 32 x 8 tiles with mu in
+// shared memory, or row-marching warp strips with several columns per lane
+// (the default).  max_blocks = the largest block count of a tube in the
+// chosen form, plus one when a tube has the two-mass source.
+enum : int { ADJ_FORM_STRIPS = 0, ADJ_FORM_TILES = 1 };
+cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_blocks,
+                                const AdjRun* run, int local, cudaStream_t stream, int form);
+int adjoint_strips(int H, int W);             // strips of an H x W frame
+int adjoint_strip_blocks(int strips);         // CTAs those strips take
 
 // Copy each tube's state (parity par) into slot 0 of its history (and the
 // two-mass state into slot 0 of tmm_hist).

@@ -157,6 +157,10 @@ class Batch:
     def set_tile(self, index: int) -> None:
         check(self.lib, self.lib.vs_batch_set_tile(self.h, index), "vs_batch_set_tile")
 
+    def set_adjoint_form(self, form: int) -> None:
+        """Reverse-step kernel of adjoint(): 0 = warp strips (default), 1 = tiles."""
+        check(self.lib, self.lib.vs_batch_set_adjoint_form(self.h, form), "vs_batch_set_adjoint_form")
+
     def set_wait_limit(self, polls: int) -> None:
         """Polls of a row-copy wait before the run gives up with VS_ERR_TIMEOUT (0 = default)."""
         check(self.lib, self.lib.vs_batch_set_wait_limit(self.h, polls), "vs_batch_set_wait_limit")
