@@ -369,16 +369,36 @@ def inversion_cost(iters: int) -> dict:
     ps, gs, targets, seeds = synthetic_problem(INV_TUBES, INV_SRATE_MUL, INV_STEPS, fast_math=1)
     inv = BatchInversion(ps, gs, targets, INV_STEPS, ckpt_every=512, lr=0.02)
     cells = inv.batch.interior_cells
-    secs, losses = [], []
+    secs, losses, parts = [], [], []
     for _ in range(iters):
         t0 = time.perf_counter()
         losses.append(inv.step())
         secs.append(time.perf_counter() - t0)
+        parts.append(inv.timings)
+    # the plain batched forward of the same tubes (graph-replayed steps, device trace)
+    import torch
+    fwd = inv.batch
+    fwd.reset()
+    torch.cuda.synchronize()
+    from vocalsim_b200.abi import VS_ERR_NONFINITE, VsError
+    t0 = time.perf_counter()
+    try:
+        fwd.run_device(INV_STEPS)
+    except VsError as e:                # a tube near the stability limit: the time still counts
+        if e.status != VS_ERR_NONFINITE:
+            raise
+    torch.cuda.synchronize()
+    fwd_s = time.perf_counter() - t0
+    fwd.reset()
+    split = {k: round(statistics.median(p[k] for p in parts), 3) for k in parts[0]}
     best = float(inv.best.mean())
     inv.close()
     return {"workload": f"{INV_TUBES} tubes (stable seeds {seeds[0]}..{seeds[-1]}), fs 44100 x {INV_SRATE_MUL}, "
                         f"{INV_STEPS} steps, {cells} interior cells, checkpoints every 512, fast_math=1",
             "iterations": iters, "s_per_iteration": round(statistics.median(secs), 3),
+            "split_s": split, "plain_forward_s": round(fwd_s, 3),
+            # gradient (recomputation + reverse steps) against one plain forward, at batch scale
+            "grad_fwd_ratio_batch": round((split["recompute_s"] + split["reverse_s"]) / fwd_s, 3),
             "spectral_error_initial": round(float(np.nanmean(losses[0])), 4),
             "spectral_error_best": round(best, 4),
             "diverged_steps": int(sum(np.isnan(x).sum() for x in losses))}

@@ -244,6 +244,11 @@ int vs_batch_set_stream(vs_batch* b, void* cuda_stream);
  * batches when the band fits a CTA's shared memory. */
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
 
+/* Device time of the last vs_batch_adjoint call, split into the segments'
+ * recomputation (history-capturing forward steps) and the reverse steps
+ * (ms, CUDA events).  No counterpart in the reference. */
+int vs_batch_adjoint_times(const vs_batch* b, float* recompute_ms, float* reverse_ms);
+
 /* Kernel form of the reverse steps of vs_batch_adjoint, no counterpart in the
  * reference: 0 = row-marching warp strips with four columns per lane (the
  * default), 1 = 32 x 8 tiles with mu in shared memory.  Both compute the same

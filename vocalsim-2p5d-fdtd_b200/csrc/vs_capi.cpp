@@ -153,6 +153,8 @@ struct vs_batch {
     cudaGraphExec_t adj_graph = nullptr;   // ck_every reverse steps
     int adj_graph_len = 0;
     int adj_graph_form = -1;
+    float adj_recompute_ms = 0.0f;         // device time of the last adjoint's recomputation / reverse steps
+    float adj_reverse_ms = 0.0f;
 
     ~vs_batch() { release(); }
 
@@ -1048,6 +1050,10 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         b->adj_graph_form = b->adj_form;
     }
     int q = 0;                    // lambda parity holding the adjoint of the later state
+    // events around each segment's recomputation and reverse steps, for the
+    // time split vs_batch_adjoint_times reports
+    std::vector<cudaEvent_t> ev(3 * (size_t)b->ck_count, nullptr);
+    for (cudaEvent_t& e : ev) ck(cudaEventCreate(&e), "event");
     for (int k = b->ck_count - 1; k >= 0; --k) {
         const int64_t start = (int64_t)k * K;
         const int len = (int)std::min<int64_t>(K, steps - start);
@@ -1061,17 +1067,31 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         ck(cudaMemcpyAsync(b->d_rs, &rs, sizeof(rs), cudaMemcpyHostToDevice, b->stream), "set run state");
         const AdjRun ar{start, len, q};
         ck(cudaMemcpyAsync(b->d_adjrun, &ar, sizeof(ar), cudaMemcpyHostToDevice, b->stream), "set adjoint run");
+        ck(cudaEventRecord(ev[3 * k], b->stream), "event");
         ck(launch_history_seed(b->d_tubes, n, max_plane, (int)(start & 1), b->stream), "history seed");
         if (len == K) {
             ck(cudaGraphLaunch(b->hist_graph, b->stream), "history graph");
+            ck(cudaEventRecord(ev[3 * k + 1], b->stream), "event");
             ck(cudaGraphLaunch(b->adj_graph, b->stream), "reverse graph");
         } else {
             for (int j = 0; j < len; ++j) ck(hist_step(j), "history step");
+            ck(cudaEventRecord(ev[3 * k + 1], b->stream), "event");
             for (int j = 0; j < len; ++j) ck(adj_step(j), "adjoint step");
         }
+        ck(cudaEventRecord(ev[3 * k + 2], b->stream), "event");
         q ^= len & 1;
     }
     ck(cudaStreamSynchronize(b->stream), "adjoint sync");
+    b->adj_recompute_ms = 0.0f;
+    b->adj_reverse_ms = 0.0f;
+    for (int k = 0; k < b->ck_count; ++k) {
+        float a = 0.0f, r = 0.0f;
+        ck(cudaEventElapsedTime(&a, ev[3 * k], ev[3 * k + 1]), "elapsed");
+        ck(cudaEventElapsedTime(&r, ev[3 * k + 1], ev[3 * k + 2]), "elapsed");
+        b->adj_recompute_ms += a;
+        b->adj_reverse_ms += r;
+    }
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
     // gradients to the caller, frame by frame (unpadded)
     size_t cell_off = 0;
     for (int i = 0; i < n; ++i) {
@@ -1368,6 +1388,13 @@ int vs_batch_set_tile(vs_batch* b, int32_t tile_index) {
     const int s = tile_index < 0 ? default_shape(b) : tile_index;
     if (!shape_fits(b, s)) return set_error(VS_ERR_UNSUPPORTED, "launch shape unavailable for this batch (shared memory, wall oscillator or fast_math)");
     b->shape = s;
+    return VS_OK;
+}
+
+int vs_batch_adjoint_times(const vs_batch* b, float* recompute_ms, float* reverse_ms) {
+    if (!b) return set_error(VS_ERR_INVALID_ARG, "null batch");
+    if (recompute_ms) *recompute_ms = b->adj_recompute_ms;
+    if (reverse_ms) *reverse_ms = b->adj_reverse_ms;
     return VS_OK;
 }
 

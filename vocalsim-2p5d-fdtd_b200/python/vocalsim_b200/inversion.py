@@ -97,12 +97,22 @@ class BatchInversion:
         for a tube whose forward diverged; it backtracks instead)."""
         params = (self.log_w, self.log_d, self.log_z)
         self.opt.zero_grad()
+        t0 = time.perf_counter()
         per_tube = self.loss()
+        t1 = time.perf_counter()
         ok = torch.isfinite(per_tube).detach()
         if not ok.any():
             raise RuntimeError("the forward diverged for every tube")
         self.best = torch.where(ok, torch.minimum(self.best, per_tube.detach()), self.best)
         torch.where(ok, per_tube, torch.zeros_like(per_tube)).sum().backward()
+        t2 = time.perf_counter()
+        rec, rev = self.batch.adjoint_times()
+        # wall time of this iteration's parts (s): the forward (depth maps on
+        # the device, checkpointed forward, spectral loss), the backward (loss
+        # gradient, adjoint, section reverse pass) and, inside the adjoint, the
+        # device time of the segment recomputation and of the reverse steps
+        self.timings = {"forward_s": t1 - t0, "backward_s": t2 - t1, "recompute_s": rec / 1e3,
+                        "reverse_s": rev / 1e3}
         before = [t.detach().clone() for t in params]
         for t in params:
             t.grad.nan_to_num_(0.0)

@@ -157,6 +157,12 @@ class Batch:
     def set_tile(self, index: int) -> None:
         check(self.lib, self.lib.vs_batch_set_tile(self.h, index), "vs_batch_set_tile")
 
+    def adjoint_times(self) -> tuple[float, float]:
+        """(recomputation ms, reverse-step ms) of the last adjoint(), device time."""
+        a, r = C.c_float(), C.c_float()
+        check(self.lib, self.lib.vs_batch_adjoint_times(self.h, C.byref(a), C.byref(r)), "vs_batch_adjoint_times")
+        return a.value, r.value
+
     def set_adjoint_form(self, form: int) -> None:
         """Reverse-step kernel of adjoint(): 0 = warp strips (default), 1 = tiles."""
         check(self.lib, self.lib.vs_batch_set_adjoint_form(self.h, form), "vs_batch_set_adjoint_form")
