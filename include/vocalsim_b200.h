@@ -329,6 +329,15 @@ int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float*
 int vs_batch_adjoint(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, float* grad_depth_x,
                      float* grad_depth_y, float* grad_z_inv);
 
+/* The same two calls with the traces and dL/dtrace in device memory (n x
+ * steps floats), so a loss computed on the GPU (the spectral loss of the
+ * inversion) feeds the adjoint without a host round trip; the per-cell
+ * gradient outputs stay host buffers.  The work runs on the batch's stream
+ * (vs_batch_set_stream): put the caller's loss kernels on the same stream. */
+int vs_batch_forward_ckpt_device(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces);
+int vs_batch_adjoint_device(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, float* grad_depth_x,
+                            float* grad_depth_y, float* grad_z_inv);
+
 /* Depth maps of every tube from section parameters, computed on the device:
  * the reference's elliptical depth kernel and post-processing
  * (TubeDepth.cu:392-490, 642-762) on each tube's nominal rasterisation (the

@@ -78,3 +78,33 @@ def test_device_section_gradients_equal_the_torch_model(cuda_ok):
         assert torch.count_nonzero(b.grad) > 0
         np.testing.assert_allclose(a.grad.numpy(), b.grad.numpy(), rtol=1e-6, atol=1e-6 * float(b.grad.abs().max()))
     np.testing.assert_allclose(z1.grad.numpy(), z2.grad.numpy(), rtol=1e-6)
+
+
+def test_device_resident_traces_give_the_same_gradients(cuda_ok):
+    """SectionTrace with the traces kept on the GPU (vs_batch_forward_ckpt_device /
+    vs_batch_adjoint_device, the spectral loss on the GPU) gives the traces and
+    section gradients of the host-trace path."""
+    steps = 1500
+    ps, gs, models = _setup(steps)
+    ws, ds, zs = _perturbed(models, 2)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    target = torch.from_numpy(V.Batch([V.params(cross_sectional_shape=2, mu3d=0.025, num_steps=steps)] * 2,
+                                      [V.Geometry(*S.vowel_tube(6))] * 2).run(steps)).double()
+    out = []
+    for device in (None, dev):
+        b = V.Batch(ps, gs)
+        if device is not None:
+            b.set_stream(torch.cuda.current_stream(device).cuda_stream)
+            b.trace_device = device
+        wl = [w.clone().requires_grad_(True) for w in ws]
+        dl = [d.clone().requires_grad_(True) for d in ds]
+        z = zs.clone().requires_grad_(True)
+        tr = SectionTrace.apply(b, steps, 256, z, *wl, *dl)
+        spectral_loss(tr, target.to(tr.device), FS).backward()
+        out.append((tr.detach().cpu(), [t.grad.clone() for t in wl + dl], z.grad.clone()))
+        b.close()
+    (ta, ga, za), (tb, gb, zb) = out
+    assert torch.equal(ta, tb)
+    for a, c in zip(ga, gb):
+        np.testing.assert_allclose(a.numpy(), c.numpy(), rtol=1e-9, atol=1e-9 * float(c.abs().max()))
+    np.testing.assert_allclose(za.numpy(), zb.numpy(), rtol=1e-9)

@@ -766,7 +766,7 @@ void copy_state(vs_batch* b, int k, bool save) {
     }
 }
 
-void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces) {
+void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces, bool traces_on_device = false) {
     check_adjoint_support(b);
     const int n = (int)b->grids.size();
     if (b->shape < 0) b->shape = default_shape(b);
@@ -800,7 +800,8 @@ void forward_checkpointed(vs_batch* b, int64_t steps, int every, float* traces) 
     b->ck_every = every;
     b->ck_count = count;
     if (traces)
-        ck(cudaMemcpyAsync(traces, b->d_trace, need * sizeof(float), cudaMemcpyDeviceToHost, b->stream),
+        ck(cudaMemcpyAsync(traces, b->d_trace, need * sizeof(float),
+                           traces_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream),
            "copy traces");
     ck(cudaStreamSynchronize(b->stream), "forward sync");
 }
@@ -917,7 +918,8 @@ void capture(vs_batch* b, cudaGraphExec_t* out, const char* what, const std::fun
     ck(e3, "instantiate graph");
 }
 
-void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float* gdY, float* gz) {
+void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float* gdY, float* gz,
+                 bool gtrace_on_device = false) {
     if (b->ck_steps <= 0) throw VsFailure{VS_ERR_INVALID_ARG, "run vs_batch_forward_ckpt before vs_batch_adjoint"};
     check_adjoint_support(b);
     const int n = (int)b->grids.size();
@@ -955,7 +957,8 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         ck(cudaMalloc(&b->d_gtrace, (size_t)n * steps * sizeof(float)), "cudaMalloc(trace gradient)");
         b->gtrace_cap = (int64_t)n * steps;
     }
-    ck(cudaMemcpyAsync(b->d_gtrace, gtrace, (size_t)n * steps * sizeof(float), cudaMemcpyHostToDevice, b->stream),
+    ck(cudaMemcpyAsync(b->d_gtrace, gtrace, (size_t)n * steps * sizeof(float),
+                       gtrace_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream),
        "upload trace gradient");
     // excitation lists, neighbourhood descriptors and coefficient tables
     std::vector<std::vector<int32_t>> eoff(n);
@@ -1512,6 +1515,18 @@ int vs_batch_adjoint(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, f
                      float* grad_depth_y, float* grad_z_inv) {
     if (!b || !dL_dtrace) return set_error(VS_ERR_INVALID_ARG, "vs_batch_adjoint arguments");
     return guarded([&] { run_adjoint(b, dL_dtrace, grad_depth_p, grad_depth_x, grad_depth_y, grad_z_inv); });
+}
+
+int vs_batch_forward_ckpt_device(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces) {
+    if (!b || steps < 1 || ckpt_every < 1 || !traces)
+        return set_error(VS_ERR_INVALID_ARG, "vs_batch_forward_ckpt_device arguments");
+    return guarded([&] { forward_checkpointed(b, steps, ckpt_every, traces, true); });
+}
+
+int vs_batch_adjoint_device(vs_batch* b, const float* dL_dtrace, float* grad_depth_p, float* grad_depth_x,
+                            float* grad_depth_y, float* grad_z_inv) {
+    if (!b || !dL_dtrace) return set_error(VS_ERR_INVALID_ARG, "vs_batch_adjoint_device arguments");
+    return guarded([&] { run_adjoint(b, dL_dtrace, grad_depth_p, grad_depth_x, grad_depth_y, grad_z_inv, true); });
 }
 
 int vs_create(const vs_params* p, const vs_geometry* g, vs_solver** out) {

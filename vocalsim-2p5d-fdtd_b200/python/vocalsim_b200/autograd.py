@@ -173,13 +173,24 @@ class SectionTrace(torch.autograd.Function):
         ws = [t.detach().cpu().numpy() for t in sections[:n]]
         ds = [t.detach().cpu().numpy() for t in sections[n:]]
         batch.set_sections(ws, ds, z_inv.detach().cpu().numpy())
-        tr = batch.forward_ckpt(steps, ckpt_every)
         ctx.batch = batch
+        ctx.device = getattr(batch, "trace_device", None)
+        if ctx.device is not None:
+            # traces stay on the GPU: the loss and its gradient are computed there
+            # and dL/dtrace goes back to the adjoint without a host copy
+            tr = torch.empty((n, steps), dtype=torch.float32, device=ctx.device)
+            batch.forward_ckpt_device(steps, ckpt_every, tr.data_ptr())
+            return tr.to(torch.float64)
+        tr = batch.forward_ckpt(steps, ckpt_every)
         return torch.from_numpy(tr).to(torch.float64)
 
     @staticmethod
     def backward(ctx, grad_trace: torch.Tensor):
-        _, gz = ctx.batch.adjoint(grad_trace.detach().to(torch.float32).cpu().numpy(), maps=False)
+        if ctx.device is not None:
+            g32 = grad_trace.detach().to(device=ctx.device, dtype=torch.float32).contiguous()
+            gz = ctx.batch.adjoint_device(g32.data_ptr())
+        else:
+            _, gz = ctx.batch.adjoint(grad_trace.detach().to(torch.float32).cpu().numpy(), maps=False)
         g = ctx.batch.section_gradients()
         return (None, None, None, torch.from_numpy(gz.astype(np.float64)),
                 *[torch.from_numpy(w) for w, _ in g], *[torch.from_numpy(d) for _, d in g])

@@ -58,12 +58,17 @@ class BatchInversion:
         self.width0 = [torch.tensor(lay["major"], dtype=torch.float64) for lay in lays]
         self.depth0 = [torch.tensor(lay["minor"], dtype=torch.float64) for lay in lays]
         self.batch = Batch(ps, gs)
+        # traces, spectra and the loss live on the GPU, on torch's current
+        # stream, which the batch also uses (no host round trip of traces)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.batch.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+        self.batch.trace_device = self.device
         self.n = len(ps)
         self.steps = steps
         self.ckpt_every = ckpt_every
         self.fs = 44100.0 * ps[0].srate_mul
         self.fmax = fmax
-        targets = torch.as_tensor(np.asarray(targets), dtype=torch.float64).reshape(self.n, steps)
+        targets = torch.as_tensor(np.asarray(targets), dtype=torch.float64).reshape(self.n, steps).to(self.device)
         self.target_spec = log_power_spectrum(targets, self.fs, fmax)
         self.amp_limit = 100.0 * targets.abs().amax(dim=1)
         self.best = torch.full((self.n,), float("inf"), dtype=torch.float64)
@@ -90,7 +95,7 @@ class BatchInversion:
         per_tube = (d * d).mean(dim=-1)
         # a diverging trace counts as not finite
         grown = tr.detach().abs().amax(dim=1) > self.amp_limit
-        return torch.where(grown, torch.full_like(per_tube, float("nan")), per_tube)
+        return torch.where(grown, torch.full_like(per_tube, float("nan")), per_tube).cpu()
 
     def step(self) -> np.ndarray:
         """One Adam iteration; returns each tube's loss before the update (NaN

@@ -124,6 +124,7 @@ class Batch:
             if g is not None:
                 garr[i] = g.struct
         self.n = n
+        self.trace_device = None        # a torch device: SectionTrace keeps traces there
         self.h = C.c_void_p()
         check(self.lib, self.lib.vs_batch_create(n, parr, garr, C.byref(self.h)), "vs_batch_create")
         self.dims = []
@@ -183,6 +184,19 @@ class Batch:
         check(self.lib, self.lib.vs_batch_forward_ckpt(self.h, steps, ckpt_every, _fp(tr)), "vs_batch_forward_ckpt")
         self._ck_steps = steps
         return tr
+
+    def forward_ckpt_device(self, steps: int, ckpt_every: int, traces_ptr: int) -> None:
+        """forward_ckpt with the (n, steps) float32 traces written to device memory at traces_ptr."""
+        check(self.lib, self.lib.vs_batch_forward_ckpt_device(self.h, steps, ckpt_every, C.c_void_p(traces_ptr)),
+              "vs_batch_forward_ckpt_device")
+        self._ck_steps = steps
+
+    def adjoint_device(self, grad_ptr: int) -> np.ndarray:
+        """adjoint(maps=False) with dL/dtrace (n, steps float32) in device memory; returns dL/dz_inv per tube."""
+        gz = np.zeros(self.n, np.float32)
+        check(self.lib, self.lib.vs_batch_adjoint_device(self.h, C.c_void_p(grad_ptr), None, None, None, _fp(gz)),
+              "vs_batch_adjoint_device")
+        return gz
 
     def set_sections(self, widths, depths, z_inv=None) -> None:
         """Depth maps of every tube from its section widths / depths (m), computed
