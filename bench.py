@@ -431,6 +431,19 @@ def run_b200(args, rank, world):
         ba.adjoint((tr * 1e-3).astype(np.float32))
         ba.close()
         return None
+    if args.profile_single:
+        # profiling workload of the cluster kernel: the uniform 17.5 x 3 cm tube,
+        # `profile_single` steps in one launch after a 256-step warm-up launch
+        from vocalsim_b200 import synthetic as S
+        s1 = V.Solver(V.params(mu3d=0.005, uniform_depth_m=0.02, fast_math=fast), V.Geometry(*S.uniform_tube()))
+        s1.set_stream(stream.cuda_stream)
+        buf = torch.empty(args.profile_single, dtype=torch.float32, device=dev)
+        s1.run_device(256, buf.data_ptr())
+        s1.reset()
+        s1.run_device(args.profile_single, buf.data_ptr())
+        torch.cuda.synchronize()
+        s1.close()
+        return None
     if args.profile_steps:
         if args.tile >= 0:
             batch.set_tile(args.tile)
@@ -651,6 +664,8 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=0)
     ap.add_argument("--profile-adjoint", type=int, default=0,
                     help="run a 16-tube checkpointed forward + adjoint of this many steps, untimed, for ncu")
+    ap.add_argument("--profile-single", type=int, default=0,
+                    help="run the uniform tube for this many steps on the cluster kernel, untimed, for ncu")
     ap.add_argument("--tile", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-single", action="store_true")
