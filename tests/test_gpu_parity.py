@@ -4,8 +4,8 @@ The kernel evaluates the reference engine's expressions with round-to-nearest
 intrinsics in the reference operand order, so on the same maps its FP32
 trace and fields must EQUAL the oracle's FP32 restatement of
 FDTDEngineCPU / FDTDEngineEigen (value equality; +0 and -0 compare equal).
-Against the double-precision restatement the tolerance is the north-star
-bound: relative L2 <= 1e-4.
+Against the double-precision restatement the tolerance is relative L2
+<= 1e-4.
 """
 import numpy as np
 import pytest

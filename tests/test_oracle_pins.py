@@ -74,8 +74,8 @@ def test_double_two_mass_model_tracks_the_fp64_restatement():
     assert err[1] <= 1e-4 and err[0] > 1e-3, err
 
 
-def test_survey_known_answers():
-    """Constants derived while surveying the reference (float probes of its expressions)."""
+def test_known_answers():
+    """Constants computed by float probes of the reference's own expressions."""
     k15, k30 = O.consts(15), O.consts(30)
     assert k15[3] == np.float32(1.51171582e-06) and k30[3] == np.float32(7.55857911e-07)
     assert k15[4] == np.float32(7.48261169e-04) and k30[4] == np.float32(3.74130585e-04)
