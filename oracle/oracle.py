@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
         L.orc_run_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, dp]
         L.orc_run_maps_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, C.c_double, dp]
         L.orc_run_maps_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, C.c_float, fp]
+        L.orc_run_maps_f32_fields.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, C.c_float, fp, fp, fp, fp]
         L.orc_set_sps_diameters.argtypes = [fp, C.c_int]
         _orc = L
     return _orc
@@ -207,13 +208,22 @@ def run_maps_f64(p: VsParams, g: Geometry | None, steps: int, depth_p, depth_x, 
     return tr
 
 
-def run_maps_f32(p: VsParams, g: Geometry | None, steps: int, depth_p, depth_x, depth_y, z_inv: float) -> np.ndarray:
-    """FP32 trace of the engine on the given depth maps (rounded to float) and z_inv value."""
+def run_maps_f32(p: VsParams, g: Geometry | None, steps: int, depth_p, depth_x, depth_y, z_inv: float,
+                 fields: bool = False):
+    """FP32 trace of the engine on the given depth maps (rounded to float) and z_inv value
+    (and, with fields=True, the final P, Vx, Vy frames)."""
     mp, mx, my = (np.ascontiguousarray(a, np.float32).reshape(-1) for a in (depth_p, depth_x, depth_y))
     tr = np.zeros(steps, np.float32)
-    _check(lib().orc_run_maps_f32(C.byref(p), g.ref() if g is not None else None, steps, _fp(mp), _fp(mx), _fp(my),
-                                  float(z_inv), _fp(tr)), "run_maps_f32")
-    return tr
+    gp = g.ref() if g is not None else None
+    if not fields:
+        _check(lib().orc_run_maps_f32(C.byref(p), gp, steps, _fp(mp), _fp(mx), _fp(my), float(z_inv), _fp(tr)),
+               "run_maps_f32")
+        return tr
+    F = [np.zeros(mp.size, np.float32) for _ in range(3)]
+    _check(lib().orc_run_maps_f32_fields(C.byref(p), gp, steps, _fp(mp), _fp(mx), _fp(my), float(z_inv), _fp(tr),
+                                         *[_fp(a) for a in F]), "run_maps_f32_fields")
+    shp = np.shape(depth_p)
+    return tr, [a.reshape(shp) for a in F]
 
 
 def source(p: VsParams, n: int) -> np.ndarray:

@@ -1096,6 +1096,22 @@ int orc_run_maps_f32(const vs_params* p, const vs_geometry* g, long long steps, 
     } catch (const OracleError& e) { return fail(e); }
 }
 
+/* orc_run_maps_f32 that also returns the final P, Vx, Vy frames (any may be NULL). */
+int orc_run_maps_f32_fields(const vs_params* p, const vs_geometry* g, long long steps, const float* dP,
+                            const float* dX, const float* dY, float zinv_val, float* trace, float* P, float* Vx,
+                            float* Vy) {
+    try {
+        Grid G;
+        build_grid(p, g, G);
+        Coeffs C;
+        build_coeffs(G, C);
+        const size_t N = (size_t)G.H * G.W;
+        std::vector<double> mP(dP, dP + N), mX(dX, dX + N), mY(dY, dY + N), zin(N, 0.0);
+        for (size_t i = 0; i < N; i++) if (G.bst[i] != 0) zin[i] = zinv_val;
+        return run_engine<float>(p, G, C, steps, trace, P, Vx, Vy, &mP, &mX, &mY, &zin);
+    } catch (const OracleError& e) { return fail(e); }
+}
+
 /* The same discrete system in double precision. */
 int orc_run_f64(const vs_params* p, const vs_geometry* g, long long steps, double* trace,
                 double* P, double* Vx, double* Vy) {

@@ -1,0 +1,86 @@
+"""BASELINE config 2 at full length: the 1 s vowel tube (seed 0, 44 sections,
+3:1 elliptical, two-mass source at 800 Pa), 661 500 steps, on the default
+single-tube path (the cluster kernel).
+
+* Reference arithmetic (fast_math = 0): the GPU trace equals the FP32 oracle
+  over all 661 500 steps, bit for bit, with the reference's float two-mass
+  model and with the model in double (tmm_f64).
+* The precision floor: the FP32 system itself drifts from the FP64
+  restatement (the self-oscillating source feeds rounding back into its
+  phase).  With the reference's float model the FP32 trace is ~0.40 away in
+  relative L2 by 1 s and its spectral peaks move by tens of Hz; with the
+  double model it is ~4e-3 away and F1-F4 (the reference's get_formants_bw,
+  1 Hz bins at 1 s) are those of the FP64 trace.  The GPU, equal to the FP32
+  system, has exactly that floor; the 1e-4 relative L2 bound holds over the
+  first 5000 steps (~7.6 ms) with the double model.
+* fast_math = 1 with the double model: F1-F4 equal the FP64 trace's and the
+  relative L2 stays within twice the floor.
+The oracle runs go to host threads (ctypes releases the GIL).
+"""
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+import oracle as O
+import vocalsim_b200 as V
+from formants import formants_bw
+from vocalsim_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 661500
+FS = 44100.0 * 15
+KW = dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0)
+
+
+def rel(a, b, n=None):
+    a = np.asarray(a[:n], np.float64)
+    b = np.asarray(b[:n], np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def runs(cuda_ok):
+    L, A = S.vowel_tube(0)
+    jobs = {"f64": (0, "f64"), "f32_tmm32": (0, "f32"), "f32_tmm64": (1, "f32")}
+    with ThreadPoolExecutor(len(jobs)) as ex:
+        fut = {k: ex.submit(O.run, O.params(**KW, tmm_f64=t), O.Geometry(L, A), STEPS, prec)
+               for k, (t, prec) in jobs.items()}
+        gpu = {}
+        for tmm64 in (0, 1):
+            for fast in (0, 1):
+                s = V.Solver(V.params(**KW, tmm_f64=tmm64, fast_math=fast), V.Geometry(L, A))
+                gpu[(tmm64, fast)] = s.run(STEPS)
+                s.close()
+        orc = {k: f.result() for k, f in fut.items()}
+    return gpu, orc
+
+
+@pytest.mark.parametrize("tmm64", [0, 1])
+def test_config2_gpu_equals_the_fp32_system_for_one_second(runs, tmm64):
+    gpu, orc = runs
+    ref = orc["f32_tmm64" if tmm64 else "f32_tmm32"]
+    got = gpu[(tmm64, 0)]
+    assert np.array_equal(got, ref), f"first difference at step {int(np.argmax(got != ref))}"
+    assert np.all(np.isfinite(got)) and np.abs(got).max() > 0
+
+
+def test_config2_double_model_formants_within_1hz(runs):
+    gpu, orc = runs
+    want = formants_bw(orc["f64"], FS, 4)[1]
+    for fast in (0, 1):
+        got = formants_bw(gpu[(1, fast)].astype(np.float64), FS, 4)[1]
+        assert np.all(want > 0) and np.all(np.abs(got - want) <= 1.0), (fast, got, want)
+
+
+def test_config2_precision_floor(runs):
+    gpu, orc = runs
+    d = orc["f64"]
+    floor = rel(orc["f32_tmm64"], d)
+    assert rel(gpu[(1, 0)], d) == floor                  # the GPU is the FP32 system
+    assert rel(gpu[(1, 1)], d) <= 2 * floor + 1e-6       # fast_math within twice the floor
+    assert rel(gpu[(1, 0)], d, 5000) <= 1e-4             # the 1e-4 bound where it holds
+    assert rel(gpu[(1, 1)], d, 5000) <= 1e-4
+    # the reference's float model: the FP32 system's own drift, recorded
+    assert rel(gpu[(0, 0)], d) == rel(orc["f32_tmm32"], d) > 10 * floor

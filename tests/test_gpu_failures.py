@@ -22,7 +22,6 @@ from vocalsim_b200 import synthetic as S
 pytestmark = pytest.mark.gpu
 
 BAND_SHAPE = 12            # band_kernel<4>: one cp.async.bulk per plane per band
-STAGED_QUAD_SHAPE = 24     # quad strips with 4 bulk-copy row stages
 CLUSTER = len(V.tile_shapes()) - 1
 
 
@@ -32,7 +31,10 @@ def _tubes():
         [V.Geometry(*t) for t in tubes], tubes
 
 
-@pytest.mark.parametrize("shape", [BAND_SHAPE, STAGED_QUAD_SHAPE])
+# The band kernel waits right after issuing its copies, so one poll cannot see
+# them land; the staged quad strips issue several rows ahead before their
+# first wait, so a one-poll limit does not reliably run out there.
+@pytest.mark.parametrize("shape", [BAND_SHAPE])
 def test_wait_that_runs_out_returns_timeout_and_the_next_run_is_clean(cuda_ok, shape):
     ps, gs, tubes = _tubes()
     b = V.Batch(ps, gs)

@@ -2,12 +2,17 @@
 
 tests/golden/reference_engine.npz holds record_pressure of the reference's
 FDTDEngineCPU run after its own setupWaveSolver (built from the reference
-sources, tests/golden/make_reference_engine.py).  vs_run in the reference
-arithmetic (fast_math = 0) must give the same trace bit for bit; with the
-reciprocal form (fast_math = 1) the trace stays within the FP32 reference's
-own distance from the double-precision restatement (x2 + 1e-6).  Where the
-reference engine is built here (oracle/_ref/ref_engine) two cases are also
-run live, to show the fixture is what that binary computes on this machine.
+sources, tests/golden/make_reference_engine.py).  The library is given the
+reference's own depth maps and z_inv (vs_batch_set_maps; the cell types it
+builds itself equal the reference's in every case), so the comparison covers
+the time loop whatever the reference's depth kernels computed.  vs_run in the
+reference arithmetic (fast_math = 0) must give the same trace bit for bit; a
+single tube runs on the cluster kernel by default, the strip kernels are run
+too.  With the reciprocal form (fast_math = 1) the trace stays within the
+FP32 reference's own distance from the FP64 engine on the same maps (x2 +
+1e-6).  Where the reference engine is built here (oracle/_ref/ref_engine),
+two circular-section cases are also run live, to show the fixture is what
+that binary computes on this machine.
 """
 import json
 from pathlib import Path
@@ -24,6 +29,7 @@ if not GOLD.exists():
 G = np.load(GOLD)
 CASES = json.loads(str(G["cases_json"]))
 IDS = [f"c{c['case']}-{c['geometry']}" for c in CASES]
+STRIP_SHAPE = 7
 
 
 def inputs(c):
@@ -32,34 +38,51 @@ def inputs(c):
     return dict(c["params"]), geo
 
 
+def reference_maps(c):
+    i = c["case"]
+    zmap = G[f"c{i}_z_inv"]
+    zval = float(zmap[zmap != 0][0]) if np.any(zmap != 0) else 0.0
+    return G[f"c{i}_depth_p"], G[f"c{i}_depth_x"], G[f"c{i}_depth_y"], zval
+
+
+def run_on_reference_maps(c, shape=None, **extra):
+    kw, geo = inputs(c)
+    b = V.Batch([V.params(**kw, **extra)], [V.Geometry(*geo) if geo is not None else None])
+    dp, dx, dy, zval = reference_maps(c)
+    b.set_maps(0, dp, dx, dy, zval)
+    if shape is not None:
+        b.set_tile(shape)
+    tr = b.run(c["steps"])[0]
+    b.close()
+    return tr
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("c", CASES, ids=IDS)
 def test_gpu_trace_equals_the_reference_engine(cuda_ok, c):
-    kw, geo = inputs(c)
     ref = G[f"c{c['case']}_trace"]
-    s = V.Solver(V.params(**kw), V.Geometry(*geo) if geo is not None else None)
-    tr = s.run(c["steps"])
-    s.close()
-    assert np.array_equal(tr, ref), f"first difference at step {int(np.argmax(tr != ref))}"
+    for shape in (None, STRIP_SHAPE):          # default (cluster kernel), strip kernel
+        tr = run_on_reference_maps(c, shape)
+        assert np.array_equal(tr, ref), f"shape {shape}: first difference at step {int(np.argmax(tr != ref))}"
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("c", [c for c in CASES if c["params"].get("source_type", 1) != 2][:6], ids=lambda c: f"c{c['case']}")
+@pytest.mark.parametrize("c", [c for c in CASES if c["params"].get("source_type", 1) != 2][:8],
+                         ids=lambda c: f"c{c['case']}")
 def test_gpu_fast_math_within_the_reference_rounding(cuda_ok, c):
     kw, geo = inputs(c)
+    dp, dx, dy, zval = reference_maps(c)
+    d = O.run_maps_f64(O.params(**kw), O.Geometry(*geo) if geo is not None else None, c["steps"],
+                       dp.astype(np.float64), dx.astype(np.float64), dy.astype(np.float64), zval)
     ref = G[f"c{c['case']}_trace"].astype(np.float64)
-    g64 = O.Geometry(*geo) if geo is not None else None
-    d = O.run(O.params(**kw), g64, c["steps"], "f64")
-    s = V.Solver(V.params(**kw, fast_math=1), V.Geometry(*geo) if geo is not None else None)
-    tr = s.run(c["steps"]).astype(np.float64)
-    s.close()
+    tr = run_on_reference_maps(c, None, fast_math=1).astype(np.float64)
     rel = lambda a: np.linalg.norm(a - d) / np.linalg.norm(d)  # noqa: E731
     assert rel(tr) <= 2 * rel(ref) + 1e-6, (rel(tr), rel(ref))
 
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not O.REF_ENGINE.exists(), reason="oracle/_ref/ref_engine not built")
-@pytest.mark.parametrize("case", [1, 9])
+@pytest.mark.parametrize("case", [0, 10])
 def test_reference_engine_reproduces_the_fixture(cuda_ok, case):
     c = next(x for x in CASES if x["case"] == case)
     kw, geo = inputs(c)
@@ -67,3 +90,4 @@ def test_reference_engine_reproduces_the_fixture(cuda_ok, case):
     r = O.reference_engine(O.params(**kw), O.Geometry(*geo) if geo is not None else None, steps)
     assert np.array_equal(r["trace"], G[f"c{case}_trace"][:steps])
     assert np.array_equal(r["cell_type"], G[f"c{case}_cell_type"].astype(np.int32))
+    assert np.array_equal(r["depth_x"], G[f"c{case}_depth_x"])
