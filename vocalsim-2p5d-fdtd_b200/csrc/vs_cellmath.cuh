@@ -27,7 +27,18 @@ constexpr unsigned kFull = 0xffffffffu;
 // One step of the Ishizaka-Flanagan two-mass model, TwoMassModel.cpp:90-232,
 // in the reference's mixed float/double precision and operand order.  The
 // reference's host build (g++) forms (rho/2)*fabs(ug) in double.
-__device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1) {
+// The model step split at its one use of the supraglottal pressure p1: the
+// first part depends on the state alone (the new displacements and the flow
+// equation's coefficients), so a caller can evaluate it before p1 is known;
+// tmm_finish applies p1 and commits the state.  prepare + finish performs
+// exactly the operations of one step, in the same order.
+struct TmmPrep {
+    float x1, x1n, x2, x2n, ug;     // state before / after the displacement update, flow before
+    float Lug, den, srate, ps;      // ugn = ((ps - p1) / srate + Lug) / den
+    bool closed;                    // glottis closed: ugn = 0
+};
+
+__device__ __forceinline__ TmmPrep tmm_prepare(const TmmConsts& k, const TmmState& s) {
     const float srate = k.srate;
     const float two_lg = fmul(2.0f, k.lg);
     float Ag1 = fadd(k.Ag01, fmul(two_lg, s.x1_curr));
@@ -89,14 +100,15 @@ __device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1
     if (det == 0.0f) det = 1.0f;
     const float x1n = fdiv(fsub(fmul(a22, b1), fmul(a12, b2)), det);
     const float x2n = fdiv(fsub(fmul(a11, b2), fmul(a21, b1)), det);
-    s.x1_old = x1; s.x1_curr = x1n;
-    s.x2_old = x2; s.x2_curr = x2n;
+    TmmPrep o;
+    o.x1 = x1; o.x1n = x1n; o.x2 = x2; o.x2n = x2n; o.ug = ug;
+    o.srate = srate; o.ps = k.ps;
     Ag1 = fadd(k.Ag01, fmul(two_lg, x1n));
     Ag2 = fadd(k.Ag02, fmul(two_lg, x2n));
-    float ugn;
-    if (Ag1 < 0.0f || Ag2 < 0.0f) {
-        ugn = 0.0f;
-    } else {
+    o.closed = Ag1 < 0.0f || Ag2 < 0.0f;
+    o.Lug = 0.0f;
+    o.den = 1.0f;
+    if (!o.closed) {
         const float r = fdiv(Ag2, k.A1);
         const float f = fdiv(fsub(1.0f, fmul(fmul(2.0f, r), fsub(1.0f, r))), fmul(Ag2, Ag2));
         const double t1 = dmul(dmul(dd(half_rho), fabs(dd(ug))),
@@ -105,19 +117,37 @@ __device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1
                                              fdiv(k.d2, fmul(fmul(Ag2, Ag2), Ag2))));
         const float Rtot = tof(dadd(t1, dd(t2)));
         const float Ltot = fmul(k.rho, fadd(fdiv(k.d1, Ag1), fdiv(k.d2, Ag2)));
-        ugn = fdiv(fadd(fdiv(fsub(k.ps, p1), srate), fmul(Ltot, ug)), fadd(fdiv(Rtot, srate), Ltot));
+        o.Lug = fmul(Ltot, ug);
+        o.den = fadd(fdiv(Rtot, srate), Ltot);
     }
-    s.ug_old = ug;
+    return o;
+}
+
+__device__ __forceinline__ float tmm_finish(const TmmPrep& o, TmmState& s, float p1) {
+    const float ugn = o.closed ? 0.0f : fdiv(fadd(fdiv(fsub(o.ps, p1), o.srate), o.Lug), o.den);
+    s.x1_old = o.x1; s.x1_curr = o.x1n;
+    s.x2_old = o.x2; s.x2_curr = o.x2n;
+    s.ug_old = o.ug;
     s.ug_curr = ugn;
     return ugn;
+}
+
+__device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1) {
+    const TmmPrep o = tmm_prepare(k, s);
+    return tmm_finish(o, s, p1);
 }
 
 // The same model step with every quantity in double (tmm_f64), following
 // TwoMassModel.cpp:90-232 operation by operation; the caller's pressure is
 // widened and the flow rounded to float for the field update.
-__device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, float p1f) {
+struct TmmPrep64 {
+    double x1, x1n, x2, x2n, ug;
+    double Lug, den, srate, ps;     // ugn = ((ps - p1) / srate + Lug) / den
+    bool closed;
+};
+
+__device__ __forceinline__ TmmPrep64 tmm_prepare64(const TmmConsts64& k, const TmmState64& s) {
     const double srate = k.srate, ss = srate * srate;
-    const double p1 = (double)p1f;
     const double x1c = s.x1_curr, x2c = s.x2_curr, ug = s.ug_curr, ugo = s.ug_old;
     double Ag1 = k.Ag01 + 2 * k.lg * x1c;
     double Ag2 = k.Ag02 + 2 * k.lg * x2c;
@@ -157,23 +187,38 @@ __device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, fl
     if (det == 0) det = 1;
     const double x1n = (a22 * b1 - a12 * b2) / det;
     const double x2n = (a11 * b2 - a21 * b1) / det;
-    s.x1_old = x1c; s.x1_curr = x1n;
-    s.x2_old = x2c; s.x2_curr = x2n;
+    TmmPrep64 o;
+    o.x1 = x1c; o.x1n = x1n; o.x2 = x2c; o.x2n = x2n; o.ug = ug;
+    o.srate = srate; o.ps = k.ps;
     Ag1 = k.Ag01 + 2 * k.lg * x1n;
     Ag2 = k.Ag02 + 2 * k.lg * x2n;
-    double ugn;
-    if (Ag1 < 0 || Ag2 < 0) {
-        ugn = 0;
-    } else {
+    o.closed = Ag1 < 0 || Ag2 < 0;
+    o.Lug = 0;
+    o.den = 1;
+    if (!o.closed) {
         const double Rtot = (k.rho / 2) * fabs(ug) *
                                 ((0.37 / (Ag1 * Ag1)) + (1 - 2 * (Ag2 / k.A1) * (1 - Ag2 / k.A1)) / (Ag2 * Ag2)) +
                             (12 * k.mu * k.lg * k.lg * (k.d1 / (Ag1 * Ag1 * Ag1) + k.d2 / (Ag2 * Ag2 * Ag2)));
         const double Ltot = k.rho * (k.d1 / Ag1 + k.d2 / Ag2);
-        ugn = ((k.ps - p1) / srate + Ltot * ug) / (Rtot / srate + Ltot);
+        o.Lug = Ltot * ug;
+        o.den = Rtot / srate + Ltot;
     }
-    s.ug_old = ug;
+    return o;
+}
+
+__device__ __forceinline__ float tmm_finish64(const TmmPrep64& o, TmmState64& s, float p1f) {
+    const double p1 = (double)p1f;
+    const double ugn = o.closed ? 0.0 : ((o.ps - p1) / o.srate + o.Lug) / o.den;
+    s.x1_old = o.x1; s.x1_curr = o.x1n;
+    s.x2_old = o.x2; s.x2_curr = o.x2n;
+    s.ug_old = o.ug;
     s.ug_curr = ugn;
     return (float)ugn;
+}
+
+__device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, float p1f) {
+    const TmmPrep64 o = tmm_prepare64(k, s);
+    return tmm_finish64(o, s, p1f);
 }
 
 // One two-mass step of tube T from the state of parity par and the pressure

@@ -16,9 +16,10 @@
 //   V' of rows r0 .. r1 (in place); the threads of the first and last row
 //   store their new velocities into the neighbours' ghost rows (distributed
 //   shared memory); the excitation velocity of the next step is prepared
-//   (table value, or the two-mass step on the new pressure, computed by one
+//   (table value, or the two-mass step on the new pressure, finished by one
 //   thread of the CTA that owns the excitation cell and sent to every CTA)
-//   cluster barrier (arrive.release / wait.acquire)
+//   cluster barrier (arrive.release / wait.acquire; the two-mass thread
+//   prepares the state-only part of a later step between the two)
 // Ghost rows and the excitation slot are double-buffered by step parity, so a
 // CTA that runs ahead into the next step never overwrites values a neighbour
 // still reads.  At the end every CTA writes its rows back to the parity set
@@ -160,26 +161,39 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
     const bool tmm = flags & TUBE_TMM, tmm64 = flags & TUBE_TMM64;
     const bool exc_owner = tmm && T->exc_y >= r0 && T->exc_y <= r1;
     const int exc_i = T->exc_y - (r0 - 1), exc_x = T->exc_x;
+    // The two-mass model runs in the last thread of the CTA that owns the
+    // excitation cell (a thread with few or no cells).  Its step is split at
+    // the one use of the pressure (tmm_prepare / tmm_finish): the state-only
+    // part for step n + 2 is computed between this thread's arrival at the
+    // cluster barrier of step n and its wait, beside the other CTAs' work, and
+    // only the last division waits for the new pressure.
+    const bool tmm_thread = exc_owner && tid == nthr - 1;
     TmmState s32{};
     TmmState64 s64{};
-    if (exc_owner && tid == 0) {
+    TmmPrep prep32{};
+    TmmPrep64 prep64{};
+    if (tmm_thread) {
         if (tmm64) s64 = T->tmm64[par0];
         else s32 = T->tmm[par0];
     }
-    auto tmm_next = [&](float p1) -> float {
-        return tmm64 ? tmm_step64(T->tmmd, s64, p1) : tmm_step(T->tmmc, s32, p1);
+    auto tmm_prepare_next = [&]() {
+        if (tmm64) prep64 = tmm_prepare64(T->tmmd, s64);
+        else prep32 = tmm_prepare(T->tmmc, s32);
+    };
+    auto tmm_finish_next = [&](float p1) -> float {
+        return tmm64 ? tmm_finish64(prep64, s64, p1) : tmm_finish(prep32, s32, p1);
     };
     auto send_exe = [&](int slot, float e) {
         for (int q = 0; q < C; ++q) *cluster.map_shared_rank(sExe + slot, q) = e;
     };
     __syncthreads();
     cluster.sync();                                       // every CTA of the cluster is running
-    if (tid == 0) {
-        if (tmm) {
-            if (exc_owner) send_exe(par0, tmm_next(row(L.P, exc_i)[exc_x]));
-        } else {
-            sExe[par0] = n0 < T->src_len ? T->src[n0] : 0.0f;
-        }
+    if (tmm_thread) {
+        tmm_prepare_next();
+        send_exe(par0, tmm_finish_next(row(L.P, exc_i)[exc_x]));
+        tmm_prepare_next();
+    } else if (!tmm && tid == 0) {
+        sExe[par0] = n0 < T->src_len ? T->src[n0] : 0.0f;
     }
     cluster.sync();
 
@@ -233,12 +247,9 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
         }
         __syncthreads();
         // ---- excitation velocity of the next step
-        if (tid == 0 && n + 1 < n_end) {
-            if (tmm) {
-                if (exc_owner) send_exe(q, tmm_next(row(L.P, exc_i)[exc_x]));
-            } else {
-                sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
-            }
+        if (n + 1 < n_end) {
+            if (tmm_thread) send_exe(q, tmm_finish_next(row(L.P, exc_i)[exc_x]));
+            else if (!tmm && tid == 0) sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
         }
         const float exeV = sExe[p];
         // ---- V' of rows r0 .. r1 (FDTDEngineCPU.cpp:364-410)
@@ -290,7 +301,10 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
                 if (i == 1 && up_gVyB) up_gVyB[(size_t)q * pitch + c] = vy;
             }
         }
-        cluster.sync();
+        // cluster barrier, split: the two-mass thread prepares step n + 2 in between
+        asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+        if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
+        asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
     }
 
     // ---- the state of step n_end back to its parity set
@@ -305,7 +319,7 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
             oVx[o] = row(L.Vx, i - 1)[c];
             oVy[o] = row(L.Vy, i - 1)[c];
         }
-    if (exc_owner && tid == 0) {
+    if (tmm_thread) {
         if (tmm64) T->tmm64[pe] = s64;
         else T->tmm[pe] = s32;
     }
