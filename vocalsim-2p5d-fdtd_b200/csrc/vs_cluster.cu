@@ -326,24 +326,383 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
     if (k == 0 && tid == 0) rs->step = n_end;    // every CTA read rs->step before the first cluster barrier
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident form (frames of at most RMAX rows per CTA and 512
+// columns).  Thread t owns column c = t + 1 of its band for the whole run: the
+// P, Vx, Vy of its rows (and of the top ghost row) and every per-cell
+// coefficient (depths, codes or descriptor) live in its registers, with the
+// rows unrolled so the cells of a column are independent instruction
+// streams.  Horizontal neighbours move by warp shuffles; only the two warp-edge
+// values of each row go through shared memory (eUX: Vx dX of the column left of
+// a warp, for its lane 0; eP: P' of the column right of a warp, for its lane
+// 31), and the ghost rows arrive in shared memory as in the first form.  The
+// step sequence, the barriers and the per-cell arithmetic are those of the
+// first form.
+// The two-mass model's state and its prepared step, kept in shared memory by
+// the one thread that runs it, so that the model's registers do not count
+// against every thread's budget (the helpers are not inlined).
+struct TmmSlot {
+    TmmState64 s64;
+    TmmPrep64 prep64;
+    TmmState s32;
+    TmmPrep prep32;
+};
+
+__device__ __noinline__ void tmm_slot_prepare(const TubeDev* __restrict__ T, TmmSlot* slot, bool tmm64) {
+    if (tmm64) slot->prep64 = tmm_prepare64(T->tmmd, slot->s64);
+    else slot->prep32 = tmm_prepare(T->tmmc, slot->s32);
+}
+
+__device__ __noinline__ float tmm_slot_finish(TmmSlot* slot, bool tmm64, float p1) {
+    return tmm64 ? tmm_finish64(slot->prep64, slot->s64, p1) : tmm_finish(slot->prep32, slot->s32, p1);
+}
+
+struct RegLayout {
+    int pitch, nw, rmax;
+    size_t gVx, gVyT, gVyB, dX0, eUX, eP, tab, sig, exe, tmm, bytes;   // byte offsets
+};
+
+__host__ __device__ inline RegLayout reg_layout(int pitch, int nthreads, int rmax, bool fast) {
+    RegLayout L{};
+    L.pitch = pitch;
+    L.nw = nthreads / 32;
+    L.rmax = rmax;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { const size_t at = o; o += (bytes + 15) / 16 * 16; return at; };
+    L.gVx = take(2 * (size_t)pitch * sizeof(float));
+    L.gVyT = take(2 * (size_t)pitch * sizeof(float));
+    L.gVyB = take(2 * (size_t)pitch * sizeof(float));
+    L.dX0 = take((size_t)pitch * sizeof(float));
+    L.eUX = take((size_t)(L.nw + 1) * (rmax + 1) * sizeof(float));
+    L.eP = take((size_t)(L.nw + 1) * (rmax + 1) * sizeof(float));
+    L.tab = take(fast ? 2 * kDescEntries * sizeof(float4) : 0);
+    L.sig = take(16 * sizeof(float));
+    L.exe = take(4 * sizeof(float));
+    L.tmm = take(sizeof(TmmSlot));
+    L.bytes = (o + 127) / 128 * 128;
+    return L;
+}
+
+template <bool FAST, int RMAX, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_t nsteps) {
+    extern __shared__ __align__(16) unsigned char r_smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int k = (int)cluster.block_rank();
+    const TubeDev* __restrict__ T = Tp;
+    const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
+    const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const RegLayout L = reg_layout(pitch, nthr, RMAX, FAST);
+    float* gVx = reinterpret_cast<float*>(r_smem + L.gVx);     // [2][pitch] ghost top Vx
+    float* gVyT = reinterpret_cast<float*>(r_smem + L.gVyT);   // [2][pitch] ghost top Vy
+    float* gVyB = reinterpret_cast<float*>(r_smem + L.gVyB);   // [2][pitch] ghost bottom Vy
+    float* sdX0 = reinterpret_cast<float*>(r_smem + L.dX0);    // dX of the top ghost row
+    float* eUX = reinterpret_cast<float*>(r_smem + L.eUX);     // [nw + 1][RMAX + 1]
+    float* eP = reinterpret_cast<float*>(r_smem + L.eP);       // [nw + 1][RMAX + 1]
+    float4* tabA = reinterpret_cast<float4*>(r_smem + L.tab);
+    float4* tabB = tabA + kDescEntries;
+    float* sSig = reinterpret_cast<float*>(r_smem + L.sig);
+    float* sExe = reinterpret_cast<float*>(r_smem + L.exe);
+
+    const int NR = H - 2;
+    const int r0 = 1 + (int)(((int64_t)k * NR) / C);
+    const int r1 = (int)(((int64_t)(k + 1) * NR) / C);
+    const int Rk = r1 - r0 + 1;                               // 1 .. RMAX
+    const int64_t n0 = rs->step;
+    const int64_t run_start = rs->run_start;
+    float* __restrict__ trace = rs->trace;
+    const int par0 = (int)(n0 & 1);
+    const int64_t pl = T->plane;
+    const float* __restrict__ gP = T->P[0] + par0 * pl;
+    const float* __restrict__ gdP = T->dP;
+    const int c = tid + 1;                                     // this thread's column
+    const bool mine = c <= W - 2;                              // an interior column
+    const int cc = c < pitch ? c : pitch - 1;                  // clamped for the loads
+
+    // ---- state, maps and codes of this column (rows r0-1 .. r1, and r1+1 for Vy / dY)
+    float P[RMAX + 1], VX[RMAX + 1], VY[RMAX + 1], dP[RMAX + 1], dX[RMAX + 1], dY[RMAX + 2];
+    uint32_t cw[RMAX + 1];      // code | right code << 8 | top code << 16 | velocity class << 24 (| desc in FAST: << 8 replaced)
+    uint32_t dsc[RMAX + 1];
+    float vyb = 0.0f;
+#pragma unroll
+    for (int i = 0; i <= RMAX; ++i) {
+        P[i] = VX[i] = VY[i] = 0.0f;
+        dP[i] = dX[i] = 1.0f;
+        dY[i] = 1.0f;
+        cw[i] = VS_CELL_DEAD;
+        dsc[i] = 0;
+        if (i <= Rk) {
+            const int r = r0 - 1 + i;
+            const int64_t o = (int64_t)r * pitch + cc;
+            P[i] = gP[o];
+            VX[i] = gP[2 * pl + o];
+            VY[i] = gP[4 * pl + o];
+            dP[i] = gdP[o];
+            dX[i] = gdP[pl + o];
+            dY[i] = gdP[2 * pl + o];
+            const int kc = T->code[o];
+            const int kr = cc + 1 < pitch ? T->code[o + 1] : VS_CELL_DEAD;
+            const int kt = r >= 1 ? T->code[o - pitch] : VS_CELL_DEAD;
+            cw[i] = (uint32_t)kc | ((uint32_t)kr << 8) | ((uint32_t)kt << 16) |
+                    ((uint32_t)velocity_class(kc, kr, kt) << 24);
+            if (FAST) dsc[i] = T->desc[o];
+        }
+    }
+    dY[RMAX + 1] = 1.0f;
+    {
+        const int64_t o = (int64_t)(r0 + Rk) * pitch + cc;   // row r1 + 1
+#pragma unroll
+        for (int i = 1; i <= RMAX + 1; ++i)
+            if (i == Rk + 1) dY[i] = gdP[2 * pl + o];
+        vyb = gP[4 * pl + o];
+    }
+    // ghost slots, edge buffers, tables
+    for (int x = tid; x < pitch; x += nthr) {
+        const int64_t o = (int64_t)(r0 - 1) * pitch + x;
+        gVx[par0 * pitch + x] = gP[2 * pl + o];
+        gVyT[par0 * pitch + x] = gP[4 * pl + o];
+        gVx[(par0 ^ 1) * pitch + x] = 0.0f;
+        gVyT[(par0 ^ 1) * pitch + x] = 0.0f;
+        const int64_t ob = (int64_t)(r0 + Rk) * pitch + x;
+        gVyB[par0 * pitch + x] = gP[4 * pl + ob];
+        gVyB[(par0 ^ 1) * pitch + x] = 0.0f;
+        sdX0[x] = gdP[pl + o];
+    }
+    for (int j = tid; j < (L.nw + 1) * (RMAX + 1); j += nthr) {
+        eUX[j] = 0.0f;
+        eP[j] = 0.0f;
+    }
+    if (FAST)
+        for (int j = tid; j < 2 * kDescEntries; j += nthr) tabA[j] = T->desc_a[j];
+    if (tid < 16) sSig[tid] = tid < 13 ? T->sigma[tid] : 0.0f;
+    __syncthreads();
+    // left-edge values of every warp for the first step (lane 31 of the warp before)
+    if (lane == 31 && warp + 1 <= L.nw) {
+#pragma unroll
+        for (int i = 1; i <= RMAX; ++i)
+            if (i <= Rk) eUX[(warp + 1) * (RMAX + 1) + i] = fmul(VX[i], dX[i]);
+    }
+
+    const bool tmm = flags & TUBE_TMM, tmm64 = flags & TUBE_TMM64;
+    const bool exc_owner = tmm && T->exc_y >= r0 && T->exc_y <= r1;
+    const int exc_i = T->exc_y - (r0 - 1), exc_x = T->exc_x;
+    const bool tmm_thread = exc_owner && tid == nthr - 1;
+    // the excitation cell's column owner publishes its P' for the two-mass thread
+    float* sPexc = sExe + 2;
+    TmmSlot* slot = reinterpret_cast<TmmSlot*>(r_smem + L.tmm);
+    if (tmm_thread) {
+        if (tmm64) slot->s64 = T->tmm64[par0];
+        else slot->s32 = T->tmm[par0];
+    }
+    auto tmm_prepare_next = [&]() { tmm_slot_prepare(T, slot, tmm64); };
+    auto tmm_finish_next = [&](float p1) -> float { return tmm_slot_finish(slot, tmm64, p1); };
+    auto send_exe = [&](int slot, float e) {
+        for (int q = 0; q < C; ++q) *cluster.map_shared_rank(sExe + slot, q) = e;
+    };
+    // P at the excitation cell, from its column owner
+    auto publish_pexc = [&]() {
+        if (exc_owner && c == exc_x) {
+#pragma unroll
+            for (int i = 1; i <= RMAX; ++i)
+                if (i == exc_i) *sPexc = P[i];
+        }
+    };
+    publish_pexc();
+    __syncthreads();
+    cluster.sync();
+    if (tmm_thread) {
+        tmm_prepare_next();
+        send_exe(par0, tmm_finish_next(*sPexc));
+        tmm_prepare_next();
+    } else if (!tmm && tid == 0) {
+        sExe[par0] = n0 < T->src_len ? T->src[n0] : 0.0f;
+    }
+    cluster.sync();
+
+    float* up_gVyB = k > 0 ? cluster.map_shared_rank(gVyB, k - 1) : nullptr;
+    float* dn_gVx = k + 1 < C ? cluster.map_shared_rank(gVx, k + 1) : nullptr;
+    float* dn_gVyT = k + 1 < C ? cluster.map_shared_rank(gVyT, k + 1) : nullptr;
+
+    const float K1 = T->K1, bco = T->bcoef;
+    const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
+    const float zval = T->zinv, dir0 = T->dir0, dir1 = T->dir1, dir2 = T->dir2, dir3 = T->dir3;
+    const int lis_y = T->lis_y, lis_x = T->lis_x;
+    const int lis_i = (lis_y >= r0 && lis_y <= r1 && c == lis_x) ? lis_y - (r0 - 1) : -1;
+    const int64_t n_end = n0 + nsteps;
+    const int ifirst = r0 == 1 ? 1 : 0;          // the ring row above the first band is never computed
+    constexpr unsigned kAll = 0xffffffffu;
+
+    for (int64_t n = n0; n < n_end; ++n) {
+        const int p = (int)(n & 1), q = p ^ 1;
+        // ghost values of this step
+        VX[0] = gVx[p * pitch + cc];
+        VY[0] = gVyT[p * pitch + cc];
+        vyb = gVyB[p * pitch + cc];
+        const float uxl_ghost = c - 1 >= 0 ? fmul(gVx[p * pitch + c - 1], sdX0[c - 1]) : 0.0f;
+        // ---- P' of rows r0-1 .. r1 (FDTDEngineCPU.cpp:316-339)
+#pragma unroll
+        for (int i = 0; i <= RMAX; ++i) {
+            if (i > Rk) break;
+            const float ux = fmul(VX[i], dX[i]);
+            float uxl = __shfl_up_sync(kAll, ux, 1);
+            if (i == 0) uxl = uxl_ghost;
+            else if (lane == 0) uxl = eUX[warp * (RMAX + 1) + i];
+            const float vyd = i == Rk ? vyb : VY[i + 1 <= RMAX ? i + 1 : RMAX];
+            const float uy = fmul(VY[i], dY[i]), uyb = fmul(vyd, dY[i + 1]);
+            float pn;
+            if constexpr (FAST) {
+                const float ks = fmul(K1, fadd(fsub(ux, uxl), fsub(uy, uyb)));
+                pn = __fmaf_rn(-ks, rcp_approx(dP[i]), P[i]);
+                if (dsc[i]) pn = fmul(pn, tabA[dsc[i]].z);
+            } else {
+                const float num = fsub(fmul(P[i], dP[i]), fmul(K1, fadd(fsub(ux, uxl), fsub(uy, uyb))));
+                const int tc = cw[i] & CODE_TYPE_MASK;
+                float den = dP[i];
+                if (tc != VS_CELL_AIR) {
+                    const float sg = sSig[tc];
+                    den = eigen ? fadd(fmul(sg, dP[i]), dP[i]) : fmul(fadd(1.0f, sg), dP[i]);
+                }
+                pn = fdiv_z(num, den);
+                if (dirichlet && tc == VS_CELL_NOPRESSURE) pn = 0.0f;
+            }
+            if (mine && !(i == 0 && ifirst == 1)) P[i] = pn;
+            if (i == lis_i && i >= 1) store_trace(rs, trace + (n - run_start), pn);
+            if (lane == 0 && i >= 1) eP[warp * (RMAX + 1) + i] = P[i];
+        }
+        publish_pexc();
+        __syncthreads();
+        if (n + 1 < n_end) {
+            if (tmm_thread) send_exe(q, tmm_finish_next(*sPexc));
+            else if (!tmm && tid == 0) sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+        }
+        const float exeV = sExe[p];
+        // ---- V' of rows r0 .. r1 (FDTDEngineCPU.cpp:364-410)
+#pragma unroll
+        for (int i = 1; i <= RMAX; ++i) {
+            if (i > Rk) break;
+            float pr = __shfl_down_sync(kAll, P[i], 1);
+            if (lane == 31) pr = eP[(warp + 1) * (RMAX + 1) + i];
+            if (c + 1 > W - 2) pr = 0.0f;                    // the ring column
+            const float pc = P[i], pt = P[i - 1];
+            float vx = VX[i], vy = VY[i];
+            const uint32_t w = cw[i];
+            const int cls = (int)(w >> 24);
+            if constexpr (FAST) {
+                vx = fsub(vx, fmul(bco, fsub(pr, pc)));
+                vy = fsub(vy, fmul(bco, fsub(pt, pc)));
+                const int d = (int)dsc[i];
+                if (d) {
+                    const float4 da = tabA[d];
+                    vx = fmul(vx, da.x);
+                    vy = fmul(vy, da.y);
+                    if (cls == V_GENERIC) {
+                        const float4 db = tabB[d];
+                        vx = __fmaf_rn(da.w, exeV, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pc, vx)));
+                        vy = __fmaf_rn(-db.w, pt, __fmaf_rn(db.z, pc, vy));
+                    }
+                }
+            } else if (cls == V_GENERIC) {
+                const VelocityOut v = velocity_generic((int)(w & 0xff), (int)((w >> 8) & 0xff), (int)((w >> 16) & 0xff),
+                                                       pc, pr, pt, vx, vy, exeV, sSig, zval, bco, dir0, dir1, dir2, dir3);
+                vx = v.vx;
+                vy = v.vy;
+            } else {
+                vx = fsub(vx, fmul(bco, fsub(pr, pc)));
+                vy = fsub(vy, fmul(bco, fsub(pt, pc)));
+                if (cls == V_BETA1) {
+                    const float sc = sSig[w & CODE_TYPE_MASK];
+                    vx = fdiv_z(vx, fadd(1.0f, fmaxf(sc, sSig[(w >> 8) & CODE_TYPE_MASK])));
+                    vy = fdiv_z(vy, fadd(1.0f, fmaxf(sc, sSig[(w >> 16) & CODE_TYPE_MASK])));
+                }
+            }
+            if (mine) {
+                VX[i] = vx;
+                VY[i] = vy;
+                if (i == Rk && dn_gVx) {
+                    dn_gVx[(size_t)q * pitch + c] = vx;
+                    dn_gVyT[(size_t)q * pitch + c] = vy;
+                }
+                if (i == 1 && up_gVyB) up_gVyB[(size_t)q * pitch + c] = vy;
+            }
+            if (lane == 31) eUX[(warp + 1) * (RMAX + 1) + i] = fmul(VX[i], dX[i]);
+        }
+        asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+        if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
+        asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
+    }
+
+    // ---- the state of step n_end back to its parity set
+    const int pe = (int)(n_end & 1);
+    float* __restrict__ oP = T->P[0] + pe * pl;
+    if (mine) {
+#pragma unroll
+        for (int i = 1; i <= RMAX; ++i) {
+            if (i > Rk) break;
+            const int64_t o = (int64_t)(r0 - 1 + i) * pitch + c;
+            oP[o] = P[i];
+            oP[2 * pl + o] = VX[i];
+            oP[4 * pl + o] = VY[i];
+        }
+    }
+    if (tmm_thread) {
+        if (tmm64) T->tmm64[pe] = slot->s64;
+        else T->tmm[pe] = slot->s32;
+    }
+    if (k == 0 && tid == 0) rs->step = n_end;
+}
+
 }  // namespace
 
 size_t cluster_smem_bytes(int pitch, int rows_max, bool fast) { return cluster_layout(pitch, rows_max, fast).bytes; }
 
 // Cluster size, threads and shared memory for one tube of H x W (pitch), or
 // false when no cluster of at least 4 CTAs fits on this device.
+namespace {
+
+// The register form is compiled for at most 4 or 8 rows per band and 256 or
+// 512 threads per CTA (a thread per column; 256 threads leave 255 registers
+// per thread).
+template <bool FAST>
+const void* reg_fn(int rmax, int threads) {
+    if (rmax <= 4) return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 4, 256>
+                                         : (const void*)cluster_reg_kernel<FAST, 4, 512>;
+    return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 8, 256> : (const void*)cluster_reg_kernel<FAST, 8, 512>;
+}
+
+const void* cluster_fn(bool fast, int form, int rmax, int threads) {
+    if (form == 0) return fast ? (const void*)cluster_kernel<true> : (const void*)cluster_kernel<false>;
+    return fast ? reg_fn<true>(rmax, threads) : reg_fn<false>(rmax, threads);
+}
+
+template <bool FAST>
+cudaError_t launch_reg(const cudaLaunchConfig_t& cfg, int rmax, int threads, const TubeDev* tube, RunState* rs,
+                       int64_t steps) {
+    if (rmax <= 4)
+        return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 256>, tube, rs, steps)
+                              : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 512>, tube, rs, steps);
+    return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 256>, tube, rs, steps)
+                          : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 512>, tube, rs, steps);
+}
+
+}  // namespace
+
 bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out) {
     const int NR = H - 2;
     if (NR < 4) return false;
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
-    const void* fn = fast ? (const void*)cluster_kernel<true> : (const void*)cluster_kernel<false>;
     const int threads = std::min(512, (W + 31) / 32 * 32);
     for (int C : {16, 8, 4}) {
         if (C > NR) continue;
         const int R = (NR + C - 1) / C;
-        const size_t smem = cluster_layout(pitch, R, fast).bytes;
+        // the register-resident form where a band has at most 8 rows and a
+        // thread per column fits a CTA, the shared-memory form otherwise
+        const int form = (R <= 8 && W <= 512) ? 1 : 0;
+        const int rmax = R <= 4 ? 4 : 8;
+        const void* fn = cluster_fn(fast, form, rmax, threads);
+        const size_t smem = form ? reg_layout(pitch, threads, rmax, fast).bytes : cluster_layout(pitch, R, fast).bytes;
         if (smem > (size_t)optin) continue;
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) continue;
         if (C > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
@@ -368,6 +727,8 @@ bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out) {
         out->threads = threads;
         out->rows_max = R;
         out->smem = smem;
+        out->form = form;
+        out->rmax = rmax;
         return true;
     }
     cudaGetLastError();
@@ -389,6 +750,9 @@ cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps,
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (c.form == 1)
+        return fast ? launch_reg<true>(cfg, c.rmax, c.threads, tube, rs, steps)
+                    : launch_reg<false>(cfg, c.rmax, c.threads, tube, rs, steps);
     if (fast) return cudaLaunchKernelEx(&cfg, cluster_kernel<true>, tube, rs, steps, c.rows_max);
     return cudaLaunchKernelEx(&cfg, cluster_kernel<false>, tube, rs, steps, c.rows_max);
 }

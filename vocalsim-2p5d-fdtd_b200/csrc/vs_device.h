@@ -180,6 +180,8 @@ int cluster_shape();
 struct ClusterConfig {
     int ctas = 0, threads = 0, rows_max = 0;
     size_t smem = 0;
+    int form = 0;         // 0: band in shared memory; 1: register-resident columns (rows_max <= rmax)
+    int rmax = 0;
 };
 // Cluster size (16, 8 or 4 CTAs), threads and shared memory for a tube of
 // H x W cells (row pitch `pitch`) on the current device, or false when none

@@ -38,6 +38,7 @@ import numpy as np
 import torch
 
 from .autograd import SectionTrace, log_power_spectrum, tube_layout
+from .abi import VS_ERR_NONFINITE, VsError
 from .solver import Batch, Geometry, params
 
 
@@ -164,7 +165,12 @@ def synthetic_problem(n_tubes: int, srate_mul: int, steps: int, seed0: int = 0, 
         gs = [Geometry(*S.batch_tube(s)[:2]) for s in cand] + [Geometry(*S.batch_target_tube(s)[:2]) for s in cand]
         b = Batch(ps, gs)
         tr = torch.zeros((2 * len(cand), steps), dtype=torch.float32, device="cuda")
-        b.run_device(steps, tr.data_ptr())
+        try:
+            b.run_device(steps, tr.data_ptr())
+        except VsError as e:
+            # unstable candidates are expected here; their traces are screened below
+            if e.status != VS_ERR_NONFINITE:
+                raise
         torch.cuda.synchronize()
         b.close()
         ok = torch.isfinite(tr).all(dim=1).cpu().numpy()
