@@ -250,10 +250,20 @@ int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
 int vs_batch_adjoint_times(const vs_batch* b, float* recompute_ms, float* reverse_ms);
 
 /* Kernel form of the reverse steps of vs_batch_adjoint, no counterpart in the
- * reference: 0 = row-marching warp strips with four columns per lane (the
- * default), 1 = 32 x 8 tiles with mu in shared memory.  Both compute the same
- * transposed step; they differ only in float rounding. */
+ * reference: 0 = automatic (the default): form 2 for a batch of table-source
+ * tubes large enough to give every SM four strips, else form 1;
+ * 1 = 32 x 8 tiles with mu in shared memory, one reverse step per launch;
+ * 2 = row-marching warp strips (two columns per lane) running two reverse
+ * steps per launch, which reads and writes the adjoint planes and the
+ * gradient accumulators once per two steps; a batch with a two-mass tube
+ * runs it as form 3 (the two-mass reverse step runs beside every step);
+ * 3 = the same strips, one reverse step per launch.  All forms compute the
+ * same transposed step; they differ only in float rounding. */
 int vs_batch_set_adjoint_form(vs_batch* b, int32_t form);
+
+/* Rows per warp strip of the strip forms: 4, 8 or 16, or 0 (the default: 8
+ * for form 2, 4 for form 3).  No counterpart in the reference. */
+int vs_batch_set_adjoint_rows(vs_batch* b, int32_t rows);
 
 /* Failure-path hook, no counterpart in the reference: the number of polls a
  * kernel's wait for its bulk row copies (band and staged quad-strip shapes)

@@ -202,13 +202,13 @@ __device__ void tmm_reverse(const TubeDev& T, const AdjTube& A, const float* __r
 // the block holding the excitation point also runs the two-mass reverse step.
 __global__ void __launch_bounds__(kAdjTileW * kAdjTileH, 3)
 adjoint_step_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
-                    const AdjRun* __restrict__ run, int local) {
+                    const AdjRun* __restrict__ run, int local, int phase) {
     const TubeDev& T = tubes[blockIdx.y];
     const AdjTube& A = adj[blockIdx.y];
     const AdjRun ar = *run;
     const int64_t n = ar.start + ar.len - 1 - local;
     const int64_t slot = n - ar.start;
-    const int par = ar.q0 ^ (local & 1);
+    const int par = ar.q0 ^ (phase & 1);
     if ((int)blockIdx.x >= A.tiles) {
         // the block after the last tile reverses the two-mass step
         if ((int)blockIdx.x == A.tiles && (T.flags & TUBE_TMM) && threadIdx.x < 32)
@@ -358,13 +358,13 @@ __device__ __forceinline__ int byte_at(uint32_t k, int q) { return (int)((k >> (
 template <int NC, int TR, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
 adjoint_strip_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
-                     const AdjRun* __restrict__ run, int local) {
+                     const AdjRun* __restrict__ run, int local, int phase) {
     const TubeDev& T = tubes[blockIdx.y];
     const AdjTube& A = adj[blockIdx.y];
     const AdjRun ar = *run;
     const int64_t n = ar.start + ar.len - 1 - local;
     const int64_t slot = n - ar.start;
-    const int par = ar.q0 ^ (local & 1);
+    const int par = ar.q0 ^ (phase & 1);
     const int nblk = (A.strips + WARPS - 1) / WARPS;
     if ((int)blockIdx.x >= nblk) {
         // the block after the last strip block reverses the two-mass step
@@ -450,7 +450,7 @@ adjoint_strip_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restric
         // ---- mu and q of row r
         const unsigned rowm = r >= 1 ? inter : 0u;
         float4 eb[NC];
-        float mu[NC], qc[NC], bxl[NC], ux[NC];
+        float mu[NC], qc[NC], bxl[NC], ux[NC], rD[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
             const float4 ea = __ldg(tab + 3 * byte_at(d_c, q));
@@ -468,7 +468,8 @@ adjoint_strip_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restric
             if (r == lis_y && q == lis_q) mu[q] += glis;
             if (tmm && r == exc_y && q == exc_q) mu[q] += pend;
             if (!((rowm >> q) & 1u) || eb[q].w != 0.0f) mu[q] = 0.0f;   // ring / Dirichlet no-pressure
-            qc[q] = mu[q] == 0.0f ? 0.0f : __fdividef(mu[q], eb[q].z * dp[q]);
+            rD[q] = __fdividef(1.0f, eb[q].z * dp[q]);               // 1 / D
+            qc[q] = mu[q] == 0.0f ? 0.0f : mu[q] * rD[q];
         }
         // ---- commit row r (FDTDEngineCPU.cpp:316-410 transposed)
         if (j >= 1) {
@@ -486,7 +487,7 @@ adjoint_strip_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restric
                 oY[q] = eb[q].y * lY[q] + dy[q] * lamW;
                 const float uxl = q > 0 ? ux[q - 1] : ux_in;
                 const float S = (ux[q] - uxl) + (vy[q] * dy[q] - vyn[q] * dyn[q]);
-                tP[q] = mu[q] != 0.0f ? qc[q] * K1 * S / dp[q] : 0.0f;
+                tP[q] = mu[q] != 0.0f ? qc[q] * K1 * S * (rD[q] * eb[q].z) : 0.0f;   // / dP
                 tX[q] = vx[q] * lamU;
                 tY[q] = vy[q] * lamW;
             }
@@ -524,7 +525,361 @@ adjoint_strip_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restric
     }
 }
 
-constexpr int kAdjNC = 2, kAdjTR = 16, kAdjWarps = 4;
+// ---------------------------------------------------------------------------
+// Two reverse steps per launch in strip form (table sources only).  The warp
+// geometry is that of the one-step strips (NC columns per lane, lanes 1..30
+// commit, strips of TR rows); the warp marches rows r = r0-2 .. rlast+1 and,
+// at row r, runs
+//   stage 0 (step n):      mu, q of row r from lambda' (the launch's input),
+//                          then lambda^n of row r (kept in registers);
+//   stage 1 (step n - 1):  mu, q of row r-1 from lambda^n of rows r-1 and r,
+//                          then lambda^(n-1) of row r-1, which is stored.
+// The valid region shrinks by one column on each side and one row per stage,
+// which the extra rows (two above the strip, one below) and the halo lanes
+// (0 and 31) absorb; those are recomputed by the neighbouring strips, so
+// lambda^n is never written or read back.  The gradient terms of both steps
+// at a cell go to its double accumulators in one read-modify-write (stage
+// 0's terms of row r wait one iteration in registers for stage 1's).
+// Per cell and step the arithmetic is that of the one-step strip kernel.
+//
+// Row supply: each lane streams its own NC-column pieces of the ten float
+// plane rows an iteration reads (lambda' P, X, Y; dP, dX, dY; Vx, Vy before
+// step n; Vx, Vy before step n-1) and of the three double gradient rows it
+// updates into a per-warp ring of kAdjDepth + 1 shared-memory stages with
+// cp.async, kAdjDepth rows ahead of their use; out-of-frame pieces are
+// zero-filled by the copy.  A lane reads back only what it copied, after
+// cp.async.wait_group, so no barrier is involved.  A stage is refilled one
+// iteration after its values were last read.  Each gradient cell is updated
+// once per launch, so its prefetched old value is current.
+constexpr int kAdjDepth = 2;          // rows in flight per warp
+constexpr int kAdjPieces = 10;        // float plane-row pieces per stage
+constexpr int kAdjGPieces = 3;        // double gradient-row pieces per stage
+
+// One piece of BYTES (4, 8 or 16) into shared memory; src and dst aligned to BYTES.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_piece(void* dst, const void* src, bool ok, const void* dummy) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const void* s = ok ? src : dummy;         // a valid address; nothing is read when ok is false
+    const int n = ok ? BYTES : 0;             // 0 source bytes: the piece is zero-filled
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(s), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(s), "n"(BYTES), "r"(n)
+                     : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int NC>
+__device__ __forceinline__ void ldsrow(float (&d)[NC], const float* p) {
+    if constexpr (NC == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        d[0] = t.x; d[1] = t.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < NC; ++q) d[q] = p[q];
+    }
+}
+
+template <int NC, int TR, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 3)
+adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ adj,
+                const AdjRun* __restrict__ run, int local, int phase) {
+    extern __shared__ float4 adj2_smem[];
+    const TubeDev& T = tubes[blockIdx.y];
+    const AdjTube& A = adj[blockIdx.y];
+    const AdjRun ar = *run;
+    const int64_t n = ar.start + ar.len - 1 - local;    // stage 0 reverses step n, stage 1 step n - 1
+    const int64_t slot = n - ar.start;                  // >= 1
+    const int par = ar.q0 ^ (phase & 1);
+    const int s = (int)blockIdx.x * WARPS + (int)(threadIdx.x >> 5);
+    if (s >= A.strips) return;
+    constexpr unsigned kAll = 0xffffffffu;
+    constexpr int kCommit = 30 * NC;
+    constexpr int kSlots = kAdjDepth + 1;
+    const int lane = threadIdx.x & 31;
+    const int W = T.W, H = T.H, pitch = T.pitch;
+    const int nsx = (W - 2) / kCommit + 1;
+    const int c0 = kCommit * (s % nsx) - NC;
+    const int r0 = 1 + (s / nsx) * TR;
+    const int rlast = min(r0 + TR - 1, H - 2);
+    const int x0 = c0 + NC * lane;
+    const bool ok = x0 >= 0 && x0 < pitch;
+    unsigned inter = 0, commit = 0;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const int x = x0 + q;
+        const bool in = x >= 1 && x <= W - 2;
+        inter |= (unsigned)in << q;
+        commit |= (unsigned)(in && lane >= 1 && lane <= 30) << q;
+    }
+    const int pl = (int)T.plane;                             // plane offsets fit in 32 bits
+    const float* __restrict__ lam = A.lam[par];
+    float* __restrict__ lout = A.lam[par ^ 1];
+    const float* __restrict__ hn = T.hist + slot * 3 * T.plane;   // state before step n (P, Vx, Vy)
+    const float* __restrict__ hm = hn - 3 * pl;              // state before step n - 1
+    const float* __restrict__ pn = hn + 3 * pl;              // P after step n (P after n - 1 = hn)
+    const float* __restrict__ mP = T.dP;
+    const uint8_t* __restrict__ dsc = A.desc;
+    const uint8_t* __restrict__ code = T.code;
+    const float4* __restrict__ tab = A.tab;
+    const float K1 = T.K1;
+    const int lis_y = T.lis_y, lis_q = T.lis_x - x0;
+    const bool lis_col = lis_q >= 0 && lis_q < NC;
+    const float g0 = (lis_col && lis_y >= r0 - 2 && lis_y <= rlast + 1) ? __ldg(A.gtrace + n) : 0.0f;
+    const float g1 = (lis_col && lis_y >= r0 - 1 && lis_y <= rlast) ? __ldg(A.gtrace + n - 1) : 0.0f;
+    auto rv = [&](int rr) { return ok && rr >= 0 && rr <= H - 1; };
+    // stage t holds the pieces of row j = r0 - 2 + t: lambda' P(j), X(j), Y(j+1), dP(j), dX(j),
+    // dY(j+1), Vx_n(j), Vy_n(j+1), Vx_(n-1)(j-1), Vy_(n-1)(j) as floats, then gP, gX, gY of
+    // row j-1 (the row stage 1 commits at iteration j) as doubles; this lane's float piece k
+    // sits at stage + (k * 32 + lane) * NC, its double piece k at gstage + (k * 32 + lane) * NC
+    constexpr int kStage = (kAdjPieces + 2 * kAdjGPieces) * 32 * NC;   // floats per stage
+    float* ring = reinterpret_cast<float*>(adj2_smem) + (threadIdx.x >> 5) * (kSlots * kStage);
+    const int t_last = rlast - r0 + 3;                       // stage of row rlast + 1
+    auto issue = [&](int t) {
+        if (t > t_last) {                                    // past the strip: keep the group count
+            cp_async_commit();
+            return;
+        }
+        float* d = ring + (t % kSlots) * kStage + lane * NC;
+        double* g = reinterpret_cast<double*>(ring + (t % kSlots) * kStage + kAdjPieces * 32 * NC) + lane * NC;
+        const int j = r0 - 2 + t;
+        const int o = j * pitch + x0;
+        const bool a = rv(j), b = rv(j + 1), c = rv(j - 1);
+        const bool gc = commit && j - 1 >= r0 && j - 1 <= rlast;
+        constexpr int B = 4 * NC;
+        cp_async_piece<B>(d + 0 * 32 * NC, lam + o, a, lam);
+        cp_async_piece<B>(d + 1 * 32 * NC, lam + pl + o, a, lam);
+        cp_async_piece<B>(d + 2 * 32 * NC, lam + 2 * pl + o + pitch, b, lam);
+        cp_async_piece<B>(d + 3 * 32 * NC, mP + o, a, lam);
+        cp_async_piece<B>(d + 4 * 32 * NC, mP + pl + o, a, lam);
+        cp_async_piece<B>(d + 5 * 32 * NC, mP + 2 * pl + o + pitch, b, lam);
+        cp_async_piece<B>(d + 6 * 32 * NC, hn + pl + o, a, lam);
+        cp_async_piece<B>(d + 7 * 32 * NC, hn + 2 * pl + o + pitch, b, lam);
+        cp_async_piece<B>(d + 8 * 32 * NC, hm + pl + o - pitch, c, lam);
+        cp_async_piece<B>(d + 9 * 32 * NC, hm + 2 * pl + o, a, lam);
+        cp_async_piece<2 * B>(g + 0 * 32 * NC, A.gP + (o - pitch), gc, A.gP);
+        cp_async_piece<2 * B>(g + 1 * 32 * NC, A.gX + (o - pitch), gc, A.gP);
+        cp_async_piece<2 * B>(g + 2 * 32 * NC, A.gY + (o - pitch), gc, A.gP);
+        cp_async_commit();
+    };
+
+    // rows held at iteration r (u = r-1, c = r, d = r+1)
+    float lPc[NC], lXc[NC], lYc[NC], lYd[NC];            // lambda' rows r (P, X, Y), r+1 (Y)
+    float dpu[NC], dpc[NC], dxu[NC], dxc[NC];            // dP, dX rows r-1, r
+    float dyu[NC], dyc[NC], dyd[NC];                     // dY rows r-1, r, r+1
+    float vxc[NC], vyc[NC], vyd[NC];                     // step n state: Vx row r, Vy rows r, r+1
+    float wxu[NC], wyu[NC], wyc[NC];                     // step n-1 state: Vx row r-1, Vy rows r-1, r
+    uint32_t du = 0, dc = 0, dd = 0;                     // descriptors rows r-1, r, r+1
+    uint32_t ku = 0, kc = 0;                             // cell codes rows r-1, r
+    float LPp[NC], LXp[NC], LYp[NC];                     // lambda^n of row r-1
+    float qa0[NC], qa1[NC];                              // q of step n at row r-1, of step n-1 at row r-2
+    float h0P[NC], h0X[NC], h0Y[NC];                     // step n's gradient terms of row r-1
+    double h0Z[NC];                                      // and its z_inv term there
+    {
+        const int r = r0 - 2;
+        const int o = r * pitch + x0;
+        const bool a = rv(r), b = rv(r + 1);
+        ldrow<NC>(lPc, lam + o, a);
+        ldrow<NC>(lXc, lam + pl + o, a);
+        ldrow<NC>(lYc, lam + 2 * pl + o, a);
+        ldrow<NC>(lYd, lam + 2 * pl + o + pitch, b);
+        ldrow<NC>(dpc, mP + o, a);
+        ldrow<NC>(dxc, mP + pl + o, a);
+        ldrow<NC>(dyc, mP + 2 * pl + o, a);
+        ldrow<NC>(dyd, mP + 2 * pl + o + pitch, b);
+        ldrow<NC>(vxc, hn + pl + o, a);
+        ldrow<NC>(vyc, hn + 2 * pl + o, a);
+        ldrow<NC>(vyd, hn + 2 * pl + o + pitch, b);
+        ldrow<NC>(wyc, hm + 2 * pl + o, a);
+        dc = ldbytes<NC>(dsc + o, a);
+        dd = ldbytes<NC>(dsc + o + pitch, b);
+        kc = ldbytes<NC>(code + o, a);
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            dpu[q] = 1.0f; dxu[q] = 0.0f; dyu[q] = 0.0f; wxu[q] = 0.0f; wyu[q] = 0.0f;
+            LPp[q] = 0.0f; LXp[q] = 0.0f; LYp[q] = 0.0f;
+            qa0[q] = 0.0f; qa1[q] = 0.0f; h0P[q] = 0.0f; h0X[q] = 0.0f; h0Y[q] = 0.0f; h0Z[q] = 0.0;
+        }
+    }
+#pragma unroll
+    for (int t = 1; t < kAdjDepth; ++t) issue(t);
+
+    for (int r = r0 - 2; r <= rlast + 1; ++r) {
+        const int tr = r - (r0 - 2);
+        issue(tr + kAdjDepth);            // into the stage moved to registers two iterations ago
+        const int o = r * pitch + x0;
+        const bool nx = r + 1 <= rlast + 1;
+        const uint32_t d2 = ldbytes<NC>(dsc + o + 2 * pitch, nx && rv(r + 2));
+        const uint32_t k1 = ldbytes<NC>(code + o + pitch, nx && rv(r + 1));
+
+        // ---- stage 0: mu and q of row r (step n)
+        const unsigned m0 = (r >= 1 && r <= H - 2) ? inter : 0u;
+        float4 eb0[NC];
+        float mu0[NC], q0[NC], bxl[NC], ux[NC], rD0[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            const float4 ea = __ldg(tab + 3 * byte_at(dc, q));
+            eb0[q] = __ldg(tab + 3 * byte_at(dc, q) + 1);
+            const float byd = __ldg(tab + 3 * byte_at(dd, q)).w;
+            bxl[q] = ea.z * lXc[q];
+            ux[q] = vxc[q] * dxc[q];
+            mu0[q] = lPc[q] + ea.x * lXc[q] + ea.y * lYc[q] - byd * lYd[q];
+        }
+        {
+            const float bx_in = __shfl_up_sync(kAll, bxl[NC - 1], 1);
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                mu0[q] -= q > 0 ? bxl[q - 1] : bx_in;
+                if (r == lis_y && q == lis_q) mu0[q] += g0;
+                if (!((m0 >> q) & 1u) || eb0[q].w != 0.0f) mu0[q] = 0.0f;   // ring / Dirichlet no-pressure
+                rD0[q] = __fdividef(1.0f, eb0[q].z * dpc[q]);                  // 1 / D
+                q0[q] = mu0[q] == 0.0f ? 0.0f : mu0[q] * rD0[q];
+            }
+        }
+        // ---- stage 0: lambda^n of row r (registers) and step n's gradient terms there
+        float LPn[NC], LXn[NC], LYn[NC], t0P[NC], t0X[NC], t0Y[NC];
+        double t0Z[NC];
+        const bool own0 = r >= r0 && r <= rlast;
+        {
+            const float q_in = __shfl_down_sync(kAll, q0[0], 1);
+            const float ux_in = __shfl_up_sync(kAll, ux[NC - 1], 1);
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                const float qr = q < NC - 1 ? q0[q + 1] : q_in;
+                const float lamU = K1 * (qr - q0[q]);
+                const float lamW = K1 * (qa0[q] - q0[q]);
+                const bool in = (m0 >> q) & 1u;
+                LPn[q] = in ? q0[q] * dpc[q] : 0.0f;
+                LXn[q] = in ? eb0[q].x * lXc[q] + dxc[q] * lamU : 0.0f;
+                LYn[q] = in ? eb0[q].y * lYc[q] + dyc[q] * lamW : 0.0f;
+                const float uxl = q > 0 ? ux[q - 1] : ux_in;
+                const float S = (ux[q] - uxl) + (vyc[q] * dyc[q] - vyd[q] * dyd[q]);
+                t0P[q] = mu0[q] != 0.0f ? q0[q] * K1 * S * (rD0[q] * eb0[q].z) : 0.0f;   // / dP
+                t0X[q] = vxc[q] * lamU;
+                t0Y[q] = vyc[q] * lamW;
+                t0Z[q] = 0.0;
+                if (own0 && ((commit >> q) & 1u) && (byte_at(kc, q) & CODE_ZINV_BIT)) {
+                    const float4 ez = __ldg(tab + 3 * byte_at(dc, q) + 2);
+                    const float pc = pn[o + q], pr = pn[o + q + 1], pt = pn[o + q - pitch];
+                    t0Z[q] = (double)(ez.x * pc - ez.y * pr) * (double)lXc[q] +
+                             (double)(ez.z * pc - ez.w * pt) * (double)lYc[q];
+                }
+            }
+        }
+        // ---- stage 1: mu and q of row r-1 (step n-1) from lambda^n of rows r-1 and r
+        if (r >= r0) {
+            const int r1 = r - 1;
+            const int o1 = o - pitch;
+            const unsigned m1 = (r1 >= 1 && r1 <= H - 2) ? inter : 0u;
+            float4 eb1[NC];
+            float mu1[NC], q1[NC], bxl1[NC], wx[NC], rD1[NC];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                const float4 ea = __ldg(tab + 3 * byte_at(du, q));
+                eb1[q] = __ldg(tab + 3 * byte_at(du, q) + 1);
+                const float byd = __ldg(tab + 3 * byte_at(dc, q)).w;
+                bxl1[q] = ea.z * LXp[q];
+                wx[q] = wxu[q] * dxu[q];
+                mu1[q] = LPp[q] + ea.x * LXp[q] + ea.y * LYp[q] - byd * LYn[q];
+            }
+            const float bx_in = __shfl_up_sync(kAll, bxl1[NC - 1], 1);
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                mu1[q] -= q > 0 ? bxl1[q - 1] : bx_in;
+                if (r1 == lis_y && q == lis_q) mu1[q] += g1;
+                if (!((m1 >> q) & 1u) || eb1[q].w != 0.0f) mu1[q] = 0.0f;
+                rD1[q] = __fdividef(1.0f, eb1[q].z * dpu[q]);
+                q1[q] = mu1[q] == 0.0f ? 0.0f : mu1[q] * rD1[q];
+            }
+            // ---- stage 1: lambda^(n-1) of row r-1 (stored) and the gradient terms of both steps there
+            if (r >= r0 + 1) {
+                const float q_in = __shfl_down_sync(kAll, q1[0], 1);
+                const float wx_in = __shfl_up_sync(kAll, wx[NC - 1], 1);
+                float oP[NC], oX[NC], oY[NC], tP[NC], tX[NC], tY[NC];
+#pragma unroll
+                for (int q = 0; q < NC; ++q) {
+                    const float qr = q < NC - 1 ? q1[q + 1] : q_in;
+                    const float lamU = K1 * (qr - q1[q]);
+                    const float lamW = K1 * (qa1[q] - q1[q]);
+                    oP[q] = q1[q] * dpu[q];
+                    oX[q] = eb1[q].x * LXp[q] + dxu[q] * lamU;
+                    oY[q] = eb1[q].y * LYp[q] + dyu[q] * lamW;
+                    const float wxl = q > 0 ? wx[q - 1] : wx_in;
+                    const float S = (wx[q] - wxl) + (wyu[q] * dyu[q] - wyc[q] * dyc[q]);
+                    tP[q] = mu1[q] != 0.0f ? q1[q] * K1 * S * (rD1[q] * eb1[q].z) : 0.0f;
+                    tX[q] = wxu[q] * lamU;
+                    tY[q] = wyu[q] * lamW;
+                }
+                if (commit) {
+                    // the old gradient values of row r-1 arrived with stage tr
+                    const double* gs = reinterpret_cast<const double*>(ring + (tr % kSlots) * kStage +
+                                                                       kAdjPieces * 32 * NC) + lane * NC;
+#pragma unroll
+                    for (int q = 0; q < NC; ++q) {
+                        if (!((commit >> q) & 1u)) continue;
+                        lout[o1 + q] = oP[q];
+                        lout[pl + o1 + q] = oX[q];
+                        lout[2 * pl + o1 + q] = oY[q];
+                        if (tP[q] != 0.0f || h0P[q] != 0.0f)
+                            A.gP[o1 + q] = gs[q] + ((double)h0P[q] + (double)tP[q]);
+                        A.gX[o1 + q] = gs[32 * NC + q] + ((double)h0X[q] + (double)tX[q]);
+                        A.gY[o1 + q] = gs[64 * NC + q] + ((double)h0Y[q] + (double)tY[q]);
+                        if (byte_at(ku, q) & CODE_ZINV_BIT) {
+                            // P after step n-1 is the P plane of the state before step n;
+                            // both steps' z_inv terms go in with one read-modify-write
+                            const float4 ez = __ldg(tab + 3 * byte_at(du, q) + 2);
+                            const float pc = hn[o1 + q], pr = hn[o1 + q + 1], pt = hn[o1 + q - pitch];
+                            A.gZ[o1 + q] += h0Z[q] + ((double)(ez.x * pc - ez.y * pr) * (double)LXp[q] +
+                                                      (double)(ez.z * pc - ez.w * pt) * (double)LYp[q]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NC; ++q) qa1[q] = q1[q];
+        }
+        if (!nx) break;
+
+        // ---- shift the row pipeline; row r+1's pieces come from its ring stage
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            LPp[q] = LPn[q]; LXp[q] = LXn[q]; LYp[q] = LYn[q];
+            qa0[q] = q0[q];
+            h0P[q] = t0P[q]; h0X[q] = t0X[q]; h0Y[q] = t0Y[q]; h0Z[q] = t0Z[q];
+            lYc[q] = lYd[q];
+            dpu[q] = dpc[q]; dxu[q] = dxc[q];
+            dyu[q] = dyc[q]; dyc[q] = dyd[q];
+            vyc[q] = vyd[q];
+            wyu[q] = wyc[q];
+        }
+        du = dc; dc = dd; dd = d2;
+        ku = kc; kc = k1;
+        cp_async_wait<kAdjDepth - 1>();
+        const float* st = ring + ((tr + 1) % kSlots) * kStage + lane * NC;
+        ldsrow<NC>(lPc, st + 0 * 32 * NC);
+        ldsrow<NC>(lXc, st + 1 * 32 * NC);
+        ldsrow<NC>(lYd, st + 2 * 32 * NC);
+        ldsrow<NC>(dpc, st + 3 * 32 * NC);
+        ldsrow<NC>(dxc, st + 4 * 32 * NC);
+        ldsrow<NC>(dyd, st + 5 * 32 * NC);
+        ldsrow<NC>(vxc, st + 6 * 32 * NC);
+        ldsrow<NC>(vyd, st + 7 * 32 * NC);
+        ldsrow<NC>(wxu, st + 8 * 32 * NC);
+        ldsrow<NC>(wyc, st + 9 * 32 * NC);
+    }
+    cp_async_wait<0>();                   // no copy outlives the warp
+}
+
+// Dynamic shared memory of adjoint2_kernel per block.
+constexpr size_t adj2_smem_bytes(int nc, int warps) {
+    return (size_t)warps * (kAdjDepth + 1) * (kAdjPieces + 2 * kAdjGPieces) * 32 * nc * sizeof(float);
+}
+
+constexpr int kAdjNC = 2, kAdjWarps = 4;
 
 // Slot 0 of every tube's history = the state before the first step of a
 // segment (P, Vx, Vy of parity par).
@@ -559,16 +914,36 @@ cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_
 }
 
 cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_blocks,
-                                const AdjRun* run, int local, cudaStream_t stream, int form) {
+                                const AdjRun* run, int local, int phase, cudaStream_t stream, int form,
+                                int rows) {
     const dim3 grid(max_blocks, ntubes);
-    if (form == ADJ_FORM_TILES)
-        adjoint_step_kernel<<<grid, kAdjTileW * kAdjTileH, 0, stream>>>(tubes, adj, run, local);
-    else
-        adjoint_strip_kernel<kAdjNC, kAdjTR, kAdjWarps><<<grid, kAdjWarps * 32, 0, stream>>>(tubes, adj, run, local);
+    constexpr int kThreads = kAdjWarps * 32;
+    constexpr size_t kSmem2 = adj2_smem_bytes(kAdjNC, kAdjWarps);   // below the 48 KB default limit
+    static_assert(kSmem2 <= 48 * 1024, "two-step ring exceeds the default dynamic shared memory");
+    if (form == ADJ_FORM_TILES) {
+        adjoint_step_kernel<<<grid, kAdjTileW * kAdjTileH, 0, stream>>>(tubes, adj, run, local, phase);
+    } else if (form == ADJ_FORM_STRIPS2) {
+        if (rows == 4)
+            adjoint2_kernel<kAdjNC, 4, kAdjWarps><<<grid, kThreads, kSmem2, stream>>>(tubes, adj, run, local, phase);
+        else if (rows == 8)
+            adjoint2_kernel<kAdjNC, 8, kAdjWarps><<<grid, kThreads, kSmem2, stream>>>(tubes, adj, run, local, phase);
+        else
+            adjoint2_kernel<kAdjNC, 16, kAdjWarps><<<grid, kThreads, kSmem2, stream>>>(tubes, adj, run, local, phase);
+    } else {
+        if (rows == 4)
+            adjoint_strip_kernel<kAdjNC, 4, kAdjWarps><<<grid, kThreads, 0, stream>>>(tubes, adj, run, local, phase);
+        else if (rows == 8)
+            adjoint_strip_kernel<kAdjNC, 8, kAdjWarps><<<grid, kThreads, 0, stream>>>(tubes, adj, run, local, phase);
+        else
+            adjoint_strip_kernel<kAdjNC, 16, kAdjWarps><<<grid, kThreads, 0, stream>>>(tubes, adj, run, local, phase);
+    }
     return cudaGetLastError();
 }
 
-int adjoint_strips(int H, int W) { return ((W - 2) / (30 * kAdjNC) + 1) * ((H - 2 + kAdjTR - 1) / kAdjTR); }
+int adjoint_strips(int H, int W, int form, int rows) {
+    (void)form;   // both strip forms use the same geometry
+    return ((W - 2) / (30 * kAdjNC) + 1) * ((H - 2 + rows - 1) / rows);
+}
 
 int adjoint_strip_blocks(int strips) { return (strips + kAdjWarps - 1) / kAdjWarps; }
 

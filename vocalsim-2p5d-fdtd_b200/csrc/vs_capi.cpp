@@ -119,7 +119,9 @@ struct vs_batch {
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
     int cluster_state = 0;                 // cluster shape: 0 = not checked, 1 = fits, -1 = does not
     uint32_t wait_polls = 0;               // RunState::wait_polls of every run (0 = the default limit)
-    int adj_form = ADJ_FORM_STRIPS;        // reverse-step kernel form (vs_batch_set_adjoint_form)
+    int adj_form = ADJ_FORM_AUTO;          // reverse-step kernel form (vs_batch_set_adjoint_form)
+    int adj_rows = 0;                      // rows per strip of the strip forms (0 = the form's default)
+    int adj_graph_rows = 0;
     ClusterConfig cluster{};
     // adjoint: checkpoints of the last checkpointed forward, history, adjoint planes
     int64_t ck_steps = 0;                  // steps of the checkpointed forward (0 = none)
@@ -925,10 +927,28 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     const int n = (int)b->grids.size();
     const int64_t steps = b->ck_steps;
     const int K = b->ck_every;
-    // device memory per tube: history (K+1 slots x 3 planes), then the part
-    // zeroed per call: lambda (2 x 3 planes), gradients (4 double planes) and,
-    // with the two-mass source, its state history (K+1) and adjoint (6)
-    std::vector<size_t> off(n), zero_off(n), zero_len(n);
+    // the form of this call's reverse steps.  Automatic: two-step strips of 8
+    // rows when the batch has table sources only and gives every SM at least
+    // four strips, else tiles (the strips' row march is latency-bound with
+    // few warps).  The two-step strips need table sources (the two-mass
+    // reverse step runs beside each single step), so a two-mass batch runs
+    // them one step per launch.
+    bool any_tmm = false;
+    int64_t strips8 = 0;
+    for (const TubeGrid& g : b->grids) {
+        any_tmm = any_tmm || g.tmm;
+        strips8 += adjoint_strips(g.H, g.W, ADJ_FORM_STRIPS2, 8);
+    }
+    int sms = 148;
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "device attribute");
+    int form = b->adj_form;
+    if (form == ADJ_FORM_AUTO) form = (!any_tmm && strips8 >= 4 * (int64_t)sms) ? ADJ_FORM_STRIPS2 : ADJ_FORM_TILES;
+    if (form == ADJ_FORM_STRIPS2 && any_tmm) form = ADJ_FORM_STRIPS;
+    const int rows = b->adj_rows ? b->adj_rows : (form == ADJ_FORM_STRIPS2 ? 8 : 4);
+    // device memory per tube, all zeroed per call: history (K+1 slots x 3
+    // planes), lambda (2 x 3 planes), gradients (4 double planes) and, with
+    // the two-mass source, its state history (K+1) and adjoint (6)
+    std::vector<size_t> off(n), zero_off(n);
     size_t total = 0;
     int max_tiles = 0, max_plane = 0;
     for (int i = 0; i < n; ++i) {
@@ -939,9 +959,8 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         zero_off[i] = total;
         total += align_up(pe * sizeof(float) * 6) + align_up(pe * sizeof(double) * 4);
         if (g.tmm) total += align_up((size_t)(K + 1) * 6 * sizeof(double)) + align_up(8 * sizeof(double));
-        zero_len[i] = total - zero_off[i];
         const int tiles = ((g.W - 2 + kAdjTileW - 1) / kAdjTileW) * ((g.H - 2 + kAdjTileH - 1) / kAdjTileH);
-        const int blocks = b->adj_form == ADJ_FORM_TILES ? tiles : adjoint_strip_blocks(adjoint_strips(g.H, g.W));
+        const int blocks = form == ADJ_FORM_TILES ? tiles : adjoint_strip_blocks(adjoint_strips(g.H, g.W, form, rows));
         max_tiles = std::max(max_tiles, blocks);
         max_plane = std::max(max_plane, g.H * g.pitch);
     }
@@ -950,8 +969,11 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         ck(cudaMalloc(&b->adj_mem, total), "cudaMalloc(adjoint)");
         b->adj_bytes = total;
     }
-    for (int i = 0; i < n; ++i)
-        ck(cudaMemsetAsync(b->adj_mem + zero_off[i], 0, zero_len[i], b->stream), "zero adjoint");
+    // everything starts at zero: lambda, the accumulators and the history,
+    // whose ring and row padding the history-capturing steps never write
+    // (the forward keeps those cells at zero; the reverse steps read them as
+    // neighbours of edge cells)
+    ck(cudaMemsetAsync(b->adj_mem, 0, total, b->stream), "zero adjoint");
     if ((int64_t)n * steps > b->gtrace_cap) {
         if (b->d_gtrace) { cudaFree(b->d_gtrace); b->d_gtrace = nullptr; }
         ck(cudaMalloc(&b->d_gtrace, (size_t)n * steps * sizeof(float)), "cudaMalloc(trace gradient)");
@@ -1026,8 +1048,8 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         adj[i].exc_coef = d_coef;
         adj[i].n_exc = (int32_t)nb;
         adj[i].tiles = ((g.W - 2 + kAdjTileW - 1) / kAdjTileW) * ((g.H - 2 + kAdjTileH - 1) / kAdjTileH);
-        adj[i].strips = adjoint_strips(g.H, g.W);
-        const int blocks = b->adj_form == ADJ_FORM_TILES ? adj[i].tiles : adjoint_strip_blocks(adj[i].strips);
+        adj[i].strips = adjoint_strips(g.H, g.W, form, rows);
+        const int blocks = form == ADJ_FORM_TILES ? adj[i].tiles : adjoint_strip_blocks(adj[i].strips);
         if (g.tmm) max_tiles = std::max(max_tiles, blocks + 1);
     }
     if (!b->d_adj) ck(cudaMalloc(&b->d_adj, n * sizeof(AdjTube)), "cudaMalloc(adjoint descriptors)");
@@ -1044,13 +1066,26 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     auto hist_step = [&](int j) {
         return launch_step_history(hshape, b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, j, b->stream);
     };
-    auto adj_step = [&](int j) { return launch_adjoint_step(b->d_tubes, b->d_adj, n, max_tiles, b->d_adjrun, j,
-                                                            b->stream, b->adj_form); };
-    if (b->adj_graph_len != K || b->adj_graph_form != b->adj_form || !b->hist_graph || !b->adj_graph) {
+    // reverse launches of a segment of len steps: one per step, or in the
+    // two-step form len / 2 two-step launches and, for odd len, one single
+    // step last; launch j reads lambda parity q0 ^ (j & 1)
+    const bool two = form == ADJ_FORM_STRIPS2;
+    auto launches = [&](int len) { return two ? len / 2 + (len & 1) : len; };
+    auto adj_launch = [&](int j, int len) {
+        if (two && 2 * j + 1 < len)
+            return launch_adjoint_step(b->d_tubes, b->d_adj, n, max_tiles, b->d_adjrun, 2 * j, j, b->stream,
+                                       ADJ_FORM_STRIPS2, rows);
+        const int local = two ? 2 * j : j;
+        return launch_adjoint_step(b->d_tubes, b->d_adj, n, max_tiles, b->d_adjrun, local, j, b->stream,
+                                   two ? ADJ_FORM_STRIPS : form, rows);
+    };
+    if (b->adj_graph_len != K || b->adj_graph_form != form || b->adj_graph_rows != rows || !b->hist_graph ||
+        !b->adj_graph) {
         capture(b, &b->hist_graph, "capture history steps", hist_step, K);
-        capture(b, &b->adj_graph, "capture reverse steps", adj_step, K);
+        capture(b, &b->adj_graph, "capture reverse steps", [&](int j) { return adj_launch(j, K); }, launches(K));
         b->adj_graph_len = K;
-        b->adj_graph_form = b->adj_form;
+        b->adj_graph_form = form;
+        b->adj_graph_rows = rows;
     }
     int q = 0;                    // lambda parity holding the adjoint of the later state
     // events around each segment's recomputation and reverse steps, for the
@@ -1079,10 +1114,10 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         } else {
             for (int j = 0; j < len; ++j) ck(hist_step(j), "history step");
             ck(cudaEventRecord(ev[3 * k + 1], b->stream), "event");
-            for (int j = 0; j < len; ++j) ck(adj_step(j), "adjoint step");
+            for (int j = 0; j < launches(len); ++j) ck(adj_launch(j, len), "adjoint step");
         }
         ck(cudaEventRecord(ev[3 * k + 2], b->stream), "event");
-        q ^= len & 1;
+        q ^= launches(len) & 1;
     }
     ck(cudaStreamSynchronize(b->stream), "adjoint sync");
     b->adj_recompute_ms = 0.0f;
@@ -1402,9 +1437,17 @@ int vs_batch_adjoint_times(const vs_batch* b, float* recompute_ms, float* revers
 }
 
 int vs_batch_set_adjoint_form(vs_batch* b, int32_t form) {
-    if (!b || (form != ADJ_FORM_STRIPS && form != ADJ_FORM_TILES))
-        return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_adjoint_form: form must be 0 (strips) or 1 (tiles)");
+    if (!b || form < ADJ_FORM_AUTO || form > ADJ_FORM_STRIPS)
+        return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_adjoint_form: form must be 0 (automatic), 1 (tiles), "
+                                             "2 (two-step strips) or 3 (one-step strips)");
     b->adj_form = form;
+    return VS_OK;
+}
+
+int vs_batch_set_adjoint_rows(vs_batch* b, int32_t rows) {
+    if (!b || (rows != 0 && rows != 4 && rows != 8 && rows != 16))
+        return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_adjoint_rows: rows must be 0 (default), 4, 8 or 16");
+    b->adj_rows = rows;
     return VS_OK;
 }
 

@@ -232,7 +232,7 @@ struct AdjTube {
     const float* exc_coef;
     int32_t n_exc;
     int32_t tiles;        // 32 x 8 cell tiles of the interior (tile form)
-    int32_t strips;       // row-marching strips of the interior (strip form)
+    int32_t strips;       // row-marching strips of the interior (strip forms)
     // per-cell neighbourhood descriptors (H x pitch bytes) into a table of
     // three float4 per descriptor: (ax, ay, bx, by), (alx, aly, 1 + sigma,
     // Dirichlet no-pressure flag), (zc_out x, zc_in x, zc_out y, zc_in y)
@@ -241,9 +241,11 @@ struct AdjTube {
 };
 
 // Segment of the reverse sweep, in device memory so that one captured graph
-// serves every segment: launch `local` reverses forward step
-// n = start + len - 1 - local, whose state-before is history slot n - start;
-// the adjoint of the state after it is in lambda parity q0 ^ (local & 1).
+// serves every segment: a launch with reverse-step index `local` reverses
+// forward step n = start + len - 1 - local (and, in the two-step form, n - 1
+// after it), whose state-before is history slot n - start; launch number
+// `phase` of the segment reads the adjoint of the state after its first step
+// from lambda parity q0 ^ (phase & 1) and writes the other parity.
 struct AdjRun {
     int64_t start;
     int32_t len;
@@ -253,20 +255,29 @@ struct AdjRun {
 // Tile of the reverse step kernel.
 constexpr int kAdjTileW = 32, kAdjTileH = 8;
 
-// One reverse step (launch index `local` of the segment in `run`) for every
-// tube: lambda of the state before the step, the map / z_inv gradient terms
-// and, for the two-mass source, its reverse step.  max_tiles = the largest
-// AdjTube::tiles of the batch, plus one when a tube has the two-mass source
-// (its reverse step runs in the block after the tiles).
-// Two implementations of the same reverse step: 32 x 8 tiles with mu in
-// shared memory, or row-marching warp strips with several columns per lane
-// (the default).  max_blocks = the largest block count of a tube in the
-// chosen form, plus one when a tube has the two-mass source.
-enum : int { ADJ_FORM_STRIPS = 0, ADJ_FORM_TILES = 1 };
+// One reverse step (reverse-step index `local`, launch number `phase` of the
+// segment in `run`) for every tube: lambda of the state before the step, the
+// map / z_inv gradient terms and, for the two-mass source, its reverse step.
+// Three implementations:
+//   ADJ_FORM_TILES    32 x 8 tiles with mu in shared memory, one step per
+//                     launch: the most parallel form, best for small batches
+//   ADJ_FORM_STRIPS2  row-marching warp strips running two reverse steps per
+//                     launch (steps n and n - 1; the second one row behind the
+//                     first on values held in registers), so lambda and the
+//                     gradient accumulators are read and written once per two
+//                     steps; table sources only (no two-mass tube)
+//   ADJ_FORM_STRIPS   the same strips, one reverse step per launch
+// ADJ_FORM_AUTO picks two-step strips for a large batch of table-source tubes
+// and tiles otherwise.  `rows` = rows per strip (4, 8 or 16) of the strip
+// forms.  max_blocks = the largest block count of a tube in the chosen form,
+// plus one when a tube has the two-mass source (its reverse step runs in the
+// block after the others).
+enum : int { ADJ_FORM_AUTO = 0, ADJ_FORM_TILES = 1, ADJ_FORM_STRIPS2 = 2, ADJ_FORM_STRIPS = 3 };
 cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_blocks,
-                                const AdjRun* run, int local, cudaStream_t stream, int form);
-int adjoint_strips(int H, int W);             // strips of an H x W frame
-int adjoint_strip_blocks(int strips);         // CTAs those strips take
+                                const AdjRun* run, int local, int phase, cudaStream_t stream, int form,
+                                int rows);
+int adjoint_strips(int H, int W, int form, int rows);   // strips of an H x W frame
+int adjoint_strip_blocks(int strips);                   // CTAs those strips take
 
 // Copy each tube's state (parity par) into slot 0 of its history (and the
 // two-mass state into slot 0 of tmm_hist).

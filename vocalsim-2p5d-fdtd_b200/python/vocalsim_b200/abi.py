@@ -154,6 +154,7 @@ def load_library(path: os.PathLike | None = None) -> C.CDLL:
         "vs_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int32]),
         "vs_batch_set_wait_limit": (C.c_int, [C.c_void_p, C.c_uint32]),
         "vs_batch_set_adjoint_form": (C.c_int, [C.c_void_p, C.c_int32]),
+        "vs_batch_set_adjoint_rows": (C.c_int, [C.c_void_p, C.c_int32]),
         "vs_batch_adjoint_times": (C.c_int, [C.c_void_p, fp, fp]),
         "vs_batch_forward_ckpt_device": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
         "vs_batch_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, fp, fp, fp, fp]),

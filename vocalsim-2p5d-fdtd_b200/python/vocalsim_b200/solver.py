@@ -165,8 +165,13 @@ class Batch:
         return a.value, r.value
 
     def set_adjoint_form(self, form: int) -> None:
-        """Reverse-step kernel of adjoint(): 0 = warp strips (default), 1 = tiles."""
+        """Reverse-step kernel of adjoint(): 0 = automatic (default), 1 = tiles,
+        2 = two-step warp strips (form 3 for two-mass batches), 3 = one-step strips."""
         check(self.lib, self.lib.vs_batch_set_adjoint_form(self.h, form), "vs_batch_set_adjoint_form")
+
+    def set_adjoint_rows(self, rows: int) -> None:
+        """Rows per strip of the strip forms: 4, 8, 16 or 0 (8 for form 2, 4 for form 3)."""
+        check(self.lib, self.lib.vs_batch_set_adjoint_rows(self.h, rows), "vs_batch_set_adjoint_rows")
 
     def set_wait_limit(self, polls: int) -> None:
         """Polls of a row-copy wait before the run gives up with VS_ERR_TIMEOUT (0 = default)."""
