@@ -187,3 +187,33 @@ def test_two_step_reverse_equals_one_step(rows, every, cuda_ok):
             bound = 4 * np.spacing(np.abs(c).astype(np.float32)) + 1e-9 * np.abs(c).max()
             assert np.all(np.abs(a - c) <= bound)
     assert np.allclose(za, zb, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("kw", [dict(cross_sectional_shape=2, mu3d=0.025, fast_math=1),
+                                dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0, tmm_f64=1,
+                                     fast_math=1)],
+                         ids=["gauss", "two_mass"])
+def test_two_step_recomputation_equals_one_step(kw, cuda_ok):
+    """With fast_math a segment of even length is recomputed by the two-step
+    kernel (both steps' states stored), an odd one step by step; the two
+    give the same history bit for bit, so with one-step reverse strips (form
+    3, each step's terms added on their own) the gradients of checkpoint
+    intervals 256 and 255 are identical."""
+    tubes = [S.batch_tube(i)[:2] for i in (1, 2, 3)]
+    steps = 1100
+    out = []
+    g = None
+    rng = np.random.default_rng(9)
+    for every in (256, 255):
+        b = V.Batch([V.params(**kw) for _ in tubes], [V.Geometry(*t) for t in tubes])
+        b.set_adjoint_form(3)
+        tr = b.forward_ckpt(steps, every)
+        if g is None:
+            g = (rng.uniform(0.5, 1.5, tr.shape) * tr).astype(np.float32)
+        out.append(b.adjoint(g))
+        b.close()
+    (ga, za), (gb, zb) = out
+    for ta, tb in zip(ga, gb):
+        for a, c in zip(ta, tb):
+            assert np.array_equal(a, c)
+    assert np.array_equal(za, zb)

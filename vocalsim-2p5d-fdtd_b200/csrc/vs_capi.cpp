@@ -140,6 +140,8 @@ struct vs_batch {
     size_t exc_bytes = 0;
     Tile* d_hist_tiles = nullptr;
     int n_hist_tiles = 0;
+    Tile* d_hist2_tiles = nullptr;         // two-step history shape (fast_math)
+    int n_hist2_tiles = 0;
     Tile* d_odd_tiles = nullptr;           // single-step tiles beside a two-step shape
     char* x_mem = nullptr;                 // third state set of the two-step shapes (TubeDev::X, tmm_x)
     size_t x_bytes = 0;
@@ -176,6 +178,7 @@ struct vs_batch {
         if (d_gtrace) cudaFree(d_gtrace);
         if (d_exc) cudaFree(d_exc);
         if (d_hist_tiles) cudaFree(d_hist_tiles);
+        if (d_hist2_tiles) cudaFree(d_hist2_tiles);
         if (d_odd_tiles) cudaFree(d_odd_tiles);
         d_odd_tiles = nullptr;
         if (x_mem) cudaFree(x_mem);
@@ -186,7 +189,7 @@ struct vs_batch {
         if (hist_graph) cudaGraphExecDestroy(hist_graph);
         if (adj_graph) cudaGraphExecDestroy(adj_graph);
         ckpt = nullptr; adj_mem = nullptr; d_adj = nullptr; d_adjrun = nullptr; d_gtrace = nullptr;
-        d_exc = nullptr; d_hist_tiles = nullptr; hist_graph = nullptr; adj_graph = nullptr;
+        d_exc = nullptr; d_hist_tiles = nullptr; d_hist2_tiles = nullptr; hist_graph = nullptr; adj_graph = nullptr;
         if (own_stream && stream) cudaStreamDestroy(stream);
         arena = nullptr; src_arena = nullptr; d_tubes = nullptr; d_tiles = nullptr;
         d_rs = nullptr; d_trace = nullptr; stream = nullptr;
@@ -269,7 +272,7 @@ bool cluster_fits(const vs_batch* b) {
         m->cluster_state = -1;
         if (b->grids.size() == 1 && !b->wall) {
             const TubeGrid& g = b->grids[0];
-            if (cluster_config(g.H, g.W, g.pitch, b->fast, &m->cluster)) m->cluster_state = 1;
+            if (cluster_config(g.H, g.W, g.pitch, b->fast, g.tmm, &m->cluster)) m->cluster_state = 1;
         }
     }
     return b->cluster_state == 1;
@@ -365,6 +368,29 @@ Tile* make_tiles(vs_batch* b, int shape, int* n) {
     return d;
 }
 
+// The third P, Vx, Vy set of the two-step kernels (zero ring cells; kGuard
+// bytes around it for the strips' edge reads) and its two-mass slots.
+void ensure_third_set(vs_batch* b) {
+    if (b->x_mem) return;
+    const size_t slots = align_up(sizeof(TmmState)) + align_up(sizeof(TmmState64));
+    size_t total = kGuard;
+    for (const TubeDev& t : b->h_tubes) total += 3 * (size_t)t.plane * sizeof(float) + slots;
+    total += kGuard;
+    ck(cudaMalloc(&b->x_mem, total), "cudaMalloc(third state set)");
+    ck(cudaMemset(b->x_mem, 0, total), "zero third state set");
+    b->x_bytes = total;
+    size_t off = kGuard;
+    for (TubeDev& t : b->h_tubes) {
+        t.X = reinterpret_cast<float*>(b->x_mem + off);
+        off += 3 * (size_t)t.plane * sizeof(float);
+        t.tmm_x = reinterpret_cast<TmmState*>(b->x_mem + off);
+        t.tmm64_x = reinterpret_cast<TmmState64*>(b->x_mem + off + align_up(sizeof(TmmState)));
+        off += slots;
+    }
+    ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev), cudaMemcpyHostToDevice),
+       "upload tube descriptors");
+}
+
 void build_tiles(vs_batch* b, int shape) {
     if (tile_shape(shape).kind == SHAPE_CLUSTER) return;     // the cluster kernel needs no tile list
     if (b->tiles_shape == shape && b->d_tiles) return;
@@ -382,28 +408,8 @@ void build_tiles(vs_batch* b, int shape) {
             b->odd_shape = single_step_shape(b);
             b->d_odd_tiles = make_tiles(b, b->odd_shape, &b->n_odd_tiles);
         }
-        // and alternates the state with a third set of planes (zero ring
-        // cells; kGuard bytes around it for the strips' edge reads)
-        if (!b->x_mem) {
-            const size_t slots = align_up(sizeof(TmmState)) + align_up(sizeof(TmmState64));
-            size_t total = kGuard;
-            for (const TubeDev& t : b->h_tubes) total += 3 * (size_t)t.plane * sizeof(float) + slots;
-            total += kGuard;
-            ck(cudaMalloc(&b->x_mem, total), "cudaMalloc(third state set)");
-            ck(cudaMemset(b->x_mem, 0, total), "zero third state set");
-            b->x_bytes = total;
-            size_t off = kGuard;
-            for (TubeDev& t : b->h_tubes) {
-                t.X = reinterpret_cast<float*>(b->x_mem + off);
-                off += 3 * (size_t)t.plane * sizeof(float);
-                t.tmm_x = reinterpret_cast<TmmState*>(b->x_mem + off);
-                t.tmm64_x = reinterpret_cast<TmmState64*>(b->x_mem + off + align_up(sizeof(TmmState)));
-                off += slots;
-            }
-            ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), b->h_tubes.size() * sizeof(TubeDev),
-                          cudaMemcpyHostToDevice),
-               "upload tube descriptors");
-        }
+        // and alternates the state with a third set of planes
+        ensure_third_set(b);
     }
 }
 
@@ -945,6 +951,10 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     if (form == ADJ_FORM_AUTO) form = (!any_tmm && strips8 >= 4 * (int64_t)sms) ? ADJ_FORM_STRIPS2 : ADJ_FORM_TILES;
     if (form == ADJ_FORM_STRIPS2 && any_tmm) form = ADJ_FORM_STRIPS;
     const int rows = b->adj_rows ? b->adj_rows : (form == ADJ_FORM_STRIPS2 ? 8 : 4);
+    // with fast_math a full segment (K even) is recomputed two steps per
+    // launch by the two-step kernel, which needs the third state set
+    const bool hist_two = b->fast && K % 2 == 0;
+    if (hist_two) ensure_third_set(b);
     // device memory per tube, all zeroed per call: history (K+1 slots x 3
     // planes), lambda (2 x 3 planes), gradients (4 double planes) and, with
     // the two-mass source, its state history (K+1) and adjoint (6)
@@ -1066,6 +1076,11 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     auto hist_step = [&](int j) {
         return launch_step_history(hshape, b->d_tubes, b->d_hist_tiles, b->n_hist_tiles, b->d_rs, j, b->stream);
     };
+    const int h2shape = hist_two ? history2_shape(cells) : -1;
+    if (hist_two && !b->d_hist2_tiles) b->d_hist2_tiles = make_tiles(b, h2shape, &b->n_hist2_tiles);
+    auto hist2_step = [&](int j) {
+        return launch_step_history2(h2shape, b->d_tubes, b->d_hist2_tiles, b->n_hist2_tiles, b->d_rs, j, b->stream);
+    };
     // reverse launches of a segment of len steps: one per step, or in the
     // two-step form len / 2 two-step launches and, for odd len, one single
     // step last; launch j reads lambda parity q0 ^ (j & 1)
@@ -1081,7 +1096,8 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     };
     if (b->adj_graph_len != K || b->adj_graph_form != form || b->adj_graph_rows != rows || !b->hist_graph ||
         !b->adj_graph) {
-        capture(b, &b->hist_graph, "capture history steps", hist_step, K);
+        if (hist_two) capture(b, &b->hist_graph, "capture history steps", hist2_step, K / 2);
+        else capture(b, &b->hist_graph, "capture history steps", hist_step, K);
         capture(b, &b->adj_graph, "capture reverse steps", [&](int j) { return adj_launch(j, K); }, launches(K));
         b->adj_graph_len = K;
         b->adj_graph_form = form;

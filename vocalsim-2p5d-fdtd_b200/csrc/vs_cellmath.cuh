@@ -249,21 +249,33 @@ __device__ __noinline__ float glottal_step(const TubeDev* T, int par, float p1, 
     return e;
 }
 
+// The six state values of a two-mass state as the adjoint's history keeps them.
+template <class S>
+__device__ __forceinline__ void tmm_to_hist(const S& s, double* h) {
+    h[0] = s.x1_old; h[1] = s.x1_curr; h[2] = s.x2_old;
+    h[3] = s.x2_curr; h[4] = s.ug_old; h[5] = s.ug_curr;
+}
+
 // Two-mass steps n and n+1 for the two-step kernels: the state of step n is
 // in the parity slot (from_x = false) or the third slot, that of step n+2
-// goes to the other one (stored by the owning strip only).
+// goes to the other one (stored by the owning strip only, which also writes
+// the states after steps n and n+1 to hist[0..5] and hist[6..11] when given).
 __device__ __noinline__ float2 glottal_two_steps(const TubeDev* T, int par, bool from_x, float p1, float p2,
-                                                 bool store) {
+                                                 bool store, double* hist = nullptr) {
     float2 e;
     if (T->flags & TUBE_TMM64) {
         TmmState64 s = from_x ? *T->tmm64_x : T->tmm64[par];
         e.x = tmm_step64(T->tmmd, s, p1);
+        if (store && hist) tmm_to_hist(s, hist);
         e.y = tmm_step64(T->tmmd, s, p2);
+        if (store && hist) tmm_to_hist(s, hist + 6);
         if (store) *(from_x ? &T->tmm64[par] : T->tmm64_x) = s;
     } else {
         TmmState s = from_x ? *T->tmm_x : T->tmm[par];
         e.x = tmm_step(T->tmmc, s, p1);
+        if (store && hist) tmm_to_hist(s, hist);
         e.y = tmm_step(T->tmmc, s, p2);
+        if (store && hist) tmm_to_hist(s, hist + 6);
         if (store) *(from_x ? &T->tmm[par] : T->tmm_x) = s;
     }
     return e;

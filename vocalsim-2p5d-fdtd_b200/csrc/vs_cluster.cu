@@ -38,8 +38,10 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "vs_cellmath.cuh"
+#include "vs_mbarrier.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -336,8 +338,30 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
 // values of each row go through shared memory (eUX: Vx dX of the column left of
 // a warp, for its lane 0; eP: P' of the column right of a warp, for its lane
 // 31), and the ghost rows arrive in shared memory as in the first form.  The
-// step sequence, the barriers and the per-cell arithmetic are those of the
-// first form.
+// step sequence and the per-cell arithmetic are those of the first form.
+//
+// Step synchronisation, two variants:
+//   P2P = false  the first form's cluster barrier after every step (its
+//                release fence waits for every thread's stores into the
+//                neighbours' ghost rows)
+//   P2P = true   point to point: a thread sends its boundary velocities with
+//                st.async, whose bytes count against the receiving CTA's
+//                mbarrier for that ghost parity; at the end of a step one
+//                thread arrives on the barrier of the next step's ghosts
+//                (expecting the bytes both neighbours send) and waits for it,
+//                and the block barrier that follows publishes the ghosts and
+//                the warp-edge values to the CTA.  A CTA then waits only for
+//                its two neighbours, never for the whole cluster.  Ghost slots
+//                stay double-buffered: a neighbour writes parity q again only
+//                after it received this CTA's ghosts of the step in between,
+//                which this CTA sends after it has read parity q.  The
+//                two-mass excitation value, which every CTA needs, travels in a
+//                ring of kExeRing tagged slots (the value and its step in one
+//                8-byte store); a CTA lags the owner of the excitation cell by
+//                at most its distance in CTAs, so a slot is never reused while
+//                a CTA may still read it.  Waits are bounded; a CTA that gives
+//                up reports VS_ERR_TIMEOUT, and every CTA meets at a final
+//                cluster barrier before any exits.
 // The two-mass model's state and its prepared step, kept in shared memory by
 // the one thread that runs it, so that the model's registers do not count
 // against every thread's budget (the helpers are not inlined).
@@ -359,8 +383,19 @@ __device__ __noinline__ float tmm_slot_finish(TmmSlot* slot, bool tmm64, float p
 
 struct RegLayout {
     int pitch, nw, rmax;
-    size_t gVx, gVyT, gVyB, dX0, eUX, eP, tab, sig, exe, tmm, bytes;   // byte offsets
+    size_t gT, gVyB, dX0, eUX, eP, tab, sig, exe, tmm, bar, exr, bytes;   // byte offsets
 };
+
+constexpr int kExeRing = 32;        // excitation values in flight (> the largest cluster)
+
+// f(integral_constant<int, I>) for I = B .. E-1, unrolled at compile time
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (B < E) {
+        f(std::integral_constant<int, B>{});
+        static_for<B + 1, E>(f);
+    }
+}
 
 __host__ __device__ inline RegLayout reg_layout(int pitch, int nthreads, int rmax, bool fast) {
     RegLayout L{};
@@ -369,8 +404,7 @@ __host__ __device__ inline RegLayout reg_layout(int pitch, int nthreads, int rma
     L.rmax = rmax;
     size_t o = 0;
     auto take = [&](size_t bytes) { const size_t at = o; o += (bytes + 15) / 16 * 16; return at; };
-    L.gVx = take(2 * (size_t)pitch * sizeof(float));
-    L.gVyT = take(2 * (size_t)pitch * sizeof(float));
+    L.gT = take(2 * (size_t)pitch * sizeof(float2));
     L.gVyB = take(2 * (size_t)pitch * sizeof(float));
     L.dX0 = take((size_t)pitch * sizeof(float));
     L.eUX = take((size_t)(L.nw + 1) * (rmax + 1) * sizeof(float));
@@ -379,11 +413,13 @@ __host__ __device__ inline RegLayout reg_layout(int pitch, int nthreads, int rma
     L.sig = take(16 * sizeof(float));
     L.exe = take(4 * sizeof(float));
     L.tmm = take(sizeof(TmmSlot));
+    L.bar = take(2 * sizeof(uint64_t));
+    L.exr = take(kExeRing * sizeof(float2));
     L.bytes = (o + 127) / 128 * 128;
     return L;
 }
 
-template <bool FAST, int RMAX, int MAXT>
+template <bool FAST, int RMAX, int MAXT, bool P2P>
 __global__ void __launch_bounds__(MAXT, 1)
 cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_t nsteps) {
     extern __shared__ __align__(16) unsigned char r_smem[];
@@ -394,9 +430,11 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
     const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const RegLayout L = reg_layout(pitch, nthr, RMAX, FAST);
-    float* gVx = reinterpret_cast<float*>(r_smem + L.gVx);     // [2][pitch] ghost top Vx
-    float* gVyT = reinterpret_cast<float*>(r_smem + L.gVyT);   // [2][pitch] ghost top Vy
+    float2* gT = reinterpret_cast<float2*>(r_smem + L.gT);     // [2][pitch] ghost top (Vx, Vy)
     float* gVyB = reinterpret_cast<float*>(r_smem + L.gVyB);   // [2][pitch] ghost bottom Vy
+    uint64_t* bar = reinterpret_cast<uint64_t*>(r_smem + L.bar);   // [2] ghost arrival, by parity
+    // [kExeRing] excitation slots: value bits | step << 32, one 8-byte (single-copy atomic) word each
+    unsigned long long* exr = reinterpret_cast<unsigned long long*>(r_smem + L.exr);
     float* sdX0 = reinterpret_cast<float*>(r_smem + L.dX0);    // dX of the top ghost row
     float* eUX = reinterpret_cast<float*>(r_smem + L.eUX);     // [nw + 1][RMAX + 1]
     float* eP = reinterpret_cast<float*>(r_smem + L.eP);       // [nw + 1][RMAX + 1]
@@ -460,10 +498,8 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     // ghost slots, edge buffers, tables
     for (int x = tid; x < pitch; x += nthr) {
         const int64_t o = (int64_t)(r0 - 1) * pitch + x;
-        gVx[par0 * pitch + x] = gP[2 * pl + o];
-        gVyT[par0 * pitch + x] = gP[4 * pl + o];
-        gVx[(par0 ^ 1) * pitch + x] = 0.0f;
-        gVyT[(par0 ^ 1) * pitch + x] = 0.0f;
+        gT[par0 * pitch + x] = make_float2(gP[2 * pl + o], gP[4 * pl + o]);
+        gT[(par0 ^ 1) * pitch + x] = make_float2(0.0f, 0.0f);
         const int64_t ob = (int64_t)(r0 + Rk) * pitch + x;
         gVyB[par0 * pitch + x] = gP[4 * pl + ob];
         gVyB[(par0 ^ 1) * pitch + x] = 0.0f;
@@ -476,6 +512,14 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     if (FAST)
         for (int j = tid; j < 2 * kDescEntries; j += nthr) tabA[j] = T->desc_a[j];
     if (tid < 16) sSig[tid] = tid < 13 ? T->sigma[tid] : 0.0f;
+    if (P2P) {
+        if (tid == 0) {
+            mbar_init(bar, 1);
+            mbar_init(bar + 1, 1);
+            mbar_fence_init();            // visible to the cluster before its first remote arrival
+        }
+        for (int j = tid; j < kExeRing; j += nthr) exr[j] = 0xffffffff00000000ull;   // tag: no step
+    }
     __syncthreads();
     // left-edge values of every warp for the first step (lane 31 of the warp before)
     if (lane == 31 && warp + 1 <= L.nw) {
@@ -508,12 +552,22 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
                 if (i == exc_i) *sPexc = P[i];
         }
     };
+    // the two-mass value of step m into every CTA's ring slot, tagged with m
+    auto send_exe_ring = [&](int64_t m, float e) {
+        const unsigned long long v = ((unsigned long long)(uint32_t)m << 32) | __float_as_uint(e);
+        for (int j = 0; j < C; ++j) {
+            volatile unsigned long long* d = cluster.map_shared_rank(exr + (m & (kExeRing - 1)), j);
+            *d = v;
+        }
+    };
     publish_pexc();
     __syncthreads();
     cluster.sync();
     if (tmm_thread) {
         tmm_prepare_next();
-        send_exe(par0, tmm_finish_next(*sPexc));
+        const float e0 = tmm_finish_next(*sPexc);
+        if (P2P) send_exe_ring(n0, e0);
+        else send_exe(par0, e0);
         tmm_prepare_next();
     } else if (!tmm && tid == 0) {
         sExe[par0] = n0 < T->src_len ? T->src[n0] : 0.0f;
@@ -521,8 +575,17 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     cluster.sync();
 
     float* up_gVyB = k > 0 ? cluster.map_shared_rank(gVyB, k - 1) : nullptr;
-    float* dn_gVx = k + 1 < C ? cluster.map_shared_rank(gVx, k + 1) : nullptr;
-    float* dn_gVyT = k + 1 < C ? cluster.map_shared_rank(gVyT, k + 1) : nullptr;
+    float2* dn_gT = k + 1 < C ? cluster.map_shared_rank(gT, k + 1) : nullptr;
+    // point to point: cluster addresses of the neighbours' ghost slots and barriers,
+    // and the bytes both neighbours send into this CTA per step
+    const uint32_t up_gVyB_a = P2P && k > 0 ? cluster_addr(gVyB, k - 1) : 0u;
+    const uint32_t up_bar_a = P2P && k > 0 ? cluster_addr(bar, k - 1) : 0u;
+    const uint32_t dn_gT_a = P2P && k + 1 < C ? cluster_addr(gT, k + 1) : 0u;
+    const uint32_t dn_bar_a = P2P && k + 1 < C ? cluster_addr(bar, k + 1) : 0u;
+    const uint32_t expect = (k > 0 ? 8u * (uint32_t)(W - 2) : 0u) + (k + 1 < C ? 4u * (uint32_t)(W - 2) : 0u);
+    const uint32_t limit = first_wait_limit(rs);
+    uint32_t phase = 0;                          // bit b: parity of the next phase of bar[b]
+    bool fail = false;
 
     const float K1 = T->K1, bco = T->bcoef;
     const bool eigen = flags & TUBE_EIGEN, dirichlet = flags & TUBE_DIRICHLET;
@@ -535,20 +598,18 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
 
     for (int64_t n = n0; n < n_end; ++n) {
         const int p = (int)(n & 1), q = p ^ 1;
-        // ghost values of this step
-        VX[0] = gVx[p * pitch + cc];
-        VY[0] = gVyT[p * pitch + cc];
-        vyb = gVyB[p * pitch + cc];
-        const float uxl_ghost = c - 1 >= 0 ? fmul(gVx[p * pitch + c - 1], sdX0[c - 1]) : 0.0f;
-        // ---- P' of rows r0-1 .. r1 (FDTDEngineCPU.cpp:316-339)
-#pragma unroll
-        for (int i = 0; i <= RMAX; ++i) {
-            if (i > Rk) break;
+        // the table value of the next step, loaded while this step runs
+        const float src_next = (P2P && !tmm && tid == 0 && n + 1 < n_end && n + 1 < T->src_len) ? T->src[n + 1]
+                                                                                               : 0.0f;
+        // ---- P' of rows r0-1 .. r1 (FDTDEngineCPU.cpp:316-339); row i of the
+        // band takes its lower Vy from vyd (the bottom ghost for row Rk)
+        float uxl_ghost = 0.0f;
+        auto prow = [&](auto ic, float vyd) {
+            constexpr int i = decltype(ic)::value;
             const float ux = fmul(VX[i], dX[i]);
             float uxl = __shfl_up_sync(kAll, ux, 1);
             if (i == 0) uxl = uxl_ghost;
             else if (lane == 0) uxl = eUX[warp * (RMAX + 1) + i];
-            const float vyd = i == Rk ? vyb : VY[i + 1 <= RMAX ? i + 1 : RMAX];
             const float uy = fmul(VY[i], dY[i]), uyb = fmul(vyd, dY[i + 1]);
             float pn;
             if constexpr (FAST) {
@@ -569,12 +630,62 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
             if (mine && !(i == 0 && ifirst == 1)) P[i] = pn;
             if (i == lis_i && i >= 1) store_trace(rs, trace + (n - run_start), pn);
             if (lane == 0 && i >= 1) eP[warp * (RMAX + 1) + i] = P[i];
+        };
+        int bad = 0;
+        if (P2P) {
+            // rows 1 .. Rk-1 need no ghost value: they run while the neighbours' rows arrive
+            static_for<1, RMAX>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                if (i < Rk) prow(ic, VY[i + 1]);
+            });
+            if (n > n0) {
+                // every thread polls the arrival of this step's ghosts (bounded)
+                const uint32_t par = (phase >> p) & 1u;
+                phase ^= 1u << p;
+                if (!mbar_wait_parity_bounded(bar + p, par, limit)) bad = 1;
+            }
+        }
+        // ghost values of this step
+        const float2 gt = gT[p * pitch + cc];
+        VX[0] = gt.x;
+        VY[0] = gt.y;
+        vyb = gVyB[p * pitch + cc];
+        uxl_ghost = c - 1 >= 0 ? fmul(gT[p * pitch + c - 1].x, sdX0[c - 1]) : 0.0f;
+        if (P2P) {
+            prow(std::integral_constant<int, 0>{}, VY[1]);
+            static_for<1, RMAX + 1>([&](auto ic) {
+                if (decltype(ic)::value == Rk) prow(ic, vyb);
+            });
+        } else {
+            static_for<0, RMAX + 1>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                if (i <= Rk) prow(ic, i == Rk ? vyb : VY[i + 1 <= RMAX ? i + 1 : RMAX]);
+            });
         }
         publish_pexc();
-        __syncthreads();
-        if (n + 1 < n_end) {
-            if (tmm_thread) send_exe(q, tmm_finish_next(*sPexc));
-            else if (!tmm && tid == 0) sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+        if (P2P) {
+            // this step's two-mass value from the ring slot its thread filled
+            if (tid == 0 && tmm) {
+                const volatile unsigned long long* e = exr + (n & (kExeRing - 1));
+                unsigned long long v = *e;
+                for (uint32_t i = 1; (uint32_t)(v >> 32) != (uint32_t)n && i < limit; ++i) v = *e;
+                if ((uint32_t)(v >> 32) == (uint32_t)n) sExe[p] = __uint_as_float((uint32_t)v);
+                else bad = 1;
+            }
+            if (__syncthreads_or(bad)) {
+                fail = true;
+                break;
+            }
+            if (n + 1 < n_end) {
+                if (tmm_thread) send_exe_ring(n + 1, tmm_finish_next(*sPexc));
+                else if (!tmm && tid == 0) sExe[q] = src_next;
+            }
+        } else {
+            __syncthreads();
+            if (n + 1 < n_end) {
+                if (tmm_thread) send_exe(q, tmm_finish_next(*sPexc));
+                else if (!tmm && tid == 0) sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+            }
         }
         const float exeV = sExe[p];
         // ---- V' of rows r0 .. r1 (FDTDEngineCPU.cpp:364-410)
@@ -619,17 +730,41 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
             if (mine) {
                 VX[i] = vx;
                 VY[i] = vy;
-                if (i == Rk && dn_gVx) {
-                    dn_gVx[(size_t)q * pitch + c] = vx;
-                    dn_gVyT[(size_t)q * pitch + c] = vy;
+                if (P2P) {
+                    if (n + 1 < n_end) {
+                        if (i == Rk && dn_gT_a)
+                            st_async_v2(dn_gT_a + 8u * (uint32_t)(q * pitch + c), vx, vy, dn_bar_a + 8u * q);
+                        if (i == 1 && up_gVyB_a)
+                            st_async_b32(up_gVyB_a + 4u * (uint32_t)(q * pitch + c), vy, up_bar_a + 8u * q);
+                    }
+                } else {
+                    if (i == Rk && dn_gT) dn_gT[(size_t)q * pitch + c] = make_float2(vx, vy);
+                    if (i == 1 && up_gVyB) up_gVyB[(size_t)q * pitch + c] = vy;
                 }
-                if (i == 1 && up_gVyB) up_gVyB[(size_t)q * pitch + c] = vy;
             }
             if (lane == 31) eUX[(warp + 1) * (RMAX + 1) + i] = fmul(VX[i], dX[i]);
         }
-        asm volatile("barrier.cluster.arrive.release;" ::: "memory");
-        if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
-        asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
+        if (P2P) {
+            // one thread arrives on the barrier of the next step's ghosts, expecting
+            // the bytes both neighbours send; the block barrier publishes the edges
+            if (n + 1 < n_end && tid == 0) mbar_expect_tx(bar + q, expect);
+            if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
+            __syncthreads();
+        } else {
+            asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+            if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
+            asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
+        }
+    }
+    if (P2P) {
+        if (fail) {
+            // a neighbour may still be sending: give its stores time to land
+            // before the CTAs meet, and leave the state as it is
+            if (tid == 0) atomicExch(&rs->error, VS_ERR_TIMEOUT);
+            for (int i = 0; i < 64; ++i) __nanosleep(1000);
+        }
+        cluster.sync();                          // no CTA exits while another may store into it
+        if (fail) return;
     }
 
     // ---- the state of step n_end back to its parity set
@@ -663,31 +798,41 @@ namespace {
 // The register form is compiled for at most 4 or 8 rows per band and 256 or
 // 512 threads per CTA (a thread per column; 256 threads leave 255 registers
 // per thread).
-template <bool FAST>
+template <bool FAST, bool P2P>
 const void* reg_fn(int rmax, int threads) {
-    if (rmax <= 4) return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 4, 256>
-                                         : (const void*)cluster_reg_kernel<FAST, 4, 512>;
-    return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 8, 256> : (const void*)cluster_reg_kernel<FAST, 8, 512>;
+    if (rmax <= 4) return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 4, 256, P2P>
+                                         : (const void*)cluster_reg_kernel<FAST, 4, 512, P2P>;
+    return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 8, 256, P2P>
+                          : (const void*)cluster_reg_kernel<FAST, 8, 512, P2P>;
 }
 
+// form 0: shared-memory bands; 1: register form, cluster barrier per step;
+// 2: register form, point-to-point neighbour exchange
 const void* cluster_fn(bool fast, int form, int rmax, int threads) {
     if (form == 0) return fast ? (const void*)cluster_kernel<true> : (const void*)cluster_kernel<false>;
-    return fast ? reg_fn<true>(rmax, threads) : reg_fn<false>(rmax, threads);
+    if (form == 1) return fast ? reg_fn<true, false>(rmax, threads) : reg_fn<false, false>(rmax, threads);
+    return fast ? reg_fn<true, true>(rmax, threads) : reg_fn<false, true>(rmax, threads);
 }
 
-template <bool FAST>
+template <bool FAST, bool P2P>
 cudaError_t launch_reg(const cudaLaunchConfig_t& cfg, int rmax, int threads, const TubeDev* tube, RunState* rs,
                        int64_t steps) {
     if (rmax <= 4)
-        return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 256>, tube, rs, steps)
-                              : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 512>, tube, rs, steps);
-    return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 256>, tube, rs, steps)
-                          : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 512>, tube, rs, steps);
+        return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 256, P2P>, tube, rs, steps)
+                              : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 512, P2P>, tube, rs, steps);
+    return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 256, P2P>, tube, rs, steps)
+                          : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 512, P2P>, tube, rs, steps);
 }
+
+// The register form's step synchronisation: point to point (form 2) for
+// table sources, except the exact arithmetic's 512-thread variants (which
+// spill, and measured slower that way), else the cluster barrier (form 1):
+// the two-mass source's per-step broadcast measured faster with the barrier.
+int reg_form(bool fast, bool tmm, int threads) { return !tmm && (fast || threads <= 256) ? 2 : 1; }
 
 }  // namespace
 
-bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out) {
+bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig* out) {
     const int NR = H - 2;
     if (NR < 4) return false;
     int dev = 0, optin = 0;
@@ -699,7 +844,7 @@ bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out) {
         const int R = (NR + C - 1) / C;
         // the register-resident form where a band has at most 8 rows and a
         // thread per column fits a CTA, the shared-memory form otherwise
-        const int form = (R <= 8 && W <= 512) ? 1 : 0;
+        const int form = (R <= 8 && W <= 512) ? reg_form(fast, tmm, threads) : 0;
         const int rmax = R <= 4 ? 4 : 8;
         const void* fn = cluster_fn(fast, form, rmax, threads);
         const size_t smem = form ? reg_layout(pitch, threads, rmax, fast).bytes : cluster_layout(pitch, R, fast).bytes;
@@ -751,8 +896,11 @@ cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (c.form == 1)
-        return fast ? launch_reg<true>(cfg, c.rmax, c.threads, tube, rs, steps)
-                    : launch_reg<false>(cfg, c.rmax, c.threads, tube, rs, steps);
+        return fast ? launch_reg<true, false>(cfg, c.rmax, c.threads, tube, rs, steps)
+                    : launch_reg<false, false>(cfg, c.rmax, c.threads, tube, rs, steps);
+    if (c.form == 2)
+        return fast ? launch_reg<true, true>(cfg, c.rmax, c.threads, tube, rs, steps)
+                    : launch_reg<false, true>(cfg, c.rmax, c.threads, tube, rs, steps);
     if (fast) return cudaLaunchKernelEx(&cfg, cluster_kernel<true>, tube, rs, steps, c.rows_max);
     return cudaLaunchKernelEx(&cfg, cluster_kernel<false>, tube, rs, steps, c.rows_max);
 }

@@ -180,13 +180,16 @@ int cluster_shape();
 struct ClusterConfig {
     int ctas = 0, threads = 0, rows_max = 0;
     size_t smem = 0;
-    int form = 0;         // 0: band in shared memory; 1: register-resident columns (rows_max <= rmax)
+    int form = 0;         // 0: band in shared memory; 1: register-resident columns (rows_max <= rmax),
+                          // cluster barrier per step; 2: the same, neighbour-to-neighbour exchange
     int rmax = 0;
 };
 // Cluster size (16, 8 or 4 CTAs), threads and shared memory for a tube of
 // H x W cells (row pitch `pitch`) on the current device, or false when none
-// fits; sets the kernel attributes it needs.
-bool cluster_config(int H, int W, int pitch, bool fast, ClusterConfig* out);
+// fits; sets the kernel attributes it needs.  `tmm`: the tube has the
+// two-mass source (its excitation value reaches every CTA each step, which
+// the cluster barrier form does faster than the neighbour exchange).
+bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig* out);
 // `steps` time steps of the tube at `tube` (device) from RunState::step, in
 // one launch; RunState::step advances by `steps`.  The state must be in its
 // parity set (bsel = 0) and stays there.
@@ -215,6 +218,13 @@ cudaError_t prepare_shape(int shape, int max_pitch);
 cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
                                 int local, cudaStream_t stream);
 int history_shape(int64_t cells, bool fast);
+// Two steps (launch `local`: steps RunState::step + 2 local and + 1) with both
+// new states stored into the history, in the reciprocal form (fast_math):
+// the two-step kernel of shape history2_shape() (tiles built for it), with
+// the third state set and RunState::bsel as in a forward run.
+cudaError_t launch_step_history2(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
+                                 int local, cudaStream_t stream);
+int history2_shape(int64_t cells);
 
 // Adjoint buffers of one tube (device memory).
 struct AdjTube {

@@ -28,6 +28,7 @@
 #include "vs_device.h"
 
 #include "vs_cellmath.cuh"
+#include "vs_mbarrier.cuh"
 
 namespace vsb {
 namespace {
@@ -226,66 +227,6 @@ strip_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         vx_c = vx_1; ux_c = fmul(vx_1, dx_1); p_c = p_1; dp_c = dp_1; k_c = k_1;
         o = o1;
     }
-}
-
-// ---- mbarrier and bulk-copy helpers (strip pipelines and bands) ----------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_fence_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// global -> shared bulk copy (no multicast); dst, src 16-byte aligned, bytes % 16 == 0
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-// Bounded wait on phase 0 of an mbarrier: gives up after `limit` polls.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; ++i)
-        if (mbar_try_wait(bar, 0)) return true;
-    return false;
-}
-
-constexpr uint32_t kWaitPolls = 1u << 22;
-
-// Poll limit of the waits whose expiry ends the launch with VS_ERR_TIMEOUT.
-__device__ __forceinline__ uint32_t first_wait_limit(const RunState* rs) {
-    const uint32_t w = rs->wait_polls;
-    return w ? w : kWaitPolls;
-}
-
-// Bounded wait on the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait_parity_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -704,6 +645,9 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 // in the reciprocal form, so the values are those of two single steps.
 // Tile masks classify the extended region (rows from r0-2 / r0-1, columns
 // c0 + NC/2 .. c0 + 32 NC - NC/2 - 1): bit j of v_generic = row r0-1+j.
+// HIST: the adjoint's segment recomputation; the committed cells' state
+// after step n and after step n+1 also go to the history slots n+1 and n+2
+// (and the two-mass states to the two-mass history).
 // ---------------------------------------------------------------------------
 
 
@@ -719,7 +663,7 @@ __device__ __forceinline__ void stn(float* p, const float (&v)[NC], unsigned mas
     }
 }
 
-template <int TR, int WARPS, int MINB, int NC>
+template <int TR, int WARPS, int MINB, int NC, bool HIST = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
              RunState* __restrict__ rs, int local) {
@@ -777,7 +721,8 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                 const float p2 = fmul(__fmaf_rn(-ks, rcp_approx(dPp[e]), p1), __ldg(ta + desc[e]).z);
                 const bool owner = T->exc_y >= r0 && T->exc_y <= rlast && T->exc_x >= c0 + NC &&
                                    T->exc_x < c0 + 31 * NC;
-                const float2 ee = glottal_two_steps(T, par, from_x, p1, p2, owner);
+                const float2 ee = glottal_two_steps(T, par, from_x, p1, p2, owner,
+                                                    HIST ? T->tmm_hist + 6 * (n + 1 - rs->run_start) : nullptr);
                 exe1 = ee.x;
                 exe2 = ee.y;
             }
@@ -789,6 +734,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         }
     }
     float* __restrict__ trace = rs->trace + (int64_t)it.tube * rs->trace_stride + (n - rs->run_start);
+    float* __restrict__ hist1 = HIST ? T->hist + (n + 1 - rs->run_start) * 3 * pl : nullptr;   // after step n
 
     // rows outside the frame read as zeros (they only feed values that are not used)
     auto ldr = [&](float (&d)[NC], const float* base, int row) {
@@ -876,6 +822,12 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             u1[q] = fmul(v1x[q], dx_c[q]);
             w1[q] = fmul(v1y[q], dy_c[q]);
         }
+        if (HIST && r >= r0 && r <= rlast) {
+            const int64_t o = (int64_t)r * pitch + x0;
+            stn<NC>(hist1 + o, pn1, commit_m);
+            stn<NC>(hist1 + pl + o, v1x, commit_m);
+            stn<NC>(hist1 + 2 * pl + o, v1y, commit_m);
+        }
         if (r == lis_y && r >= r0 && r <= rlast && lis_here) {
             float pv = pn1[0];
 #pragma unroll
@@ -920,6 +872,12 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                 stn<NC>(Pout + o, pn2, commit_m);
                 stn<NC>(Vxout + o, vx2, commit_m);
                 stn<NC>(Vyout + o, vy2, commit_m);
+                if (HIST) {
+                    float* hist2 = hist1 + 3 * pl;                // after step n+1
+                    stn<NC>(hist2 + o, pn2, commit_m);
+                    stn<NC>(hist2 + pl + o, vx2, commit_m);
+                    stn<NC>(hist2 + 2 * pl + o, vy2, commit_m);
+                }
                 if (s == lis_y && lis_here) {
                     float pv = pn2[0];
 #pragma unroll
@@ -1288,6 +1246,22 @@ cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* til
         quad_kernel<2, 2, 8, 0, true, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else if (shape == 17)
         quad_kernel<16, 4, 4, 0, true, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+int history2_shape(int64_t cells) { return cells < 200000 ? 42 : 36; }
+
+cudaError_t launch_step_history2(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
+                                 int local, cudaStream_t stream) {
+    // the two-step shapes 36 (32-row strips, 4 warps per CTA) and 42 (2-row
+    // strips, 2 warps) of the table, storing the history of both steps
+    if (ntiles <= 0) return cudaSuccess;
+    if (shape == 36)
+        quad2_kernel<32, 4, 4, 2, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else if (shape == 42)
+        quad2_kernel<2, 2, 8, 2, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
