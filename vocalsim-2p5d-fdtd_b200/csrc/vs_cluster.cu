@@ -411,7 +411,7 @@ __host__ __device__ inline RegLayout reg_layout(int pitch, int nthreads, int rma
     L.eP = take((size_t)(L.nw + 1) * (rmax + 1) * sizeof(float));
     L.tab = take(fast ? 2 * kDescEntries * sizeof(float4) : 0);
     L.sig = take(16 * sizeof(float));
-    L.exe = take(4 * sizeof(float));
+    L.exe = take(8 * sizeof(float));
     L.tmm = take(sizeof(TmmSlot));
     L.bar = take(2 * sizeof(uint64_t));
     L.exr = take(kExeRing * sizeof(float2));
@@ -419,9 +419,31 @@ __host__ __device__ inline RegLayout reg_layout(int pitch, int nthreads, int rma
     return L;
 }
 
-template <bool FAST, int RMAX, int MAXT, bool P2P>
-__global__ void __launch_bounds__(MAXT, 1)
+// Named barrier 1 over the first `count` threads of the CTA (the column
+// warps), plain and with an OR reduction.
+__device__ __forceinline__ void cols_sync(int count) { asm volatile("bar.sync 1, %0;" ::"r"(count) : "memory"); }
+
+__device__ __forceinline__ int cols_sync_or(int count, int pred) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.s32 p, %2, 0;\n\t"
+        "bar.red.or.pred q, 1, %1, p;\n\t"
+        "selp.s32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(count), "r"(pred)
+        : "memory");
+    return r;
+}
+
+// SYNC: 0 = cluster barrier per step, 1 = point to point, 2 = point to point
+// with the two-mass model in an extra warp (launched with MAXT + 32 threads;
+// the extra warp's registers come out of every thread's budget, so this
+// variant is only used for two-mass tubes)
+template <bool FAST, int RMAX, int MAXT, int SYNC>
+__global__ void __launch_bounds__(SYNC == 2 ? MAXT + 32 : MAXT, 1)
 cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_t nsteps) {
+    constexpr bool P2P = SYNC >= 1;
     extern __shared__ __align__(16) unsigned char r_smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int C = (int)cluster.num_blocks();
@@ -429,6 +451,10 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const TubeDev* __restrict__ T = Tp;
     const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
     const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    // point to point with the two-mass source: the last warp runs the model
+    // (two_mass_warp); the column warps are the ones before it
+    const bool two_mass_warp = SYNC == 2 && (T->flags & TUBE_TMM);
+    const int ncols = two_mass_warp ? nthr - 32 : nthr;
     const RegLayout L = reg_layout(pitch, nthr, RMAX, FAST);
     float2* gT = reinterpret_cast<float2*>(r_smem + L.gT);     // [2][pitch] ghost top (Vx, Vy)
     float* gVyB = reinterpret_cast<float*>(r_smem + L.gVyB);   // [2][pitch] ghost bottom Vy
@@ -455,7 +481,7 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const float* __restrict__ gP = T->P[0] + par0 * pl;
     const float* __restrict__ gdP = T->dP;
     const int c = tid + 1;                                     // this thread's column
-    const bool mine = c <= W - 2;                              // an interior column
+    const bool mine = c <= W - 2 && tid < ncols;               // an interior column
     const int cc = c < pitch ? c : pitch - 1;                  // clamped for the loads
 
     // ---- state, maps and codes of this column (rows r0-1 .. r1, and r1+1 for Vy / dY)
@@ -531,9 +557,13 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const bool tmm = flags & TUBE_TMM, tmm64 = flags & TUBE_TMM64;
     const bool exc_owner = tmm && T->exc_y >= r0 && T->exc_y <= r1;
     const int exc_i = T->exc_y - (r0 - 1), exc_x = T->exc_x;
-    const bool tmm_thread = exc_owner && tid == nthr - 1;
-    // the excitation cell's column owner publishes its P' for the two-mass thread
+    const bool tmm_thread = exc_owner && tid == (two_mass_warp ? ncols : nthr - 1);
+    // the excitation cell's column owner publishes its P' for the two-mass thread;
+    // for the two-mass warp as tagged words (P bits | step << 32) by step parity
+    // in sExe[4..7] (the owner writes step n + 2 only after the warp sent the
+    // excitation value of step n + 1, which needed the word of step n)
     float* sPexc = sExe + 2;
+    volatile unsigned long long* pexw = reinterpret_cast<volatile unsigned long long*>(sExe + 4);
     TmmSlot* slot = reinterpret_cast<TmmSlot*>(r_smem + L.tmm);
     if (tmm_thread) {
         if (tmm64) slot->s64 = T->tmm64[par0];
@@ -546,12 +576,20 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     };
     // P at the excitation cell, from its column owner
     auto publish_pexc = [&]() {
-        if (exc_owner && c == exc_x) {
+        if (exc_owner && c == exc_x && tid < ncols) {
 #pragma unroll
             for (int i = 1; i <= RMAX; ++i)
                 if (i == exc_i) *sPexc = P[i];
         }
     };
+    auto publish_pexc_tagged = [&](int64_t m) {
+        if (exc_owner && c == exc_x && tid < ncols) {
+#pragma unroll
+            for (int i = 1; i <= RMAX; ++i)
+                if (i == exc_i) pexw[m & 1] = ((unsigned long long)(uint32_t)m << 32) | __float_as_uint(P[i]);
+        }
+    };
+    if (tid < 2) pexw[tid] = 0xffffffff00000000ull;               // tag: no step
     // the two-mass value of step m into every CTA's ring slot, tagged with m
     auto send_exe_ring = [&](int64_t m, float e) {
         const unsigned long long v = ((unsigned long long)(uint32_t)m << 32) | __float_as_uint(e);
@@ -596,7 +634,7 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const int ifirst = r0 == 1 ? 1 : 0;          // the ring row above the first band is never computed
     constexpr unsigned kAll = 0xffffffffu;
 
-    for (int64_t n = n0; n < n_end; ++n) {
+    for (int64_t n = n0; n < n_end && tid < ncols; ++n) {
         const int p = (int)(n & 1), q = p ^ 1;
         // the table value of the next step, loaded while this step runs
         const float src_next = (P2P && !tmm && tid == 0 && n + 1 < n_end && n + 1 < T->src_len) ? T->src[n + 1]
@@ -662,9 +700,10 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
                 if (i <= Rk) prow(ic, i == Rk ? vyb : VY[i + 1 <= RMAX ? i + 1 : RMAX]);
             });
         }
-        publish_pexc();
+        if (two_mass_warp) publish_pexc_tagged(n);
+        else publish_pexc();
         if (P2P) {
-            // this step's two-mass value from the ring slot its thread filled
+            // this step's two-mass value from the ring slot its warp filled
             if (tid == 0 && tmm) {
                 const volatile unsigned long long* e = exr + (n & (kExeRing - 1));
                 unsigned long long v = *e;
@@ -672,14 +711,11 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
                 if ((uint32_t)(v >> 32) == (uint32_t)n) sExe[p] = __uint_as_float((uint32_t)v);
                 else bad = 1;
             }
-            if (__syncthreads_or(bad)) {
+            if (cols_sync_or(ncols, bad)) {
                 fail = true;
                 break;
             }
-            if (n + 1 < n_end) {
-                if (tmm_thread) send_exe_ring(n + 1, tmm_finish_next(*sPexc));
-                else if (!tmm && tid == 0) sExe[q] = src_next;
-            }
+            if (n + 1 < n_end && !tmm && tid == 0) sExe[q] = src_next;
         } else {
             __syncthreads();
             if (n + 1 < n_end) {
@@ -748,19 +784,32 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
             // one thread arrives on the barrier of the next step's ghosts, expecting
             // the bytes both neighbours send; the block barrier publishes the edges
             if (n + 1 < n_end && tid == 0) mbar_expect_tx(bar + q, expect);
-            if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
-            __syncthreads();
+            cols_sync(ncols);
         } else {
             asm volatile("barrier.cluster.arrive.release;" ::: "memory");
             if (tmm_thread && n + 2 < n_end) tmm_prepare_next();
             asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
         }
     }
+    if (two_mass_warp && tmm_thread) {
+        // the two-mass warp: the excitation value of step n + 1 from the
+        // owner's P' of step n, then the state-only part of the next step
+        for (int64_t n = n0; n + 1 < n_end; ++n) {
+            unsigned long long v = pexw[n & 1];
+            for (uint32_t i = 1; (uint32_t)(v >> 32) != (uint32_t)n && i < limit; ++i) v = pexw[n & 1];
+            if ((uint32_t)(v >> 32) != (uint32_t)n) {
+                fail = true;
+                break;
+            }
+            send_exe_ring(n + 1, tmm_finish_next(__uint_as_float((uint32_t)v)));
+            if (n + 2 < n_end) tmm_prepare_next();
+        }
+    }
     if (P2P) {
         if (fail) {
             // a neighbour may still be sending: give its stores time to land
             // before the CTAs meet, and leave the state as it is
-            if (tid == 0) atomicExch(&rs->error, VS_ERR_TIMEOUT);
+            if (tid == 0 || tmm_thread) atomicExch(&rs->error, VS_ERR_TIMEOUT);
             for (int i = 0; i < 64; ++i) __nanosleep(1000);
         }
         cluster.sync();                          // no CTA exits while another may store into it
@@ -798,37 +847,43 @@ namespace {
 // The register form is compiled for at most 4 or 8 rows per band and 256 or
 // 512 threads per CTA (a thread per column; 256 threads leave 255 registers
 // per thread).
-template <bool FAST, bool P2P>
-const void* reg_fn(int rmax, int threads) {
-    if (rmax <= 4) return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 4, 256, P2P>
-                                         : (const void*)cluster_reg_kernel<FAST, 4, 512, P2P>;
-    return threads <= 256 ? (const void*)cluster_reg_kernel<FAST, 8, 256, P2P>
-                          : (const void*)cluster_reg_kernel<FAST, 8, 512, P2P>;
+template <bool FAST, int SYNC>
+const void* reg_fn(int rmax, int cols) {
+    if (rmax <= 4) return cols <= 256 ? (const void*)cluster_reg_kernel<FAST, 4, 256, SYNC>
+                                      : (const void*)cluster_reg_kernel<FAST, 4, 512, SYNC>;
+    return cols <= 256 ? (const void*)cluster_reg_kernel<FAST, 8, 256, SYNC>
+                       : (const void*)cluster_reg_kernel<FAST, 8, 512, SYNC>;
 }
 
-// form 0: shared-memory bands; 1: register form, cluster barrier per step;
-// 2: register form, point-to-point neighbour exchange
-const void* cluster_fn(bool fast, int form, int rmax, int threads) {
+// form 0: shared-memory bands; register form with 1: a cluster barrier per
+// step, 2: the point-to-point neighbour exchange, 3: the exchange and the
+// two-mass model in its own warp
+const void* cluster_fn(bool fast, int form, int rmax, int cols) {
     if (form == 0) return fast ? (const void*)cluster_kernel<true> : (const void*)cluster_kernel<false>;
-    if (form == 1) return fast ? reg_fn<true, false>(rmax, threads) : reg_fn<false, false>(rmax, threads);
-    return fast ? reg_fn<true, true>(rmax, threads) : reg_fn<false, true>(rmax, threads);
+    if (form == 1) return fast ? reg_fn<true, 0>(rmax, cols) : reg_fn<false, 0>(rmax, cols);
+    if (form == 2) return fast ? reg_fn<true, 1>(rmax, cols) : reg_fn<false, 1>(rmax, cols);
+    return fast ? reg_fn<true, 2>(rmax, cols) : reg_fn<false, 2>(rmax, cols);
 }
 
-template <bool FAST, bool P2P>
-cudaError_t launch_reg(const cudaLaunchConfig_t& cfg, int rmax, int threads, const TubeDev* tube, RunState* rs,
+template <bool FAST, int SYNC>
+cudaError_t launch_reg(const cudaLaunchConfig_t& cfg, int rmax, int cols, const TubeDev* tube, RunState* rs,
                        int64_t steps) {
     if (rmax <= 4)
-        return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 256, P2P>, tube, rs, steps)
-                              : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 512, P2P>, tube, rs, steps);
-    return threads <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 256, P2P>, tube, rs, steps)
-                          : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 512, P2P>, tube, rs, steps);
+        return cols <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 256, SYNC>, tube, rs, steps)
+                           : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 4, 512, SYNC>, tube, rs, steps);
+    return cols <= 256 ? cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 256, SYNC>, tube, rs, steps)
+                       : cudaLaunchKernelEx(&cfg, cluster_reg_kernel<FAST, 8, 512, SYNC>, tube, rs, steps);
 }
 
-// The register form's step synchronisation: point to point (form 2) for
-// table sources, except the exact arithmetic's 512-thread variants (which
-// spill, and measured slower that way), else the cluster barrier (form 1):
-// the two-mass source's per-step broadcast measured faster with the barrier.
-int reg_form(bool fast, bool tmm, int threads) { return !tmm && (fast || threads <= 256) ? 2 : 1; }
+// The register form's step synchronisation: point to point (form 2), or for
+// two-mass tubes point to point with the model in its own warp (form 3, up
+// to 256 columns: the extra warp lowers every thread's register budget), else
+// the cluster barrier (form 1).  The exact arithmetic's 512-column variants
+// spill and measured slower point to point.
+int reg_form(bool fast, bool tmm, int cols) {
+    if (tmm) return cols <= 256 ? 3 : 1;
+    return fast || cols <= 256 ? 2 : 1;
+}
 
 }  // namespace
 
@@ -838,15 +893,16 @@ bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig*
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
-    const int threads = std::min(512, (W + 31) / 32 * 32);
+    const int cols = std::min(512, (W + 31) / 32 * 32);     // a thread per column
     for (int C : {16, 8, 4}) {
         if (C > NR) continue;
         const int R = (NR + C - 1) / C;
         // the register-resident form where a band has at most 8 rows and a
         // thread per column fits a CTA, the shared-memory form otherwise
-        const int form = (R <= 8 && W <= 512) ? reg_form(fast, tmm, threads) : 0;
+        const int form = (R <= 8 && W <= 512) ? reg_form(fast, tmm, cols) : 0;
         const int rmax = R <= 4 ? 4 : 8;
-        const void* fn = cluster_fn(fast, form, rmax, threads);
+        const int threads = cols + (form == 3 ? 32 : 0);         // + the two-mass warp
+        const void* fn = cluster_fn(fast, form, rmax, cols);
         const size_t smem = form ? reg_layout(pitch, threads, rmax, fast).bytes : cluster_layout(pitch, R, fast).bytes;
         if (smem > (size_t)optin) continue;
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) continue;
@@ -870,6 +926,7 @@ bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig*
         }
         out->ctas = C;
         out->threads = threads;
+        out->cols = cols;
         out->rows_max = R;
         out->smem = smem;
         out->form = form;
@@ -896,11 +953,14 @@ cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (c.form == 1)
-        return fast ? launch_reg<true, false>(cfg, c.rmax, c.threads, tube, rs, steps)
-                    : launch_reg<false, false>(cfg, c.rmax, c.threads, tube, rs, steps);
+        return fast ? launch_reg<true, 0>(cfg, c.rmax, c.cols, tube, rs, steps)
+                    : launch_reg<false, 0>(cfg, c.rmax, c.cols, tube, rs, steps);
     if (c.form == 2)
-        return fast ? launch_reg<true, true>(cfg, c.rmax, c.threads, tube, rs, steps)
-                    : launch_reg<false, true>(cfg, c.rmax, c.threads, tube, rs, steps);
+        return fast ? launch_reg<true, 1>(cfg, c.rmax, c.cols, tube, rs, steps)
+                    : launch_reg<false, 1>(cfg, c.rmax, c.cols, tube, rs, steps);
+    if (c.form == 3)
+        return fast ? launch_reg<true, 2>(cfg, c.rmax, c.cols, tube, rs, steps)
+                    : launch_reg<false, 2>(cfg, c.rmax, c.cols, tube, rs, steps);
     if (fast) return cudaLaunchKernelEx(&cfg, cluster_kernel<true>, tube, rs, steps, c.rows_max);
     return cudaLaunchKernelEx(&cfg, cluster_kernel<false>, tube, rs, steps, c.rows_max);
 }

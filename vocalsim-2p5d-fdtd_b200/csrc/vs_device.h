@@ -179,9 +179,11 @@ int cluster_shape();
 // Launch configuration of the cluster kernel for one tube.
 struct ClusterConfig {
     int ctas = 0, threads = 0, rows_max = 0;
+    int cols = 0;         // column threads (threads less the two-mass warp of form 2)
     size_t smem = 0;
     int form = 0;         // 0: band in shared memory; 1: register-resident columns (rows_max <= rmax),
-                          // cluster barrier per step; 2: the same, neighbour-to-neighbour exchange
+                          // cluster barrier per step; 2: the same, neighbour-to-neighbour exchange;
+                          // 3: form 2 with the two-mass model in an extra warp
     int rmax = 0;
 };
 // Cluster size (16, 8 or 4 CTAs), threads and shared memory for a tube of
