@@ -419,12 +419,13 @@ def run_b200(args, rank, world):
     cells = batch.interior_cells
     sim_steps = args.sim_steps
     if args.profile_adjoint:
-        # profiling workload of the reverse sweep: 16 stable fs x 30 tubes,
-        # checkpointed forward + adjoint over `profile_adjoint` steps
+        # profiling workload of the reverse sweep: 16 stable fs x 30 tubes in
+        # the bench's arithmetic, checkpointed forward + adjoint over
+        # `profile_adjoint` steps
         from vocalsim_b200 import synthetic as S
         seeds = [1, 2, 3, 5, 6, 8, 9, 11, 14, 16, 17, 18, 19, 20, 21, 22]
         k = args.profile_adjoint
-        pa = [V.params(cross_sectional_shape=2, srate_mul=30, num_steps=k) for _ in seeds]
+        pa = [V.params(cross_sectional_shape=2, srate_mul=30, num_steps=k, fast_math=fast) for _ in seeds]
         ga = [V.Geometry(*S.batch_tube(sd)[:2]) for sd in seeds]
         ba = V.Batch(pa, ga)
         tr = ba.forward_ckpt(k, 512)
