@@ -327,6 +327,16 @@ int vs_audio_filter(int32_t srate_mul, double* b3, double* a3);
 int vs_batch_set_maps(vs_batch* b, int32_t tube, const float* depth_p, const float* depth_x,
                       const float* depth_y, float z_inv);
 
+/* The maps tube i steps with, read back from the device (frameH*frameW each,
+ * host buffers, NULL skips one), in the layout of vs_build_maps: cell types,
+ * depth_p / depth_x / depth_y and the z_inv map.  Circular and elliptical
+ * tube sections are painted on the device at vs_batch_create (the batched map
+ * builder, FDTDSolver::setupWaveSolver's setup kernels restated); the
+ * open-space domain and single-plane-symmetric sections are built on the
+ * host.  Either way the values are vs_build_maps's bit for bit. */
+int vs_batch_get_maps(const vs_batch* b, int32_t tube, int32_t* cell_type, float* depth_p, float* depth_x,
+                      float* depth_y, float* z_inv);
+
 /* Forward `steps` steps from rest, keeping a state checkpoint every
  * ckpt_every steps for vs_batch_adjoint; traces (host, n x steps) may be NULL. */
 int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces);

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
               f"-I{INCLUDE}", "-Wno-deprecated-gpu-targets"]
 
-SOURCES = ["vs_grid.cpp", "vs_capi.cpp", "vs_step.cu", "vs_cluster.cu", "vs_noalloc.cu", "vs_adjoint.cu", "vs_spectrum.cu",
+SOURCES = ["vs_grid.cpp", "vs_capi.cpp", "vs_step.cu", "vs_cluster.cu", "vs_noalloc.cu", "vs_adjoint.cu", "vs_mapbuild.cu", "vs_spectrum.cu",
            "vs_sections.cu", "vs_audio.cu", "vs_shapes.cpp"]
 
 

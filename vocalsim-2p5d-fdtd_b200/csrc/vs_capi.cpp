@@ -502,6 +502,126 @@ void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vecto
     }
 }
 
+// Paint the maps of every device-built tube (TubeGrid::device_maps) into its
+// arena planes with the device map builder, then bring the code planes back
+// to the host, where the strip lists, the fast_math descriptors and the
+// adjoint's tables are derived from them.  The state planes P[0], P[1] serve
+// as the builder's scratch (reset_state zeroes them afterwards).
+void build_maps_on_device(vs_batch* b) {
+    std::vector<size_t> which;
+    for (size_t i = 0; i < b->grids.size(); ++i)
+        if (b->grids[i].device_maps) which.push_back(i);
+    if (which.empty()) return;
+    // per tube: up, down, utop, dbot, seg (L ints each), then the minor axes
+    std::vector<size_t> ioff(which.size()), foff(which.size());
+    size_t ni = 0, nf = 0;
+    for (size_t j = 0; j < which.size(); ++j) {
+        const TubeGrid& g = b->grids[which[j]];
+        ioff[j] = ni;
+        ni += 5 * g.upper.size();
+        foff[j] = nf;
+        nf += std::max<size_t>(g.minor_m.size(), 1);
+    }
+    std::vector<int32_t> ibuf(ni);
+    std::vector<float> fbuf(nf, 0.0f);
+    for (size_t j = 0; j < which.size(); ++j) {
+        const TubeGrid& g = b->grids[which[j]];
+        const size_t L = g.upper.size();
+        int32_t* d = ibuf.data() + ioff[j];
+        std::copy(g.upper.begin(), g.upper.end(), d);
+        std::copy(g.lower.begin(), g.lower.end(), d + L);
+        std::copy(g.upper_top.begin(), g.upper_top.end(), d + 2 * L);
+        std::copy(g.lower_bot.begin(), g.lower_bot.end(), d + 3 * L);
+        std::copy(g.colseg.begin(), g.colseg.end(), d + 4 * L);
+        std::copy(g.minor_m.begin(), g.minor_m.end(), fbuf.begin() + (long)foff[j]);
+    }
+    int32_t* d_i = nullptr;
+    float* d_f = nullptr;
+    MapBuild* d_m = nullptr;
+    int* d_err = nullptr;
+    auto release = [&] {
+        cudaFree(d_i);
+        cudaFree(d_f);
+        cudaFree(d_m);
+        cudaFree(d_err);
+    };
+    try {
+        ck(cudaMalloc(&d_i, std::max<size_t>(ni, 1) * sizeof(int32_t)), "cudaMalloc(map columns)");
+        ck(cudaMalloc(&d_f, nf * sizeof(float)), "cudaMalloc(map sections)");
+        ck(cudaMalloc(&d_m, which.size() * sizeof(MapBuild)), "cudaMalloc(map tubes)");
+        ck(cudaMalloc(&d_err, sizeof(int)), "cudaMalloc(map status)");
+        ck(cudaMemsetAsync(d_err, 0, sizeof(int), b->stream), "zero map status");
+        ck(cudaMemcpyAsync(d_i, ibuf.data(), ni * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream),
+           "upload map columns");
+        ck(cudaMemcpyAsync(d_f, fbuf.data(), nf * sizeof(float), cudaMemcpyHostToDevice, b->stream),
+           "upload map sections");
+        std::vector<MapBuild> mb(which.size());
+        int64_t max_cells = 0;
+        for (size_t j = 0; j < which.size(); ++j) {
+            const TubeGrid& g = b->grids[which[j]];
+            const TubeDev& t = b->h_tubes[which[j]];
+            const vs_params& p = g.src_params;
+            const int L = (int)g.upper.size();
+            MapBuild& m = mb[j];
+            m.H = g.H; m.W = g.W; m.pitch = g.pitch;
+            m.sx = g.dims.tube_start_x; m.L = L; m.my = g.dims.tube_mid_y; m.ex = g.dims.tube_end_x;
+            m.npc = g.dirichlet ? g.dims.tube_end_x + 1 : -1;
+            m.pml = g.pml_layers;
+            m.depth = p.fdtd_solver_type != 1 ? MAP_DEPTH_NONE
+                      : p.cross_sectional_shape == 2 ? MAP_DEPTH_ELLIPSE : MAP_DEPTH_CIRCLE;
+            m.depth_fma = p.depth_fma;
+            m.ds = g.dims.ds;
+            m.ud = p.uniform_depth_m;
+            const int32_t* c = d_i + ioff[j];
+            m.up = c; m.down = c + L; m.utop = c + 2 * L; m.dbot = c + 3 * L; m.seg = c + 4 * L;
+            m.minor = d_f + foff[j];
+            m.dP = const_cast<float*>(t.dP);
+            m.dX = const_cast<float*>(t.dX);
+            m.dY = const_cast<float*>(t.dY);
+            m.code = const_cast<uint8_t*>(t.code);
+            m.tmpx = t.P[0];
+            m.tmpy = t.P[1];
+            max_cells = std::max<int64_t>(max_cells, (int64_t)g.H * g.pitch);
+        }
+        ck(cudaMemcpyAsync(d_m, mb.data(), mb.size() * sizeof(MapBuild), cudaMemcpyHostToDevice, b->stream),
+           "upload map tubes");
+        ck(launch_build_maps(d_m, (int)which.size(), max_cells, d_err, b->stream), "map builder");
+        int err = 0;
+        ck(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream), "read map status");
+        for (size_t j = 0; j < which.size(); ++j) {
+            TubeGrid& g = b->grids[which[j]];
+            g.code.resize((size_t)g.H * g.pitch);
+            ck(cudaMemcpyAsync(g.code.data(), b->h_tubes[which[j]].code, g.code.size(), cudaMemcpyDeviceToHost,
+                               b->stream),
+               "read codes");
+        }
+        ck(cudaStreamSynchronize(b->stream), "map builder sync");
+        if (err == VS_ERR_NEGATIVE_SQRT)
+            throw VsFailure{VS_ERR_NEGATIVE_SQRT, "negative radicand in the tube depth formula"};
+    } catch (...) {
+        release();
+        throw;
+    }
+    release();
+}
+
+// Host copies of a device-built tube's depth maps (frame-shaped), for the
+// paths that edit them on the host.
+void fetch_device_maps(vs_batch* b, size_t i) {
+    TubeGrid& g = b->grids[i];
+    if (!g.device_maps || !g.dP.empty()) return;
+    const TubeDev& t = b->h_tubes[i];
+    const size_t n = (size_t)g.H * g.W;
+    g.dP.resize(n);
+    g.dX.resize(n);
+    g.dY.resize(n);
+    for (auto [dst, src] : {std::pair<float*, const float*>{g.dP.data(), t.dP}, {g.dX.data(), t.dX},
+                            {g.dY.data(), t.dY}})
+        ck(cudaMemcpy2D(dst, g.W * sizeof(float), src, g.pitch * sizeof(float), g.W * sizeof(float), g.H,
+                        cudaMemcpyDeviceToHost),
+           "read depth maps");
+}
+
 // Depth planes, code bytes (and fast_math descriptors) of tube i, padded to
 // the row pitch.
 void upload_static_tube(vs_batch* b, size_t i) {
@@ -546,6 +666,18 @@ void upload_static(vs_batch* b) {
         auto at = [&](const void* p) { return (size_t)(reinterpret_cast<const char*>(p) - base); };
         const size_t end = b->fast ? at(t.desc_b) + kDescTableBytes / 2 : at(t.code) + align_up((size_t)g.H * g.pitch);
         std::vector<char>& m = img[i];
+        if (g.device_maps) {
+            // the planes and codes are on the device already: the descriptors only
+            if (!b->fast) return;
+            m.assign(end, 0);
+            std::vector<uint8_t> desc;
+            std::vector<float> ta, tb;
+            build_descriptors(g, desc, ta, tb);
+            std::memcpy(m.data() + at(t.desc), desc.data(), desc.size());
+            std::memcpy(m.data() + at(t.desc_a), ta.data(), ta.size() * sizeof(float));
+            std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
+            return;
+        }
         m.assign(end, 0);
         auto plane = [&](const std::vector<float>& src, const float* dst) {
             float* d = reinterpret_cast<float*>(m.data() + at(dst));
@@ -565,9 +697,15 @@ void upload_static(vs_batch* b) {
             std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
         }
     });
-    for (size_t i = 0; i < n; ++i)
-        ck(cudaMemcpy((void*)b->h_tubes[i].dP, img[i].data(), img[i].size(), cudaMemcpyHostToDevice),
+    for (size_t i = 0; i < n; ++i) {
+        if (img[i].empty()) continue;
+        const TubeDev& t = b->h_tubes[i];
+        const char* base = reinterpret_cast<const char*>(t.dP);
+        // a device-built tube's image starts at its descriptors
+        const size_t from = b->grids[i].device_maps ? (size_t)(reinterpret_cast<const char*>(t.desc) - base) : 0;
+        ck(cudaMemcpy((void*)(base + from), img[i].data() + from, img[i].size() - from, cudaMemcpyHostToDevice),
            "upload maps");
+    }
 }
 
 void reset_state(vs_batch* b) {
@@ -586,8 +724,11 @@ void reset_state(vs_batch* b) {
 void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_batch* b) {
     ck(cudaGetDevice(&b->device), "cudaGetDevice");
     b->grids.resize(n);
+    // tubes the device map builder covers get only their per-column data on
+    // the host; their maps are painted on the device (build_maps_on_device)
     parallel_for((size_t)n, [&](size_t i) {
-        build_tube(&params[i], geoms ? &geoms[i] : nullptr, b->grids[i], 0);
+        if (device_buildable(&params[i])) build_tube_columns(&params[i], geoms ? &geoms[i] : nullptr, b->grids[i], 0);
+        else build_tube(&params[i], geoms ? &geoms[i] : nullptr, b->grids[i], 0);
         std::memcpy(&b->grids[i].src_params, &params[i], sizeof(vs_params));
     });
     // arena layout: per tube, planes of H*pitch floats (+ codes) + two-mass
@@ -666,6 +807,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
     int64_t need = 0;
     for (const TubeGrid& g : b->grids) need = std::max<int64_t>(need, g.dims.num_steps);
     upload_sources(b, need);
+    build_maps_on_device(b);
     upload_static(b);
     reset_state(b);
     // small grids (a single tube) need short strips to spread over the SMs
@@ -1322,6 +1464,7 @@ void section_gradients(vs_batch* b, double* dwidth, double* ddepth) {
 }
 
 void set_maps(vs_batch* b, int i, const float* dP, const float* dX, const float* dY, float zinv) {
+    fetch_device_maps(b, (size_t)i);
     TubeGrid& g = b->grids[i];
     const size_t n = (size_t)g.H * g.W;
     if (dP) std::memcpy(g.dP.data(), dP, n * sizeof(float));
@@ -1553,6 +1696,28 @@ int vs_batch_set_maps(vs_batch* b, int32_t tube, const float* depth_p, const flo
                       float z_inv) {
     if (!b || tube < 0 || tube >= (int)b->grids.size()) return set_error(VS_ERR_INVALID_ARG, "vs_batch_set_maps");
     return guarded([&] { set_maps(b, tube, depth_p, depth_x, depth_y, z_inv); });
+}
+
+int vs_batch_get_maps(const vs_batch* b, int32_t tube, int32_t* cell_type, float* depth_p, float* depth_x,
+                      float* depth_y, float* z_inv) {
+    if (!b || tube < 0 || tube >= (int)b->grids.size()) return set_error(VS_ERR_INVALID_ARG, "vs_batch_get_maps");
+    return guarded([&] {
+        const TubeGrid& g = b->grids[tube];
+        const TubeDev& t = b->h_tubes[tube];
+        ck(cudaStreamSynchronize(b->stream), "sync");
+        const size_t row = g.W * sizeof(float), dpitch = g.pitch * sizeof(float);
+        if (depth_p) ck(cudaMemcpy2D(depth_p, row, t.dP, dpitch, row, g.H, cudaMemcpyDeviceToHost), "read depth_p");
+        if (depth_x) ck(cudaMemcpy2D(depth_x, row, t.dX, dpitch, row, g.H, cudaMemcpyDeviceToHost), "read depth_x");
+        if (depth_y) ck(cudaMemcpy2D(depth_y, row, t.dY, dpitch, row, g.H, cudaMemcpyDeviceToHost), "read depth_y");
+        if (cell_type || z_inv) {
+            std::vector<uint8_t> code((size_t)g.H * g.W);
+            ck(cudaMemcpy2D(code.data(), g.W, t.code, g.pitch, g.W, g.H, cudaMemcpyDeviceToHost), "read codes");
+            for (size_t k = 0; k < code.size(); ++k) {
+                if (cell_type) cell_type[k] = code[k] & CODE_TYPE_MASK;
+                if (z_inv) z_inv[k] = (code[k] & CODE_ZINV_BIT) ? t.zinv : 0.0f;
+            }
+        }
+    });
 }
 
 int vs_batch_set_sections(vs_batch* b, const double* width_m, const double* depth_m, const double* z_inv) {

@@ -295,6 +295,38 @@ int adjoint_strip_blocks(int strips);                   // CTAs those strips tak
 // two-mass state into slot 0 of tmm_hist).
 cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_cells, int par, cudaStream_t stream);
 
+// ---- device map builder (vs_mapbuild.cu) ------------------------------------
+enum : int { MAP_DEPTH_NONE = 0, MAP_DEPTH_CIRCLE = 1, MAP_DEPTH_ELLIPSE = 2 };
+
+// One tube for the device map builder: the frame, the tube's columns (from
+// build_tube_columns) and the device planes to paint (row pitch `pitch`).
+struct MapBuild {
+    int H, W, pitch;
+    int sx, L, my, ex;        // first tube column, tube length in cells, axis row, last tube column
+    int npc;                  // the no-pressure column (Dirichlet mouth), or -1
+    int pml;                  // PML layers (0 or 6)
+    int depth;                // MAP_DEPTH_*: 2D solver (unit depths), circular or elliptical sections
+    int depth_fma;            // vs_params::depth_fma
+    float ds, ud;             // cell size, uniform depth (0: none)
+    const int32_t* up;        // per tube column: wall rows, the gap fill's extent, 0-based segment
+    const int32_t* down;
+    const int32_t* utop;
+    const int32_t* dbot;
+    const int32_t* seg;
+    const float* minor;       // per section: elliptical minor axis (m)
+    float* dP;
+    float* dX;
+    float* dY;
+    uint8_t* code;
+    float* tmpx;              // two scratch planes (H x pitch)
+    float* tmpy;
+};
+
+// Paint the maps of `ntubes` tubes (device array `tubes`); max_cells = the
+// largest H * pitch.  A negative depth radicand sets *err (device int) to
+// VS_ERR_NEGATIVE_SQRT.
+cudaError_t launch_build_maps(const MapBuild* tubes, int ntubes, int64_t max_cells, int* err, cudaStream_t stream);
+
 // ---- section depth model (vs_sections.cu) -----------------------------------
 // A frame cell the reference's elliptical depth kernel writes: its section,
 // the nominal semi-major axis a0 (m) of its column and its distance from the

@@ -106,16 +106,20 @@ struct Column {
 
 class Builder {
 public:
-    Builder(const vs_params* p, const vs_geometry* g, TubeGrid& out) : p_(*p), g_(g), T_(out) {}
+    // planes = false: columns only (build_tube_columns), no H x W vector
+    Builder(const vs_params* p, const vs_geometry* g, TubeGrid& out, bool planes = true)
+        : p_(*p), g_(g), T_(out), planes_(planes) {}
 
     void run() {
         validate();
         k_ = physics(p_.srate_mul);
         pml_ = kPmlLayers * p_.pml_flag;
+        T_.pml_layers = pml_;
+        T_.device_maps = !planes_;
         tables();
         if (p_.simulation_type == 0) open_space();
         else tube();
-        dead_ring_and_pml();
+        if (planes_) dead_ring_and_pml();
         listener_override();
         pack();
     }
@@ -124,6 +128,7 @@ private:
     const vs_params& p_;
     const vs_geometry* g_;
     TubeGrid& T_;
+    const bool planes_;
     Physics k_{};
     int pml_ = 0;
     std::vector<int> seg_;      // boundary_segment_type, H*W
@@ -170,10 +175,12 @@ private:
         if (H < 3 || W < 3 || (int64_t)H * W > (int64_t)1 << 28) raise(VS_ERR_GEOMETRY, "frame size out of range");
         T_.H = H; T_.W = W;
         size_t n = (size_t)H * W;
-        T_.cell_type.assign(n, VS_CELL_AIR);
-        seg_.assign(n, 0);
-        T_.zinv.assign(n, 0.0f);
-        T_.dP.assign(n, 1.0f); T_.dX.assign(n, 1.0f); T_.dY.assign(n, 1.0f);
+        if (planes_) {
+            T_.cell_type.assign(n, VS_CELL_AIR);
+            seg_.assign(n, 0);
+            T_.zinv.assign(n, 0.0f);
+            T_.dP.assign(n, 1.0f); T_.dX.assign(n, 1.0f); T_.dY.assign(n, 1.0f);
+        }
         T_.dims.frame_h = H; T_.dims.frame_w = W;
         T_.dims.interior_cells = (int64_t)(H - 2) * (W - 2);
     }
@@ -251,14 +258,38 @@ private:
             const int r = (dcell[s] - 1) / 2;
             col[i] = {my - r - 1, my + r + 1, s};
             if (col[i].up < 0 || col[i].down >= T_.H) raise(VS_ERR_GEOMETRY, "wall outside the frame");
+            if (!planes_) continue;
             type(col[i].up, sx + i) = VS_CELL_WALL;
             type(col[i].down, sx + i) = VS_CELL_WALL;
             seg(col[i].up, sx + i) = s + 1;
             seg(col[i].down, sx + i) = s + 1;
         }
+        // the wall-gap fill below paints, in column i, rows up[i-1] .. up[i]
+        // (and lower[i] .. lower[i-1]) when the upper wall drops by more than
+        // one row from column i-1 (i in 1..L-2), and rows up[i+1] .. up[i]
+        // (lower[i] .. lower[i+1]) when it rises by more than one row to
+        // column i+1 (i+1 in 1..L-2), always with the column's own segment id
+        // (the largest id in a column is its own); so each wall is one run of
+        // rows per column, which the device builder paints from these bounds
+        T_.upper_top.assign(L, 0);
+        T_.lower_bot.assign(L, 0);
+        for (int i = 0; i < L; ++i) {
+            int top = col[i].up, bot = col[i].down;
+            if (i >= 1 && i <= L - 2 && col[i].up - col[i - 1].up > 1) {
+                top = std::min(top, col[i - 1].up);
+                bot = std::max(bot, col[i - 1].down);
+            }
+            if (i + 1 >= 1 && i + 1 <= L - 2 && col[i + 1].up - col[i].up < -1) {
+                top = std::min(top, col[i + 1].up);
+                bot = std::max(bot, col[i + 1].down);
+            }
+            T_.upper_top[i] = top;
+            T_.lower_bot[i] = bot;
+        }
         // connectSagittalWallsGap (TubeGeometry.cu:496-569): sequential fill of
         // jumps larger than one row, columns 1..L-2
         auto column_max_seg = [&](int c) {
+            if (!planes_) return col[c - sx].seg + 1;     // the column's own id (see above)
             int m = 0;
             for (int r = 0; r < T_.H; ++r) m = std::max(m, seg(r, c));
             return m;
@@ -266,7 +297,7 @@ private:
         auto paint = [&](int c, int r0, int r1, int s) {
             for (int r = r0; r <= r1; ++r) { type(r, c) = VS_CELL_WALL; seg(r, c) = s; }
         };
-        for (int i = 1; i <= L - 2; ++i) {
+        for (int i = 1; i <= L - 2 && planes_; ++i) {
             const Column& a = col[i - 1];
             const Column& b = col[i];
             const int jump = b.up - a.up;
@@ -281,13 +312,16 @@ private:
             }
         }
         // setExcitationCells (TubeGeometry.cu:571-594)
-        for (int r = col[0].up + 1; r < col[0].down; ++r) type(r, sx - 1) = VS_CELL_EXCITATION;
-        type(col[0].up, sx - 1) = VS_CELL_WALL;
-        type(col[0].down, sx - 1) = VS_CELL_WALL;
+        if (planes_) {
+            for (int r = col[0].up + 1; r < col[0].down; ++r) type(r, sx - 1) = VS_CELL_EXCITATION;
+            type(col[0].up, sx - 1) = VS_CELL_WALL;
+            type(col[0].down, sx - 1) = VS_CELL_WALL;
+        }
         vs_dims& d = T_.dims;
         // listener / excitation (FDTDSolver.cu:591-611)
         if (dir) {
-            for (int r = col[L - 1].up; r <= col[L - 1].down; ++r) type(r, ex + 1) = VS_CELL_NOPRESSURE;
+            if (planes_)
+                for (int r = col[L - 1].up; r <= col[L - 1].down; ++r) type(r, ex + 1) = VS_CELL_NOPRESSURE;
             d.listener_x = ex - mic;
         } else {
             d.listener_x = ex + 3 + mic;
@@ -308,7 +342,7 @@ private:
         for (size_t i = 0; i < seg_.size(); ++i)
             if (seg_[i] != 0) T_.zinv[i] = T_.zinv_val;
 
-        if (p_.fdtd_solver_type == 1) depth(col, minor, sx, my, ex, column_max_seg);
+        if (p_.fdtd_solver_type == 1 && planes_) depth(col, minor, sx, my, ex, column_max_seg);
         (void)W;
         for (int i = 0; i < L; ++i) {
             T_.upper.push_back(col[i].up);
@@ -511,6 +545,7 @@ private:
         // Device planes are padded to a 32-element row pitch; padding cells are
         // dead and never updated.
         T_.pitch = (T_.W + 31) / 32 * 32;
+        if (!planes_) return;
         T_.code.assign((size_t)T_.H * T_.pitch, (uint8_t)VS_CELL_DEAD);
         for (int r = 0; r < T_.H; ++r)
             for (int c = 0; c < T_.W; ++c) {
@@ -620,6 +655,21 @@ static void fill_tmm(const vs_params* p, TubeGrid& out) {
 void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source) {
     if (!p) throw VsFailure{VS_ERR_INVALID_ARG, "null vs_params"};
     Builder(p, g, out).run();
+    const int64_t n = steps_for_source > 0 ? steps_for_source : out.dims.num_steps;
+    if (p->source_type == VS_SRC_TMM) out.source.clear();
+    else build_source(p, out.dt, n, out.source);
+    fill_tmm(p, out);
+}
+
+bool device_buildable(const vs_params* p) {
+    return p && p->simulation_type == 1 && (p->cross_sectional_shape == 1 || p->cross_sectional_shape == 2);
+}
+
+void build_tube_columns(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source) {
+    if (!p) throw VsFailure{VS_ERR_INVALID_ARG, "null vs_params"};
+    if (!device_buildable(p)) throw VsFailure{VS_ERR_UNSUPPORTED, "the device map builder covers circular and "
+                                                                   "elliptical tube sections"};
+    Builder(p, g, out, false).run();
     const int64_t n = steps_for_source > 0 ? steps_for_source : out.dims.num_steps;
     if (p->source_type == VS_SRC_TMM) out.source.clear();
     else build_source(p, out.dt, n, out.source);

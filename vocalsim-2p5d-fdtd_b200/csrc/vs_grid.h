@@ -69,6 +69,14 @@ struct TubeGrid {
     // tube rasterisation (empty for the open-space domain)
     std::vector<int32_t> upper, lower, colseg;   // per tube column: wall rows, 0-based segment
     std::vector<float> major_m, minor_m;         // per section: width used for walls, minor axis
+    // per tube column, after the wall-gap fill: the upper wall occupies rows
+    // upper_top .. upper, the lower wall lower .. lower_bot
+    std::vector<int32_t> upper_top, lower_bot;
+    int pml_layers = 0;                           // graded PML layers painted inside the dead ring
+    // the H x W vectors above (cell_type, code, zinv, dP, dX, dY) were not
+    // built on the host: the device map builder paints them from the column
+    // data (build_tube_columns)
+    bool device_maps = false;
 };
 
 // Fill p with the reference's defaults.
@@ -77,6 +85,18 @@ void default_params(vs_params* p);
 // Build a tube (or the open-space domain) exactly as FDTDSolver::setupWaveSolver.
 // `steps_for_source` > 0 sizes the source table; 0 uses dims.num_steps.
 void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source);
+
+// Whether the device map builder covers these parameters: a tube simulation
+// with circular or elliptical sections (not the open-space domain, not
+// single-plane-symmetric sections).
+bool device_buildable(const vs_params* p);
+
+// build_tube without any H x W map: the frame, the dims, the constants, the
+// source and the per-column wall data (upper, lower, upper_top, lower_bot,
+// colseg) that the device map builder paints the maps from
+// (out.device_maps = true).  Checks that need the maps (a negative depth
+// radicand) are made by the device builder.
+void build_tube_columns(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source);
 
 // Only the scalar constants and tables of a tube (K1, K2, bcoef, dt, the wall
 // parameters, sigma/beta/direction tables, two-mass constants and the flags

@@ -183,6 +183,20 @@ class Batch:
         ptrs = [None if a is None else _fp(a) for a in arrs]
         check(self.lib, self.lib.vs_batch_set_maps(self.h, tube, *ptrs, float(z_inv)), "vs_batch_set_maps")
 
+    def get_maps(self, tube: int) -> dict:
+        """The maps tube `tube` steps with, read back from the device:
+        cell_type, depth_p, depth_x, depth_y, z_inv (frame-shaped), as
+        build_maps returns them."""
+        d = self.dims[tube]
+        H, W = int(d["frame_h"]), int(d["frame_w"])
+        out = {"cell_type": np.zeros((H, W), np.int32)}
+        for k in ("depth_p", "depth_x", "depth_y", "z_inv"):
+            out[k] = np.zeros((H, W), np.float32)
+        check(self.lib, self.lib.vs_batch_get_maps(self.h, tube, out["cell_type"].ctypes.data_as(C.POINTER(C.c_int32)),
+                                                   _fp(out["depth_p"]), _fp(out["depth_x"]), _fp(out["depth_y"]),
+                                                   _fp(out["z_inv"])), "vs_batch_get_maps")
+        return out
+
     def forward_ckpt(self, steps: int, ckpt_every: int = 512) -> np.ndarray:
         """Forward from rest keeping checkpoints for adjoint(); returns (n, steps) traces."""
         tr = np.zeros((self.n, steps), np.float32)
