@@ -595,11 +595,18 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
     const int64_t n = ar.start + ar.len - 1 - local;    // stage 0 reverses step n, stage 1 step n - 1
     const int64_t slot = n - ar.start;                  // >= 1
     const int par = ar.q0 ^ (phase & 1);
+    // the tube's coefficient table (A.ndesc descriptors x 3 float4) in shared
+    // memory after the row rings, loaded once per block
+    constexpr int kSlots = kAdjDepth + 1;
+    constexpr int kStage = (kAdjPieces + 2 * kAdjGPieces) * 32 * NC;   // floats per stage
+    float4* stab = adj2_smem + WARPS * kSlots * kStage / 4;
+    if ((int)blockIdx.x * WARPS >= A.strips) return;                   // the whole block: no strip
+    for (int j = threadIdx.x; j < 3 * A.ndesc; j += WARPS * 32) stab[j] = __ldg(A.tab + j);
+    __syncthreads();
     const int s = (int)blockIdx.x * WARPS + (int)(threadIdx.x >> 5);
     if (s >= A.strips) return;
     constexpr unsigned kAll = 0xffffffffu;
     constexpr int kCommit = 30 * NC;
-    constexpr int kSlots = kAdjDepth + 1;
     const int lane = threadIdx.x & 31;
     const int W = T.W, H = T.H, pitch = T.pitch;
     const int nsx = (W - 2) / kCommit + 1;
@@ -625,7 +632,7 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
     const float* __restrict__ mP = T.dP;
     const uint8_t* __restrict__ dsc = A.desc;
     const uint8_t* __restrict__ code = T.code;
-    const float4* __restrict__ tab = A.tab;
+    const float4* tab = stab;
     const float K1 = T.K1;
     const int lis_y = T.lis_y, lis_q = T.lis_x - x0;
     const bool lis_col = lis_q >= 0 && lis_q < NC;
@@ -636,7 +643,6 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
     // dY(j+1), Vx_n(j), Vy_n(j+1), Vx_(n-1)(j-1), Vy_(n-1)(j) as floats, then gP, gX, gY of
     // row j-1 (the row stage 1 commits at iteration j) as doubles; this lane's float piece k
     // sits at stage + (k * 32 + lane) * NC, its double piece k at gstage + (k * 32 + lane) * NC
-    constexpr int kStage = (kAdjPieces + 2 * kAdjGPieces) * 32 * NC;   // floats per stage
     float* ring = reinterpret_cast<float*>(adj2_smem) + (threadIdx.x >> 5) * (kSlots * kStage);
     const int t_last = rlast - r0 + 3;                       // stage of row rlast + 1
     auto issue = [&](int t) {
@@ -722,9 +728,9 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
         float mu0[NC], q0[NC], bxl[NC], ux[NC], rD0[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
-            const float4 ea = __ldg(tab + 3 * byte_at(dc, q));
-            eb0[q] = __ldg(tab + 3 * byte_at(dc, q) + 1);
-            const float byd = __ldg(tab + 3 * byte_at(dd, q)).w;
+            const float4 ea = tab[3 * byte_at(dc, q)];
+            eb0[q] = tab[3 * byte_at(dc, q) + 1];
+            const float byd = tab[3 * byte_at(dd, q)].w;
             bxl[q] = ea.z * lXc[q];
             ux[q] = vxc[q] * dxc[q];
             mu0[q] = lPc[q] + ea.x * lXc[q] + ea.y * lYc[q] - byd * lYd[q];
@@ -763,7 +769,7 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
                 t0Y[q] = vyc[q] * lamW;
                 t0Z[q] = 0.0;
                 if (own0 && ((commit >> q) & 1u) && (byte_at(kc, q) & CODE_ZINV_BIT)) {
-                    const float4 ez = __ldg(tab + 3 * byte_at(dc, q) + 2);
+                    const float4 ez = tab[3 * byte_at(dc, q) + 2];
                     const float pc = pn[o + q], pr = pn[o + q + 1], pt = pn[o + q - pitch];
                     t0Z[q] = (double)(ez.x * pc - ez.y * pr) * (double)lXc[q] +
                              (double)(ez.z * pc - ez.w * pt) * (double)lYc[q];
@@ -779,9 +785,9 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
             float mu1[NC], q1[NC], bxl1[NC], wx[NC], rD1[NC];
 #pragma unroll
             for (int q = 0; q < NC; ++q) {
-                const float4 ea = __ldg(tab + 3 * byte_at(du, q));
-                eb1[q] = __ldg(tab + 3 * byte_at(du, q) + 1);
-                const float byd = __ldg(tab + 3 * byte_at(dc, q)).w;
+                const float4 ea = tab[3 * byte_at(du, q)];
+                eb1[q] = tab[3 * byte_at(du, q) + 1];
+                const float byd = tab[3 * byte_at(dc, q)].w;
                 bxl1[q] = ea.z * LXp[q];
                 wx[q] = wxu[q] * dxu[q];
                 mu1[q] = LPp[q] + ea.x * LXp[q] + ea.y * LYp[q] - byd * LYn[q];
@@ -831,7 +837,7 @@ adjoint2_kernel(const TubeDev* __restrict__ tubes, const AdjTube* __restrict__ a
                         if (byte_at(ku, q) & CODE_ZINV_BIT) {
                             // P after step n-1 is the P plane of the state before step n;
                             // both steps' z_inv terms go in with one read-modify-write
-                            const float4 ez = __ldg(tab + 3 * byte_at(du, q) + 2);
+                            const float4 ez = tab[3 * byte_at(du, q) + 2];
                             const float pc = hn[o1 + q], pr = hn[o1 + q + 1], pt = hn[o1 + q - pitch];
                             A.gZ[o1 + q] += h0Z[q] + ((double)(ez.x * pc - ez.y * pr) * (double)LXp[q] +
                                                       (double)(ez.z * pc - ez.w * pt) * (double)LYp[q]);
@@ -879,6 +885,12 @@ constexpr size_t adj2_smem_bytes(int nc, int warps) {
     return (size_t)warps * (kAdjDepth + 1) * (kAdjPieces + 2 * kAdjGPieces) * 32 * nc * sizeof(float);
 }
 
+// ... plus the coefficient table of up to kMaxAdjDescriptors descriptors.
+constexpr int kMaxAdjDescriptors = 256;
+constexpr size_t adj2_smem_max(int nc, int warps) {
+    return adj2_smem_bytes(nc, warps) + (size_t)kMaxAdjDescriptors * 3 * sizeof(float4);
+}
+
 constexpr int kAdjNC = 2, kAdjWarps = 4;
 
 // Slot 0 of every tube's history = the state before the first step of a
@@ -913,22 +925,34 @@ cudaError_t launch_history_seed(const TubeDev* tubes, int ntubes, int max_plane_
     return cudaGetLastError();
 }
 
+// The two-step kernel's shared memory (row rings + the coefficient table)
+// exceeds the default 48 KB: the attribute is set on every launch (it is per
+// device, and cheap; graph replays do not repeat it).
+template <int TR>
+cudaError_t launch_adj2(dim3 grid, const TubeDev* tubes, const AdjTube* adj, const AdjRun* run, int local,
+                        int phase, cudaStream_t stream) {
+    constexpr size_t smem = adj2_smem_max(kAdjNC, kAdjWarps);
+    static_assert(smem <= 200 * 1024, "two-step shared memory exceeds a third of the SM's");
+    const cudaError_t e = cudaFuncSetAttribute(adjoint2_kernel<kAdjNC, TR, kAdjWarps>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    adjoint2_kernel<kAdjNC, TR, kAdjWarps><<<grid, kAdjWarps * 32, smem, stream>>>(tubes, adj, run, local, phase);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_adjoint_step(const TubeDev* tubes, const AdjTube* adj, int ntubes, int max_blocks,
                                 const AdjRun* run, int local, int phase, cudaStream_t stream, int form,
                                 int rows) {
     const dim3 grid(max_blocks, ntubes);
     constexpr int kThreads = kAdjWarps * 32;
-    constexpr size_t kSmem2 = adj2_smem_bytes(kAdjNC, kAdjWarps);   // below the 48 KB default limit
-    static_assert(kSmem2 <= 48 * 1024, "two-step ring exceeds the default dynamic shared memory");
     if (form == ADJ_FORM_TILES) {
         adjoint_step_kernel<<<grid, kAdjTileW * kAdjTileH, 0, stream>>>(tubes, adj, run, local, phase);
     } else if (form == ADJ_FORM_STRIPS2) {
         if (rows == 4)
-            adjoint2_kernel<kAdjNC, 4, kAdjWarps><<<grid, kThreads, kSmem2, stream>>>(tubes, adj, run, local, phase);
-        else if (rows == 8)
-            adjoint2_kernel<kAdjNC, 8, kAdjWarps><<<grid, kThreads, kSmem2, stream>>>(tubes, adj, run, local, phase);
-        else
-            adjoint2_kernel<kAdjNC, 16, kAdjWarps><<<grid, kThreads, kSmem2, stream>>>(tubes, adj, run, local, phase);
+            return launch_adj2<4>(grid, tubes, adj, run, local, phase, stream);
+        if (rows == 8)
+            return launch_adj2<8>(grid, tubes, adj, run, local, phase, stream);
+        return launch_adj2<16>(grid, tubes, adj, run, local, phase, stream);
     } else {
         if (rows == 4)
             adjoint_strip_kernel<kAdjNC, 4, kAdjWarps><<<grid, kThreads, 0, stream>>>(tubes, adj, run, local, phase);

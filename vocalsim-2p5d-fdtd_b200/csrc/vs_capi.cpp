@@ -1051,6 +1051,7 @@ void adjoint_coefficients(const TubeGrid& g, std::vector<uint8_t>& desc, std::ve
         e[7] = (g.dirichlet && tc == VS_CELL_NOPRESSURE) ? 1.0f : 0.0f;
         e[8] = x.zc_out; e[9] = x.zc_in; e[10] = y.zc_out; e[11] = y.zc_in;
     }
+    tab.resize(12 * std::max<size_t>(key_of_id.size(), 1));     // the descriptors in use
 }
 
 void capture(vs_batch* b, cudaGraphExec_t* out, const char* what, const std::function<cudaError_t(int)>& launch,
@@ -1196,6 +1197,7 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
            "upload adjoint coefficient table");
         adj[i].desc = d_desc;
         adj[i].tab = reinterpret_cast<const float4*>(d_tab);
+        adj[i].ndesc = (int32_t)(atab[i].size() / 12);
         adj[i].exc_off = d_off;
         adj[i].exc_coef = d_coef;
         adj[i].n_exc = (int32_t)nb;

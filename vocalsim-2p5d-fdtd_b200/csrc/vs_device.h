@@ -245,6 +245,7 @@ struct AdjTube {
     int32_t n_exc;
     int32_t tiles;        // 32 x 8 cell tiles of the interior (tile form)
     int32_t strips;       // row-marching strips of the interior (strip forms)
+    int32_t ndesc;        // neighbourhood descriptors in use (entries of `tab`)
     // per-cell neighbourhood descriptors (H x pitch bytes) into a table of
     // three float4 per descriptor: (ax, ay, bx, by), (alx, aly, 1 + sigma,
     // Dirichlet no-pressure flag), (zc_out x, zc_in x, zc_out y, zc_in y)
