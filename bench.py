@@ -123,7 +123,9 @@ def profiled_kernel(cells: int, shape: int, fast: int) -> dict:
             out["traffic"] = int(d["dram_bytes_per_launch"])
         else:
             continue
-        if int(d.get("shape", -1)) == int(shape) and "smsp_issue_active_pct" in d:
+        if str(shape) in by_shape and "smsp_issue_active_pct" in by_shape[str(shape)]:
+            out["issue_active_pct"] = float(by_shape[str(shape)]["smsp_issue_active_pct"])
+        elif int(d.get("shape", -1)) == int(shape) and "smsp_issue_active_pct" in d:
             out["issue_active_pct"] = float(d["smsp_issue_active_pct"])
         return out
     return out

@@ -446,7 +446,7 @@ constexpr int kMaxDescriptors = kDescEntries;
 constexpr size_t kDescTableBytes = 2 * kMaxDescriptors * 4 * sizeof(float);
 
 void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vector<float>& ta,
-                       std::vector<float>& tb) {
+                       std::vector<float>& tb, int32_t* ndesc = nullptr) {
     desc.assign((size_t)g.H * g.pitch, 0);
     ta.assign(4 * kMaxDescriptors, 0.0f);
     tb.assign(4 * kMaxDescriptors, 0.0f);
@@ -468,6 +468,7 @@ void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vecto
             }
             desc[(size_t)r * g.pitch + c] = (uint8_t)id_of_key[k];
         }
+    if (ndesc) *ndesc = (int32_t)key_of_id.size();
     for (size_t id = 0; id < key_of_id.size(); ++id) {
         const int k = key_of_id[id];
         const int kc = k / 256, tr = (k / 16) % 16, tt = k % 16;
@@ -643,7 +644,7 @@ void upload_static_tube(vs_batch* b, size_t i) {
         if (b->fast) {
             std::vector<uint8_t> desc;
             std::vector<float> ta, tb;
-            build_descriptors(g, desc, ta, tb);
+            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc);
             ck(cudaMemcpy((void*)t.desc, desc.data(), desc.size(), cudaMemcpyHostToDevice), "upload descriptors");
             ck(cudaMemcpy((void*)t.desc_a, ta.data(), ta.size() * sizeof(float), cudaMemcpyHostToDevice),
                "upload descriptor table");
@@ -672,7 +673,7 @@ void upload_static(vs_batch* b) {
             m.assign(end, 0);
             std::vector<uint8_t> desc;
             std::vector<float> ta, tb;
-            build_descriptors(g, desc, ta, tb);
+            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc);
             std::memcpy(m.data() + at(t.desc), desc.data(), desc.size());
             std::memcpy(m.data() + at(t.desc_a), ta.data(), ta.size() * sizeof(float));
             std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
@@ -691,7 +692,7 @@ void upload_static(vs_batch* b) {
         if (b->fast) {
             std::vector<uint8_t> desc;
             std::vector<float> ta, tb;
-            build_descriptors(g, desc, ta, tb);
+            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc);
             std::memcpy(m.data() + at(t.desc), desc.data(), desc.size());
             std::memcpy(m.data() + at(t.desc_a), ta.data(), ta.size() * sizeof(float));
             std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
@@ -706,6 +707,9 @@ void upload_static(vs_batch* b) {
         ck(cudaMemcpy((void*)(base + from), img[i].data() + from, img[i].size() - from, cudaMemcpyHostToDevice),
            "upload maps");
     }
+    // the descriptor counts (TubeDev::ndesc) are known now
+    ck(cudaMemcpy(b->d_tubes, b->h_tubes.data(), n * sizeof(TubeDev), cudaMemcpyHostToDevice),
+       "upload tube descriptors");
 }
 
 void reset_state(vs_batch* b) {

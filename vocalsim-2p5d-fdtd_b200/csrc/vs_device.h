@@ -52,6 +52,7 @@ struct TubeDev {
     const uint8_t* desc;
     const float4* desc_a;
     const float4* desc_b;  // = desc_a + kDescEntries (the two tables are contiguous)
+    int32_t ndesc;        // descriptors in use (ids 0 .. ndesc-1)
     float* X;             // fast_math: a third P, Vx, Vy set (`plane` apart) for the two-step kernels
     TmmState* tmm_x;      // the two-step kernels' third two-mass state slot (float and double model)
     TmmState64* tmm64_x;

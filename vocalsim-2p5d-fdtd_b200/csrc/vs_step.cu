@@ -672,6 +672,24 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     if (wi >= nitems) return;
     const Tile it = items[wi];
     const TubeDev* __restrict__ T = tubes + it.tube;
+    // each warp copies the descriptors its tube uses (desc_a, then desc_b at
+    // kDescEntries) into its own shared-memory slot, where the rows' lookups
+    // go; up to 4 warps per CTA (32 KB), wider CTAs read through L1
+    constexpr bool kSmemTab = WARPS <= 4;
+    __shared__ float4 s_tab[kSmemTab ? WARPS : 1][kSmemTab ? 2 * kDescEntries : 1];
+    float4* wtab = s_tab[kSmemTab ? (threadIdx.x >> 5) : 0];
+    if constexpr (kSmemTab) {
+        const float4* __restrict__ src = T->desc_a;
+        for (int j = lane; j < T->ndesc; j += 32) {
+            wtab[j] = __ldg(src + j);
+            wtab[kDescEntries + j] = __ldg(src + kDescEntries + j);
+        }
+        __syncwarp();
+    }
+    auto tab = [&](int i) -> float4 {
+        if constexpr (kSmemTab) return wtab[i];
+        else return __ldg(T->desc_a + i);
+    };
     const int64_t n = rs->step + 2 * (int64_t)local;
     const int par = (int)(n & 1);
     const bool from_x = ((rs->bsel ^ local) & 1) != 0;
@@ -795,7 +813,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         float pn1[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
-            da[q] = __ldg(ta + code_byte(k_c, q));
+            da[q] = tab(code_byte(k_c, q));
             const float uxl = q == 0 ? ux_l : ux_c[q - 1];
             const float ks = fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(fmul(vy_c[q], dy_c[q]), fmul(vy_n[q], dy_n[q]))));
             const float v = fmul(__fmaf_rn(-ks, rcp_approx(dp_c[q]), p_c[q]), da[q].z);
@@ -813,7 +831,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             float vx = fmul(fsub(vx_c[q], fmul(bco, fsub(pr, pn1[q]))), da[q].x);
             float vy = fmul(fsub(vy_c[q], fmul(bco, fsub(pn1_p[q], pn1[q]))), da[q].y);
             if (gen1) {
-                const float4 db = __ldg(ta + (kDescEntries + code_byte(k_c, q)));
+                const float4 db = tab(kDescEntries + code_byte(k_c, q));
                 vx = __fmaf_rn(da[q].w, exe1, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn1[q], vx)));
                 vy = __fmaf_rn(-db.w, pn1_p[q], __fmaf_rn(db.z, pn1[q], vy));
             }
@@ -845,7 +863,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             float4 da_p[NC];
 #pragma unroll
             for (int q = 0; q < NC; ++q) {
-                da_p[q] = __ldg(ta + code_byte(k_p, q));
+                da_p[q] = tab(code_byte(k_p, q));
                 const float uxl = q == 0 ? ul : u1_p[q - 1];
                 const float ks = fmul(K1, fadd(fsub(u1_p[q], uxl), fsub(w1_p[q], w1[q])));
                 const float v = fmul(__fmaf_rn(-ks, rcp_approx(dp_p[q]), pn1_p[q]), da_p[q].z);
@@ -861,7 +879,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                     float vx = fmul(fsub(v1x_p[q], fmul(bco, fsub(pr, pn2[q]))), da_p[q].x);
                     float vy = fmul(fsub(v1y_p[q], fmul(bco, fsub(pn2_p[q], pn2[q]))), da_p[q].y);
                     if (gen2) {
-                        const float4 db = __ldg(ta + (kDescEntries + code_byte(k_p, q)));
+                        const float4 db = tab(kDescEntries + code_byte(k_p, q));
                         vx = __fmaf_rn(da_p[q].w, exe2, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn2[q], vx)));
                         vy = __fmaf_rn(-db.w, pn2_p[q], __fmaf_rn(db.z, pn2[q], vy));
                     }
