@@ -1100,7 +1100,12 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     const int rows = b->adj_rows ? b->adj_rows : (form == ADJ_FORM_STRIPS2 ? 8 : 4);
     // with fast_math a full segment (K even) is recomputed two steps per
     // launch by the two-step kernel, which needs the third state set
-    const bool hist_two = b->fast && K % 2 == 0;
+    // a single tube that steps on the cluster kernel (register form) recomputes
+    // each segment with one cluster launch that stores every step's state;
+    // otherwise, with fast_math, a full segment (K even) is recomputed two
+    // steps per launch by the two-step kernel, which needs the third state set
+    const bool hist_cluster = n == 1 && tile_shape(b->shape).kind == SHAPE_CLUSTER && b->cluster.form != 0;
+    const bool hist_two = !hist_cluster && b->fast && K % 2 == 0;
     if (hist_two) ensure_third_set(b);
     // device memory per tube, all zeroed per call: history (K+1 slots x 3
     // planes), lambda (2 x 3 planes), gradients (4 double planes) and, with
@@ -1271,7 +1276,13 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
         ck(cudaMemcpyAsync(b->d_adjrun, &ar, sizeof(ar), cudaMemcpyHostToDevice, b->stream), "set adjoint run");
         ck(cudaEventRecord(ev[3 * k], b->stream), "event");
         ck(launch_history_seed(b->d_tubes, n, max_plane, (int)(start & 1), b->stream), "history seed");
-        if (len == K) {
+        if (hist_cluster) {
+            ck(launch_cluster_run(b->d_tubes, b->d_rs, len, b->fast, b->cluster, b->stream), "history (cluster)");
+            ck(cudaEventRecord(ev[3 * k + 1], b->stream), "event");
+            if (len == K) ck(cudaGraphLaunch(b->adj_graph, b->stream), "reverse graph");
+            else
+                for (int j = 0; j < launches(len); ++j) ck(adj_launch(j, len), "adjoint step");
+        } else if (len == K) {
             ck(cudaGraphLaunch(b->hist_graph, b->stream), "history graph");
             ck(cudaEventRecord(ev[3 * k + 1], b->stream), "event");
             ck(cudaGraphLaunch(b->adj_graph, b->stream), "reverse graph");

@@ -381,6 +381,12 @@ __device__ __noinline__ float tmm_slot_finish(TmmSlot* slot, bool tmm64, float p
     return tmm64 ? tmm_finish64(slot->prep64, slot->s64, p1) : tmm_finish(slot->prep32, slot->s32, p1);
 }
 
+// The model's current state as the adjoint's two-mass history keeps it.
+__device__ __noinline__ void tmm_slot_hist(const TmmSlot* slot, bool tmm64, double* h) {
+    if (tmm64) tmm_to_hist(slot->s64, h);
+    else tmm_to_hist(slot->s32, h);
+}
+
 struct RegLayout {
     int pitch, nw, rmax;
     size_t gT, gVyB, dX0, eUX, eP, tab, sig, exe, tmm, bar, exr, bytes;   // byte offsets
@@ -558,6 +564,10 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const bool exc_owner = tmm && T->exc_y >= r0 && T->exc_y <= r1;
     const int exc_i = T->exc_y - (r0 - 1), exc_x = T->exc_x;
     const bool tmm_thread = exc_owner && tid == (two_mass_warp ? ncols : nthr - 1);
+    // the adjoint's segment recomputation: every step's state (and the
+    // two-mass state) also goes to the history slots
+    float* __restrict__ hist = T->hist;
+    double* __restrict__ thist = T->tmm_hist;
     // the excitation cell's column owner publishes its P' for the two-mass thread;
     // for the two-mass warp as tagged words (P bits | step << 32) by step parity
     // in sExe[4..7] (the owner writes step n + 2 only after the warp sent the
@@ -604,6 +614,7 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     if (tmm_thread) {
         tmm_prepare_next();
         const float e0 = tmm_finish_next(*sPexc);
+        if (thist) tmm_slot_hist(slot, tmm64, thist + 6 * (n0 + 1 - run_start));
         if (P2P) send_exe_ring(n0, e0);
         else send_exe(par0, e0);
         tmm_prepare_next();
@@ -719,8 +730,12 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
         } else {
             __syncthreads();
             if (n + 1 < n_end) {
-                if (tmm_thread) send_exe(q, tmm_finish_next(*sPexc));
-                else if (!tmm && tid == 0) sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+                if (tmm_thread) {
+                    send_exe(q, tmm_finish_next(*sPexc));
+                    if (thist) tmm_slot_hist(slot, tmm64, thist + 6 * (n + 2 - run_start));
+                } else if (!tmm && tid == 0) {
+                    sExe[q] = n + 1 < T->src_len ? T->src[n + 1] : 0.0f;
+                }
             }
         }
         const float exeV = sExe[p];
@@ -780,6 +795,17 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
             }
             if (lane == 31) eUX[(warp + 1) * (RMAX + 1) + i] = fmul(VX[i], dX[i]);
         }
+        if (hist && mine) {
+            float* h = hist + (n + 1 - run_start) * 3 * pl;
+#pragma unroll
+            for (int i = 1; i <= RMAX; ++i) {
+                if (i > Rk) break;
+                const int64_t o = (int64_t)(r0 - 1 + i) * pitch + c;
+                h[o] = P[i];
+                h[pl + o] = VX[i];
+                h[2 * pl + o] = VY[i];
+            }
+        }
         if (P2P) {
             // one thread arrives on the barrier of the next step's ghosts, expecting
             // the bytes both neighbours send; the block barrier publishes the edges
@@ -802,6 +828,7 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
                 break;
             }
             send_exe_ring(n + 1, tmm_finish_next(__uint_as_float((uint32_t)v)));
+            if (thist) tmm_slot_hist(slot, tmm64, thist + 6 * (n + 2 - run_start));
             if (n + 2 < n_end) tmm_prepare_next();
         }
     }
