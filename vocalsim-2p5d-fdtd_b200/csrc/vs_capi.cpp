@@ -207,14 +207,12 @@ namespace {
 // CTA, and 4-row strips with 2 warps per CTA below kSmallGridCells cells;
 // with fast_math the quad strips of the same heights (16 rows x 4 warps,
 // 2 rows x 2 warps), and for fast_math batches without the coupled wall
-// the two-step strips of 64 columns (32 rows x 4 warps; 2 rows x 2 warps
-// below kSmallGridCells).
+// the two-step strips of 64 columns with the strip height of
+// two_step_shape() (2 to 32 rows by batch size).
 constexpr int kDefaultShape = 1;
 constexpr int kSmallShape = 8;
 constexpr int kFastShape = 17;
 constexpr int kFastSmallShape = 21;
-constexpr int kTwoStepShape = 36;
-constexpr int kTwoStepSmallShape = 42;
 constexpr int64_t kSmallGridCells = 200000;
 
 int planes_per_tube(const TubeGrid& g) { return g.wall_ode ? 13 : 9; }
@@ -302,8 +300,8 @@ int default_shape(const vs_batch* b) {
     // a single tube keeps its state on one thread-block cluster for the whole run
     if (b->grids.size() == 1 && shape_fits(b, cluster_shape())) return cluster_shape();
     int64_t cells = 0;
-    for (const TubeGrid& g : b->grids) cells += (int64_t)g.H * g.W;
-    const int two = cells >= kSmallGridCells ? kTwoStepShape : kTwoStepSmallShape;
+    for (const TubeGrid& g : b->grids) cells += g.dims.interior_cells;
+    const int two = two_step_shape(cells);
     if (tile_shape(two).kind == SHAPE_QUAD2 && shape_fits(b, two)) return two;
     return single_step_shape(b);
 }

@@ -228,6 +228,9 @@ int history_shape(int64_t cells, bool fast);
 cudaError_t launch_step_history2(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
                                  int local, cudaStream_t stream);
 int history2_shape(int64_t cells);
+// The two-step launch shape for a batch of `cells` interior cells (strip
+// height by batch size; the default of fast_math batches).
+int two_step_shape(int64_t cells);
 
 // Adjoint buffers of one tube (device memory).
 struct AdjTube {

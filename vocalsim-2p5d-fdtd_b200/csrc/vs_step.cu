@@ -1269,23 +1269,26 @@ cudaError_t launch_step_history(int shape, const TubeDev* tubes, const Tile* til
     return cudaGetLastError();
 }
 
-// Strip height of the two-step history kernel by batch size, measured on
-// fs x 30 / x 15 batches (B200): taller strips waste fewer halo rows, shorter
-// ones give the row march more warps per SM -- 8 rows at 0.7 M interior cells
-// (9.2 us per step, against 16.8 with 32 rows), 16 rows at 1.6 M, 32 rows
-// from 2.5 M.
-int history2_shape(int64_t cells) {
-    if (cells < 200000) return 42;
-    if (cells < 1000000) return 44;
-    if (cells < 2000000) return 34;
-    return 36;
+// Strip height of the two-step kernels (forward and history) by batch size,
+// measured on fs x 1 / x 15 / x 30 batches (B200, forward, us per step):
+// taller strips waste fewer halo rows, shorter ones give the row march more
+// warps per SM.  0.38 M interior cells: 4 rows 4.03, 8 rows 4.44, 32 rows 9.18;
+// 0.67 M: 8 rows 4.99, 16 rows 6.50, 32 rows 9.32; 1.55 M: 16 rows 9.01,
+// 32 rows 12.45; 2.55 M: 32 rows 15.4, 16 rows 16.4.
+int two_step_shape(int64_t cells) {
+    if (cells < 200000) return 42;       // 2 rows, 2 warps
+    if (cells < 600000) return 43;       // 4 rows, 2 warps
+    if (cells < 1000000) return 44;      // 8 rows, 2 warps
+    if (cells < 2000000) return 34;      // 16 rows, 4 warps
+    return 36;                           // 32 rows, 4 warps
 }
+
+int history2_shape(int64_t cells) { return two_step_shape(cells); }
 
 cudaError_t launch_step_history2(int shape, const TubeDev* tubes, const Tile* tiles, int ntiles, RunState* rs,
                                  int local, cudaStream_t stream) {
-    // the two-step shapes 36 (32-row strips, 4 warps per CTA), 34 (16 rows,
-    // 4 warps), 44 (8 rows, 2 warps) and 42 (2 rows, 2 warps) of the table,
-    // storing the history of both steps
+    // the two-step shapes of two_step_shape() (36, 34, 44, 43, 42), storing
+    // the history of both steps
     if (ntiles <= 0) return cudaSuccess;
     if (shape == 36)
         quad2_kernel<32, 4, 4, 2, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
@@ -1293,6 +1296,8 @@ cudaError_t launch_step_history2(int shape, const TubeDev* tubes, const Tile* ti
         quad2_kernel<16, 4, 4, 2, true><<<(ntiles + 3) / 4, 128, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else if (shape == 44)
         quad2_kernel<8, 2, 8, 2, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
+    else if (shape == 43)
+        quad2_kernel<4, 2, 8, 2, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else if (shape == 42)
         quad2_kernel<2, 2, 8, 2, true><<<(ntiles + 1) / 2, 64, 0, stream>>>(tubes, tiles, ntiles, rs, local);
     else
