@@ -337,6 +337,10 @@ int vs_batch_set_maps(vs_batch* b, int32_t tube, const float* depth_p, const flo
 int vs_batch_get_maps(const vs_batch* b, int32_t tube, int32_t* cell_type, float* depth_p, float* depth_x,
                       float* depth_y, float* z_inv);
 
+/* vs_get_fields for tube i of a batch: its current P, Vx, Vy frames
+ * (frameH*frameW floats each, host buffers, NULL skips one). */
+int vs_batch_get_fields(const vs_batch* b, int32_t tube, float* p, float* vx, float* vy);
+
 /* Forward `steps` steps from rest, keeping a state checkpoint every
  * ckpt_every steps for vs_batch_adjoint; traces (host, n x steps) may be NULL. */
 int vs_batch_forward_ckpt(vs_batch* b, int64_t steps, int32_t ckpt_every, float* traces);

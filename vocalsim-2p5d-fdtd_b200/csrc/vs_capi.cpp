@@ -116,6 +116,7 @@ struct vs_batch {
     int device = 0;
     bool wall = false;                     // some tube has the coupled wall oscillator
     bool fast = false;                     // reciprocal-form arithmetic (vs_params::fast_math)
+    bool desc = false;                     // descriptor planes and tables (fast_math, or no wall oscillator)
     int max_pitch = 0;                     // largest row pitch of the batch (band shared memory)
     int cluster_state = 0;                 // cluster shape: 0 = not checked, 1 = fits, -1 = does not
     uint32_t wait_polls = 0;               // RunState::wait_polls of every run (0 = the default limit)
@@ -280,8 +281,13 @@ bool shape_fits(const vs_batch* b, int shape) {
     const int kind = tile_shape(shape).kind;
     if (kind == SHAPE_CLUSTER) return cluster_fits(b);
     if (b->wall && (kind == SHAPE_QUAD || kind == SHAPE_QUAD2)) return false;   // no wall-oscillator variant
-    // two-step kernels: fast_math only
-    if (kind == SHAPE_QUAD2 && !b->fast) return false;
+    // two-step kernels in the reference arithmetic: the 2-column shapes, when
+    // every tube's neighbourhoods fit its descriptor tables
+    if (kind == SHAPE_QUAD2 && !b->fast) {
+        if (!b->desc || !shape_has_plain(shape)) return false;
+        for (const TubeDev& t : b->h_tubes)
+            if (t.ndesc <= 0) return false;
+    }
     if (b->fast && !shape_has_fast(shape)) return false;
     return shape_smem_bytes(shape, b->max_pitch) <= smem_optin_limit(b->device);
 }
@@ -432,19 +438,65 @@ void ensure_graph(vs_batch* b) {
     b->graph_shape = b->shape;
 }
 
-// fast_math descriptors of one tube: every interior cell gets the index of its
-// (code, right type, top type) neighbourhood, and the two tables hold the
-// velocity and pressure factors of each neighbourhood (FDTDSolver.cu:652-801
-// with every beta 0 or 1), computed in double and rounded once:
+// Descriptors of one tube: every interior cell gets the index of its
+// (code, right type, top type) neighbourhood; index 0 is plain air, and ring
+// cells keep index 0 (they are never computed).  fast_math: the two tables
+// hold the velocity and pressure factors of each neighbourhood
+// (FDTDSolver.cu:652-801 with every beta 0 or 1), computed in double and
+// rounded once:
 //   rden = 1 / (mB + mS); al = mB rden; zo = mS zinv n x_out Nout rden;
 //   zi = mS zinv n x_in Nin rden; ce = ew mS rden; g = 1 / (1 + sigma_c)
-// (g = 0 on the no-pressure cells of a Dirichlet mouth).  Index 0 is plain
-// air.  Ring cells keep index 0 (they are never computed).
+// (g = 0 on the no-pressure cells of a Dirichlet mouth).
+// Reference arithmetic (`exact`): the neighbourhood's factors as the per-cell
+// update of the strip kernel forms them in float (velocity_generic and the
+// pressure denominator), desc_a = (sP, den_x, den_y, EXD_* bits) and desc_b =
+// (mS_x, W_x, mS_y, W_y); more than kDescEntries neighbourhoods leave *ndesc
+// = 0 there (the two-step shapes are then not offered) instead of failing.
 constexpr int kMaxDescriptors = kDescEntries;
 constexpr size_t kDescTableBytes = 2 * kMaxDescriptors * 4 * sizeof(float);
 
+// one rounded float product (the host build does not contract, and the
+// volatile keeps the product a separate rounding in any case)
+float fprod(float a, float b) {
+    volatile float p = a * b;
+    return p;
+}
+
+void exact_descriptor(const TubeGrid& g, int kc, int tr, int tt, float* a, float* bq) {
+    const int tc = kc & CODE_TYPE_MASK;
+    const bool zbit = (kc & CODE_ZINV_BIT) != 0;
+    const bool bc = beta_one(tc), br = beta_one(tr), bt = beta_one(tt);
+    const bool ec = tc == VS_CELL_EXCITATION, er = tr == VS_CELL_EXCITATION, et = tt == VS_CELL_EXCITATION;
+    const float sc = g.sigma[tc];
+    unsigned bits = (g.dirichlet && tc == VS_CELL_NOPRESSURE) ? EXD_PZERO : 0u;
+    // one direction: neighbour beta bn / excitation en / sigma sn, the other
+    // neighbour's beta bo, the source directions dirc (cell) and dirn (neighbour)
+    auto dir = [&](bool bn, bool en, float sn, bool bo, float dirc, float dirn, float* den, float* mS, float* W) {
+        const bool mB = bc && bn;
+        const bool src = ec || en;
+        *mS = std::max(sc, sn);
+        *W = fprod(ec ? 1.0f : 0.0f, dirc) + fprod(en ? 1.0f : 0.0f, dirn);
+        *den = (mB ? 1.0f : 0.0f) + *mS;
+        unsigned f = 0;
+        if (mB) f |= EXD_MB;
+        if (src) f |= EXD_SRC;
+        if (zbit && !src && bc != bn) f |= EXD_WALL;
+        if (bc) f |= EXD_WALL_PC;
+        if (bo) f |= EXD_NOUT1;
+        return f;
+    };
+    float denx, mSx, Wx, deny, mSy, Wy;
+    bits |= dir(br, er, g.sigma[tr], bt, g.dir[2], g.dir[0], &denx, &mSx, &Wx);
+    bits |= dir(bt, et, g.sigma[tt], br, g.dir[3], g.dir[1], &deny, &mSy, &Wy) << EXD_Y_SHIFT;
+    a[0] = g.eigen ? sc : 1.0f + sc;
+    a[1] = denx;
+    a[2] = deny;
+    std::memcpy(&a[3], &bits, sizeof(float));
+    bq[0] = mSx; bq[1] = Wx; bq[2] = mSy; bq[3] = Wy;
+}
+
 void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vector<float>& ta,
-                       std::vector<float>& tb, int32_t* ndesc = nullptr) {
+                       std::vector<float>& tb, int32_t* ndesc = nullptr, bool exact = false) {
     desc.assign((size_t)g.H * g.pitch, 0);
     ta.assign(4 * kMaxDescriptors, 0.0f);
     tb.assign(4 * kMaxDescriptors, 0.0f);
@@ -459,8 +511,14 @@ void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vecto
             const int k = key(code_at(r, c) & 0x1f, code_at(r, c + 1) & CODE_TYPE_MASK,
                               code_at(r - 1, c) & CODE_TYPE_MASK);
             if (id_of_key[k] < 0) {
-                if ((int)key_of_id.size() >= kMaxDescriptors)
+                if ((int)key_of_id.size() >= kMaxDescriptors) {
+                    if (exact) {
+                        desc.assign(desc.size(), 0);
+                        if (ndesc) *ndesc = 0;
+                        return;
+                    }
                     throw VsFailure{VS_ERR_UNSUPPORTED, "fast_math: more than 256 distinct cell neighbourhoods"};
+                }
                 id_of_key[k] = (int)key_of_id.size();
                 key_of_id.push_back(k);
             }
@@ -470,6 +528,10 @@ void build_descriptors(const TubeGrid& g, std::vector<uint8_t>& desc, std::vecto
     for (size_t id = 0; id < key_of_id.size(); ++id) {
         const int k = key_of_id[id];
         const int kc = k / 256, tr = (k / 16) % 16, tt = k % 16;
+        if (exact) {
+            exact_descriptor(g, kc, tr, tt, &ta[4 * id], &tb[4 * id]);
+            continue;
+        }
         const int tc = kc & CODE_TYPE_MASK;
         const bool zbit = (kc & CODE_ZINV_BIT) != 0;
         const double zinv = zbit ? (double)g.zinv_val : 0.0;
@@ -639,10 +701,10 @@ void upload_static_tube(vs_batch* b, size_t i) {
         up(g.dX, t.dX);
         up(g.dY, t.dY);
         ck(cudaMemcpy((void*)t.code, g.code.data(), g.code.size(), cudaMemcpyHostToDevice), "upload codes");
-        if (b->fast) {
+        if (b->desc) {
             std::vector<uint8_t> desc;
             std::vector<float> ta, tb;
-            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc);
+            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc, !b->fast);
             ck(cudaMemcpy((void*)t.desc, desc.data(), desc.size(), cudaMemcpyHostToDevice), "upload descriptors");
             ck(cudaMemcpy((void*)t.desc_a, ta.data(), ta.size() * sizeof(float), cudaMemcpyHostToDevice),
                "upload descriptor table");
@@ -663,15 +725,15 @@ void upload_static(vs_batch* b) {
         const TubeDev& t = b->h_tubes[i];
         const char* base = reinterpret_cast<const char*>(t.dP);
         auto at = [&](const void* p) { return (size_t)(reinterpret_cast<const char*>(p) - base); };
-        const size_t end = b->fast ? at(t.desc_b) + kDescTableBytes / 2 : at(t.code) + align_up((size_t)g.H * g.pitch);
+        const size_t end = b->desc ? at(t.desc_b) + kDescTableBytes / 2 : at(t.code) + align_up((size_t)g.H * g.pitch);
         std::vector<char>& m = img[i];
         if (g.device_maps) {
             // the planes and codes are on the device already: the descriptors only
-            if (!b->fast) return;
+            if (!b->desc) return;
             m.assign(end, 0);
             std::vector<uint8_t> desc;
             std::vector<float> ta, tb;
-            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc);
+            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc, !b->fast);
             std::memcpy(m.data() + at(t.desc), desc.data(), desc.size());
             std::memcpy(m.data() + at(t.desc_a), ta.data(), ta.size() * sizeof(float));
             std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
@@ -687,10 +749,10 @@ void upload_static(vs_batch* b) {
         plane(g.dX, t.dX);
         plane(g.dY, t.dY);
         std::memcpy(m.data() + at(t.code), g.code.data(), g.code.size());
-        if (b->fast) {
+        if (b->desc) {
             std::vector<uint8_t> desc;
             std::vector<float> ta, tb;
-            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc);
+            build_descriptors(g, desc, ta, tb, &b->h_tubes[i].ndesc, !b->fast);
             std::memcpy(m.data() + at(t.desc), desc.data(), desc.size());
             std::memcpy(m.data() + at(t.desc_a), ta.data(), ta.size() * sizeof(float));
             std::memcpy(m.data() + at(t.desc_b), tb.data(), tb.size() * sizeof(float));
@@ -736,18 +798,6 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
     // arena layout: per tube, planes of H*pitch floats (+ codes) + two-mass
     // state, with kGuard bytes before the first and after the last tube: the
     // step kernel reads one element before and up to 29 after a plane
-    size_t total = kGuard;
-    std::vector<size_t> base(n);
-    for (int i = 0; i < n; ++i) {
-        const TubeGrid& g = b->grids[i];
-        base[i] = total;
-        const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
-        total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState)) +
-                 align_up(2 * sizeof(TmmState64));
-        if (params[0].fast_math) total += align_up((size_t)g.H * g.pitch) + kDescTableBytes;
-    }
-    total += kGuard;
-    b->arena_bytes = total;
     for (const TubeGrid& g : b->grids) {
         b->wall = b->wall || g.wall_ode;
         b->max_pitch = std::max(b->max_pitch, g.pitch);
@@ -756,6 +806,21 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
     for (int i = 1; i < n; ++i)
         if ((params[i].fast_math != 0) != b->fast)
             throw VsFailure{VS_ERR_INVALID_ARG, "every tube of a batch needs the same fast_math"};
+    // descriptor planes for the kernels that read them: fast_math, and the
+    // two-step kernel in the reference arithmetic (no coupled wall)
+    b->desc = b->fast || !b->wall;
+    size_t total = kGuard;
+    std::vector<size_t> base(n);
+    for (int i = 0; i < n; ++i) {
+        const TubeGrid& g = b->grids[i];
+        base[i] = total;
+        const size_t pl = align_up((size_t)g.H * g.pitch * sizeof(float));
+        total += pl * planes_per_tube(g) + align_up((size_t)g.H * g.pitch) + align_up(2 * sizeof(TmmState)) +
+                 align_up(2 * sizeof(TmmState64));
+        if (b->desc) total += align_up((size_t)g.H * g.pitch) + kDescTableBytes;
+    }
+    total += kGuard;
+    b->arena_bytes = total;
     ck(cudaMalloc(&b->arena, total), "cudaMalloc(arena)");
     b->h_tubes.resize(n);
     b->src_len.assign(n, 0);
@@ -784,7 +849,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         t.dX = (const float*)next(pl);
         t.dY = (const float*)next(pl);
         t.code = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
-        if (b->fast) {
+        if (b->desc) {
             t.desc = (const uint8_t*)next(align_up((size_t)g.H * g.pitch));
             t.desc_a = (const float4*)next(kDescTableBytes / 2);
             t.desc_b = (const float4*)next(kDescTableBytes / 2);    // desc_a + kDescEntries
@@ -1798,10 +1863,14 @@ int vs_reset(vs_solver* s) {
 
 int vs_get_fields(const vs_solver* s, float* p, float* vx, float* vy) {
     if (!s) return set_error(VS_ERR_INVALID_ARG, "null solver");
-    const vs_batch* b = s->b;
+    return vs_batch_get_fields(s->b, 0, p, vx, vy);
+}
+
+int vs_batch_get_fields(const vs_batch* b, int32_t tube, float* p, float* vx, float* vy) {
+    if (!b || tube < 0 || tube >= (int)b->grids.size()) return set_error(VS_ERR_INVALID_ARG, "vs_batch_get_fields");
     return guarded([&] {
-        const TubeGrid& g = b->grids[0];
-        const TubeDev& t = b->h_tubes[0];
+        const TubeGrid& g = b->grids[(size_t)tube];
+        const TubeDev& t = b->h_tubes[(size_t)tube];
         const int par = (int)(b->step & 1);
         const float* src[3] = {t.P[par], t.Vx[par], t.Vy[par]};
         float* dst[3] = {p, vx, vy};

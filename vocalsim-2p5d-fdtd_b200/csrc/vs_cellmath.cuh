@@ -333,6 +333,29 @@ __device__ __forceinline__ VelocityOut velocity_generic(
             velocity_dir(bc, bt, br, ec, et, dir3, dir1, vy0, pc, pt, exeV, fmaxf(sc, sig[tt]), zinv, bco)};
 }
 
+// velocity_dir with its neighbourhood resolved ahead: `bits` = the EXD_*
+// flags of one direction, den = mB + mS rounded, mS and the source weight
+// W = ec dirc + en dirn rounded as velocity_dir forms them.  The same
+// products, sums and division in the same order; the division by den = 1 is
+// the identity and is skipped.
+__device__ __forceinline__ float velocity_tab(unsigned bits, float den, float mS, float W, float v0, float pc,
+                                              float pn, float exeV, float zval, float bco) {
+    float v = (bits & EXD_MB) ? fsub(v0, fmul(bco, fsub(pn, pc))) : 0.0f;
+    if (bits & EXD_SRC) v = fadd(v, fmul(fmul(exeV, W), mS));
+    if ((bits & EXD_WALL) && zval != 0.0f) {
+        const float vb = (bits & EXD_WALL_PC) ? fmul(pc, (bits & EXD_NOUT1) ? 1.0f : 0.707106f) : -pn;
+        v = fadd(v, fmul(mS, fmul(vb, zval)));
+    }
+    return den != 1.0f ? fdiv_z(v, den) : v;
+}
+
+// Pressure denominator of a cell, (1 + sigma) dP (FDTDEngineCPU.cpp:330) with
+// sP = 1 + sigma rounded, or sigma dP + dP (FDTDEngineEigen.cpp:251) with
+// sP = sigma.
+__device__ __forceinline__ float pressure_den(float sP, float dp, bool eigen) {
+    return eigen ? fadd(fmul(sP, dp), dp) : fmul(sP, dp);
+}
+
 // Listener sample of a step; a non-finite value (an unstable tube) also
 // raises the run's sticky error word, so runs that keep their traces on the
 // device report VS_ERR_NONFINITE too.

@@ -48,7 +48,11 @@ struct TubeDev {
     // fast_math: per-cell descriptor bytes (same layout as `code`) into two
     // coefficient tables, desc_a = (alx, aly, g, cex), desc_b = (zox, zix, zoy,
     // ziy): P' = (P - K1 S / dP) g and
-    // V' = al (V - bcoef (P'n - P'c)) + zo P'c - zi P'n + ce exeV (x and y)
+    // V' = al (V - bcoef (P'n - P'c)) + zo P'c - zi P'n + ce exeV (x and y).
+    // Reference arithmetic (batches without the coupled wall): the same
+    // descriptor bytes into tables of the exactly rounded factors of the
+    // reference update, desc_a = (sP, den_x, den_y, flag bits EXD_*),
+    // desc_b = (mS_x, W_x, mS_y, W_y); see the two-step kernel.
     const uint8_t* desc;
     const float4* desc_a;
     const float4* desc_b;  // = desc_a + kDescEntries (the two tables are contiguous)
@@ -68,8 +72,19 @@ struct TubeDev {
 
 // Mutable run bookkeeping kept in device memory so that CUDA graphs captured
 // once can be replayed for any run length.
-// Entries of each fast_math descriptor table (desc_a, desc_b).
+// Entries of each descriptor table (desc_a, desc_b).
 constexpr int kDescEntries = 256;
+
+// Flag bits of a reference-arithmetic descriptor (desc_a.w as raw bits): per
+// velocity direction (x in bits 0-7, y in bits 8-15) mB = beta_c beta_n, a
+// source term (excitation cell or neighbour), the wall term (z_inv bit, no
+// excitation, beta_c != beta_n), its pressure (the cell's, else the
+// neighbour's) and Nout = 1 (else 1/sqrt 2); the no-pressure cells of a
+// Dirichlet mouth.
+enum : unsigned {
+    EXD_MB = 1u, EXD_SRC = 2u, EXD_WALL = 4u, EXD_WALL_PC = 8u, EXD_NOUT1 = 16u,
+    EXD_Y_SHIFT = 8u, EXD_PZERO = 1u << 16,
+};
 
 struct RunState {
     int64_t step;         // global step of the next launch with local index 0
@@ -207,6 +222,8 @@ cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps,
 cudaError_t launch_step(int shape, bool wall, bool fast, const TubeDev* tubes, const Tile* tiles, int ntiles,
                         RunState* rs, int local, cudaStream_t stream, int max_pitch);
 bool shape_has_fast(int shape);
+// true when the shape has a reference-arithmetic kernel without the wall oscillator
+bool shape_has_plain(int shape);
 
 // Dynamic shared memory a shape needs for frames of row pitch up to
 // max_pitch (0 for strips), and the one-time kernel attribute set-up for it.

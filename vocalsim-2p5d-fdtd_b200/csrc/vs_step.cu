@@ -663,7 +663,7 @@ __device__ __forceinline__ void stn(float* p, const float (&v)[NC], unsigned mas
     }
 }
 
-template <int TR, int WARPS, int MINB, int NC, bool HIST = false>
+template <int TR, int WARPS, int MINB, int NC, bool HIST = false, bool EXACT = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, int nitems,
              RunState* __restrict__ rs, int local) {
@@ -718,11 +718,17 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
     const float4* __restrict__ ta = T->desc_a;
     // desc_b follows desc_a (kDescEntries entries each): one base, immediate offsets
     const float K1 = T->K1, bco = T->bcoef;
+    const bool eigen = (T->flags & TUBE_EIGEN) != 0;
+    const float zval = T->zinv;
     const int lis_y = T->lis_y, lis_q = T->lis_x - x0;
     const bool lis_here = lis_q >= 0 && lis_q < NC && ((commit_m >> lis_q) & 1u);
-    // bit 1 of gm = velocity class of step n's row r (v_generic bit j-1),
-    // bit 0 = that of step n+1's row r-1 (bit j-2); shifted once per row
-    uint64_t gm = it.v_generic << 2;
+    // bit 1 of gm = velocity class of step n's row r (v_generic bit j-1; in
+    // the reference arithmetic v_beta1, every row with a velocity division),
+    // bit 0 = that of step n+1's row r-1 (bit j-2); bit 1 of pm = step n's
+    // row r holds a cell other than air (p_rows bit j), bit 0 = step n+1's
+    // row r-1; both shifted once per row
+    uint64_t gm = (EXACT ? it.v_beta1 : it.v_generic) << 2;
+    uint64_t pm = it.p_rows << 1;
     float exe1 = 0.0f, exe2 = 0.0f;
     const int rlast = min(r0 + TR - 1, H - 2);
     if (it.has_exc) {
@@ -736,7 +742,11 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
                 const float p1 = Pin[e];
                 const float ks = fmul(K1, fadd(fsub(fmul(Vxin[e], dXp[e]), fmul(Vxin[e - 1], dXp[e - 1])),
                                                fsub(fmul(Vyin[e], dYp[e]), fmul(Vyin[e + pitch], dYp[e + pitch]))));
-                const float p2 = fmul(__fmaf_rn(-ks, rcp_approx(dPp[e]), p1), __ldg(ta + desc[e]).z);
+                float p2;
+                if constexpr (EXACT)
+                    p2 = fdiv_z(fsub(fmul(p1, dPp[e]), ks), pressure_den(__ldg(ta + desc[e]).x, dPp[e], eigen));
+                else
+                    p2 = fmul(__fmaf_rn(-ks, rcp_approx(dPp[e]), p1), __ldg(ta + desc[e]).z);
                 const bool owner = T->exc_y >= r0 && T->exc_y <= rlast && T->exc_x >= c0 + NC &&
                                    T->exc_x < c0 + 31 * NC;
                 const float2 ee = glottal_two_steps(T, par, from_x, p1, p2, owner,
@@ -811,12 +821,27 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         const float ux_l = __shfl_up_sync(kFull, ux_c[NC - 1], 1);
         float4 da[NC];
         float pn1[NC];
+        const bool pg1 = (pm & 2u) != 0;
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
-            da[q] = tab(code_byte(k_c, q));
             const float uxl = q == 0 ? ux_l : ux_c[q - 1];
             const float ks = fmul(K1, fadd(fsub(ux_c[q], uxl), fsub(fmul(vy_c[q], dy_c[q]), fmul(vy_n[q], dy_n[q]))));
-            const float v = fmul(__fmaf_rn(-ks, rcp_approx(dp_c[q]), p_c[q]), da[q].z);
+            float v;
+            if constexpr (EXACT) {
+                // (P dP - K1 S) / ((1 + sigma) dP), the denominator dP on rows of air
+                float den = dp_c[q];
+                bool pz = false;
+                if (pg1) {
+                    const float4 a = tab(code_byte(k_c, q));
+                    den = pressure_den(a.x, dp_c[q], eigen);
+                    pz = (__float_as_uint(a.w) & EXD_PZERO) != 0u;
+                }
+                v = fdiv_z(fsub(fmul(p_c[q], dp_c[q]), ks), den);
+                if (pz) v = 0.0f;
+            } else {
+                da[q] = tab(code_byte(k_c, q));
+                v = fmul(__fmaf_rn(-ks, rcp_approx(dp_c[q]), p_c[q]), da[q].z);
+            }
             pn1[q] = ((cm1 >> q) & 1u) ? v : 0.0f;
         }
         const float p_r = __shfl_down_sync(kFull, pn1[0], 1);
@@ -828,12 +853,27 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
             const float pr = q < NC - 1 ? pn1[q + 1] : p_r;
-            float vx = fmul(fsub(vx_c[q], fmul(bco, fsub(pr, pn1[q]))), da[q].x);
-            float vy = fmul(fsub(vy_c[q], fmul(bco, fsub(pn1_p[q], pn1[q]))), da[q].y);
-            if (gen1) {
-                const float4 db = tab(kDescEntries + code_byte(k_c, q));
-                vx = __fmaf_rn(da[q].w, exe1, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn1[q], vx)));
-                vy = __fmaf_rn(-db.w, pn1_p[q], __fmaf_rn(db.z, pn1[q], vy));
+            float vx, vy;
+            if constexpr (EXACT) {
+                if (gen1) {
+                    const int d = code_byte(k_c, q);
+                    const float4 a = tab(d), bt = tab(kDescEntries + d);
+                    const unsigned bits = __float_as_uint(a.w);
+                    vx = velocity_tab(bits, a.y, bt.x, bt.y, vx_c[q], pn1[q], pr, exe1, zval, bco);
+                    vy = velocity_tab(bits >> EXD_Y_SHIFT, a.z, bt.z, bt.w, vy_c[q], pn1[q], pn1_p[q], exe1, zval,
+                                      bco);
+                } else {
+                    vx = fsub(vx_c[q], fmul(bco, fsub(pr, pn1[q])));
+                    vy = fsub(vy_c[q], fmul(bco, fsub(pn1_p[q], pn1[q])));
+                }
+            } else {
+                vx = fmul(fsub(vx_c[q], fmul(bco, fsub(pr, pn1[q]))), da[q].x);
+                vy = fmul(fsub(vy_c[q], fmul(bco, fsub(pn1_p[q], pn1[q]))), da[q].y);
+                if (gen1) {
+                    const float4 db = tab(kDescEntries + code_byte(k_c, q));
+                    vx = __fmaf_rn(da[q].w, exe1, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn1[q], vx)));
+                    vy = __fmaf_rn(-db.w, pn1_p[q], __fmaf_rn(db.z, pn1[q], vy));
+                }
             }
             v1x[q] = ((vm1 >> q) & 1u) ? vx : 0.0f;
             v1y[q] = ((vm1 >> q) & 1u) ? vy : 0.0f;
@@ -861,12 +901,26 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
             const float ul = __shfl_up_sync(kFull, u1_p[NC - 1], 1);
             float pn2[NC];
             float4 da_p[NC];
+            const bool pg2 = (pm & 1u) != 0;
 #pragma unroll
             for (int q = 0; q < NC; ++q) {
-                da_p[q] = tab(code_byte(k_p, q));
                 const float uxl = q == 0 ? ul : u1_p[q - 1];
                 const float ks = fmul(K1, fadd(fsub(u1_p[q], uxl), fsub(w1_p[q], w1[q])));
-                const float v = fmul(__fmaf_rn(-ks, rcp_approx(dp_p[q]), pn1_p[q]), da_p[q].z);
+                float v;
+                if constexpr (EXACT) {
+                    float den = dp_p[q];
+                    bool pz = false;
+                    if (pg2) {
+                        const float4 a = tab(code_byte(k_p, q));
+                        den = pressure_den(a.x, dp_p[q], eigen);
+                        pz = (__float_as_uint(a.w) & EXD_PZERO) != 0u;
+                    }
+                    v = fdiv_z(fsub(fmul(pn1_p[q], dp_p[q]), ks), den);
+                    if (pz) v = 0.0f;
+                } else {
+                    da_p[q] = tab(code_byte(k_p, q));
+                    v = fmul(__fmaf_rn(-ks, rcp_approx(dp_p[q]), pn1_p[q]), da_p[q].z);
+                }
                 pn2[q] = ((cm2 >> q) & 1u) ? v : 0.0f;
             }
             const float p2_r = __shfl_down_sync(kFull, pn2[0], 1);
@@ -876,12 +930,27 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
 #pragma unroll
                 for (int q = 0; q < NC; ++q) {
                     const float pr = q < NC - 1 ? pn2[q + 1] : p2_r;
-                    float vx = fmul(fsub(v1x_p[q], fmul(bco, fsub(pr, pn2[q]))), da_p[q].x);
-                    float vy = fmul(fsub(v1y_p[q], fmul(bco, fsub(pn2_p[q], pn2[q]))), da_p[q].y);
-                    if (gen2) {
-                        const float4 db = tab(kDescEntries + code_byte(k_p, q));
-                        vx = __fmaf_rn(da_p[q].w, exe2, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn2[q], vx)));
-                        vy = __fmaf_rn(-db.w, pn2_p[q], __fmaf_rn(db.z, pn2[q], vy));
+                    float vx, vy;
+                    if constexpr (EXACT) {
+                        if (gen2) {
+                            const int d = code_byte(k_p, q);
+                            const float4 a = tab(d), bt = tab(kDescEntries + d);
+                            const unsigned bits = __float_as_uint(a.w);
+                            vx = velocity_tab(bits, a.y, bt.x, bt.y, v1x_p[q], pn2[q], pr, exe2, zval, bco);
+                            vy = velocity_tab(bits >> EXD_Y_SHIFT, a.z, bt.z, bt.w, v1y_p[q], pn2[q], pn2_p[q], exe2,
+                                              zval, bco);
+                        } else {
+                            vx = fsub(v1x_p[q], fmul(bco, fsub(pr, pn2[q])));
+                            vy = fsub(v1y_p[q], fmul(bco, fsub(pn2_p[q], pn2[q])));
+                        }
+                    } else {
+                        vx = fmul(fsub(v1x_p[q], fmul(bco, fsub(pr, pn2[q]))), da_p[q].x);
+                        vy = fmul(fsub(v1y_p[q], fmul(bco, fsub(pn2_p[q], pn2[q]))), da_p[q].y);
+                        if (gen2) {
+                            const float4 db = tab(kDescEntries + code_byte(k_p, q));
+                            vx = __fmaf_rn(da_p[q].w, exe2, __fmaf_rn(-db.y, pr, __fmaf_rn(db.x, pn2[q], vx)));
+                            vy = __fmaf_rn(-db.w, pn2_p[q], __fmaf_rn(db.z, pn2[q], vy));
+                        }
                     }
                     vx2[q] = vx;
                     vy2[q] = vy;
@@ -928,6 +997,7 @@ quad2_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, 
         k_p = k_c;
         k_c = k_1;
         gm >>= 1;
+        pm >>= 1;
     }
 }
 
@@ -1158,10 +1228,17 @@ struct ShapeEntry {
 #define VS_QUAD(R, WARPS, MINB)                                                                          \
     {SHAPE_QUAD, R, WARPS, quad_kernel<R, WARPS, MINB, 0, false>, nullptr, 0, quad_kernel<R, WARPS, MINB, 0, true>}
 #define VS_QUAD2(R, WARPS, MINB, NC) \
-    {SHAPE_QUAD2, R, WARPS, nullptr, nullptr, 0, quad2_kernel<R, WARPS, MINB, NC>, NC}
+    {SHAPE_QUAD2, R, WARPS, quad2_exact<R, WARPS, MINB, NC>(), nullptr, 0, quad2_kernel<R, WARPS, MINB, NC>, NC}
 #define VS_QPIPE(R, WARPS, MINB, ST)                                                                     \
     {SHAPE_QUAD, R, WARPS, quad_kernel<R, WARPS, MINB, ST, false>, nullptr, ST,                          \
      quad_kernel<R, WARPS, MINB, ST, true>}
+
+// the two-step kernel in the reference arithmetic: the 2-column shapes
+template <int R, int WARPS, int MINB, int NC>
+constexpr StepFn quad2_exact() {
+    if constexpr (NC == 2) return quad2_kernel<R, WARPS, MINB, NC, false, true>;
+    else return nullptr;
+}
 
 // strips: (rows per strip, warps per CTA, CTAs per SM the register budget
 // targets); bands: rows per band (one CTA of 256 threads each)
@@ -1220,6 +1297,8 @@ cudaError_t prepare_shape(int shape, int max_pitch) {
         e = cudaFuncSetAttribute(kShapes[shape].fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return e;
 }
+
+bool shape_has_plain(int shape) { return shape >= 0 && shape < kNumShapes && kShapes[shape].plain != nullptr; }
 
 bool shape_has_fast(int shape) {
     return shape == kNumShapes || (shape >= 0 && shape < kNumShapes && kShapes[shape].fast != nullptr);

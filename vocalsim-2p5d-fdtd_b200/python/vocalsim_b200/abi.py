@@ -167,6 +167,7 @@ def load_library(path: os.PathLike | None = None) -> C.CDLL:
         "vs_batch_destroy": (None, [C.c_void_p]),
         "vs_batch_set_maps": (C.c_int, [C.c_void_p, C.c_int32, fp, fp, fp, C.c_float]),
         "vs_batch_get_maps": (C.c_int, [C.c_void_p, C.c_int32, i32p, fp, fp, fp, fp]),
+        "vs_batch_get_fields": (C.c_int, [C.c_void_p, C.c_int32, fp, fp, fp]),
         "vs_batch_forward_ckpt": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, fp]),
         "vs_batch_adjoint": (C.c_int, [C.c_void_p, fp, fp, fp, fp, fp]),
         "vs_run_noalloc": (C.c_int, [vp, vd, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -197,6 +197,14 @@ class Batch:
                                                    _fp(out["z_inv"])), "vs_batch_get_maps")
         return out
 
+    def fields(self, tube: int):
+        """Tube `tube`'s current P, Vx, Vy frames."""
+        d = self.dims[tube]
+        H, W = int(d["frame_h"]), int(d["frame_w"])
+        P, Vx, Vy = (np.zeros((H, W), np.float32) for _ in range(3))
+        check(self.lib, self.lib.vs_batch_get_fields(self.h, tube, _fp(P), _fp(Vx), _fp(Vy)), "vs_batch_get_fields")
+        return P, Vx, Vy
+
     def forward_ckpt(self, steps: int, ckpt_every: int = 512) -> np.ndarray:
         """Forward from rest keeping checkpoints for adjoint(); returns (n, steps) traces."""
         tr = np.zeros((self.n, steps), np.float32)
