@@ -109,7 +109,8 @@ def profiled_kernel(cells: int, shape: int, fast: int) -> dict:
     and arithmetic) on this same workload (same interior cell count); None
     where no summary matches."""
     out = {"traffic": None, "issue_active_pct": None}
-    for name in ("quad2_kernel_fast_batch256.json", "quad_kernel_fast_batch256.json", "strip_kernel_batch256.json"):
+    for name in ("quad2_kernel_fast_batch256.json", "quad_kernel_fast_batch256.json", "quad2_kernel_exact_batch256.json",
+                 "strip_kernel_batch256.json"):
         f = REPO / "profiles" / name
         if not f.exists():
             continue
