@@ -1161,8 +1161,6 @@ void run_adjoint(vs_batch* b, const float* gtrace, float* gdP, float* gdX, float
     if (form == ADJ_FORM_AUTO) form = (!any_tmm && strips8 >= 4 * (int64_t)sms) ? ADJ_FORM_STRIPS2 : ADJ_FORM_TILES;
     if (form == ADJ_FORM_STRIPS2 && any_tmm) form = ADJ_FORM_STRIPS;
     const int rows = b->adj_rows ? b->adj_rows : (form == ADJ_FORM_STRIPS2 ? 8 : 4);
-    // with fast_math a full segment (K even) is recomputed two steps per
-    // launch by the two-step kernel, which needs the third state set
     // a single tube that steps on the cluster kernel (register form) recomputes
     // each segment with one cluster launch that stores every step's state;
     // otherwise, with fast_math, a full segment (K even) is recomputed two
