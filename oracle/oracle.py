@@ -72,6 +72,7 @@ def lib() -> C.CDLL:
         L.orc_source_f32.argtypes = [vp, C.c_longlong, fp]
         L.orc_tmm_f32.argtypes = [C.c_float, C.c_int, fp, C.c_longlong, fp]
         L.orc_tmm_f64.argtypes = [C.c_float, C.c_int, dp, C.c_longlong, dp]
+        L.orc_tmm_f64r.argtypes = [C.c_float, C.c_int, dp, C.c_longlong, dp]
         L.orc_run_f32.argtypes = [vp, vg, C.c_longlong, fp, fp, fp, fp]
         L.orc_run_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, dp]
         L.orc_run_maps_f64.argtypes = [vp, vg, C.c_longlong, dp, dp, dp, C.c_double, dp]
@@ -233,6 +234,9 @@ def source(p: VsParams, n: int) -> np.ndarray:
 
 
 def tmm(ps: float, srate_mul: int, p1: np.ndarray, precision: str = "f32") -> np.ndarray:
+    """The two-mass model driven by the pressure sequence p1: "f32" the
+    reference's float model, "f64" its expressions in double, "f64r" the
+    tmm_f64 option's arrangement of the double model."""
     if precision == "f32":
         p1 = np.ascontiguousarray(p1, np.float32)
         ug = np.zeros_like(p1)
@@ -240,7 +244,8 @@ def tmm(ps: float, srate_mul: int, p1: np.ndarray, precision: str = "f32") -> np
     else:
         p1 = np.ascontiguousarray(p1, np.float64)
         ug = np.zeros_like(p1)
-        lib().orc_tmm_f64(ps, srate_mul, _dp(p1), len(p1), _dp(ug))
+        fn = lib().orc_tmm_f64r if precision == "f64r" else lib().orc_tmm_f64
+        fn(ps, srate_mul, _dp(p1), len(p1), _dp(ug))
     return ug
 
 

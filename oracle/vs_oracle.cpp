@@ -742,6 +742,110 @@ struct TwoMass {
     }
 };
 
+/* ---- the double two-mass model of the tmm_f64 option ------------------------
+ * The model of TwoMassModel.cpp:90-232 in double, arranged to divide only by
+ * the glottal openings (before and after the displacement update) and by the
+ * flow denominator: the per-model constants below (reciprocals of the sample
+ * rate, the thresholds, the displacement-update matrix and its inverse
+ * determinant per contact state) are formed once.  This is the arrangement
+ * the GPU's tmm_f64 model uses, operation for operation, so the FP32 engine
+ * with tmm_f64 pins it bit for bit; TwoMass<double> (the literal expressions)
+ * stays the FP64 engine's model, the accuracy reference. */
+struct TwoMassR {
+    TwoMass<double> k;                    /* primaries and state */
+    double isr, is2, two_lg, g1, g2, c12, cR1, cR2, cL1, cL2, hr, hr137, d1lg, d2lg, iA1, k1e, k2e;
+    double a11[2], a22[2], a12, b1c[2], b2c[2], idet[2][2];
+    double srate;
+
+    void init(float ps_pa, int srate_mul) {
+        k.init(ps_pa);
+        srate = 44100 * static_cast<double>(srate_mul);
+        isr = 1.0 / srate;
+        is2 = isr * isr;
+        two_lg = 2.0 * k.lg;
+        g1 = k.Ag01 / two_lg;
+        g2 = k.Ag02 / two_lg;
+        c12 = 12.0 * k.mu * k.lg * k.lg;
+        cR1 = c12 * k.d1;
+        cR2 = c12 * k.d2;
+        cL1 = k.rho * k.d1;
+        cL2 = k.rho * k.d2;
+        hr = k.rho / 2.0;
+        hr137 = 1.37 * hr;
+        d1lg = k.d1 * k.lg;
+        d2lg = k.d2 * k.lg;
+        iA1 = 1.0 / k.A1;
+        k1e = k.k1 * k.etak1;
+        k2e = k.k2 * k.etak2;
+        for (int c = 0; c < 2; c++) {
+            const double h1u = c ? k.h1 : 0.0, r1u = c ? k.r1c : k.r1o;
+            const double h2u = c ? k.h2 : 0.0, r2u = c ? k.r2c : k.r2o;
+            a11[c] = (k.k1 + h1u + k.kc) * is2 + r1u * isr + k.m1;
+            a22[c] = (k.k2 + h2u + k.kc) * is2 + r2u * isr + k.m2;
+            b1c[c] = 2.0 * k.m1 + r1u * isr;
+            b2c[c] = 2.0 * k.m2 + r2u * isr;
+        }
+        a12 = -k.kc * is2;
+        for (int c1 = 0; c1 < 2; c1++)
+            for (int c2 = 0; c2 < 2; c2++) {
+                double det = a11[c1] * a22[c2] - a12 * a12;
+                if (det == 0.0) det = 1.0;
+                idet[c1][c2] = 1.0 / det;
+            }
+    }
+
+    /* one step with supraglottal pressure p1; returns the new flow */
+    double step(double p1) {
+        const double x1c = k.x1_curr, x2c = k.x2_curr, ug = k.ug_curr, ugo = k.ug_old;
+        const double ia1 = 1.0 / (k.Ag01 + two_lg * x1c);
+        const double ia2 = 1.0 / (k.Ag02 + two_lg * x2c);
+        const double ia1s = ia1 * ia1, ia2s = ia2 * ia2;
+        const double Rv1 = cR1 * (ia1s * ia1), Lg1 = cL1 * ia1;
+        const double Rv2 = cR2 * (ia2s * ia2), Lg2 = cL2 * ia2;
+        const double dug = ug - ugo;
+        const bool open1 = x1c > -g1, open2 = x2c > -g2;
+        double pm1 = k.ps;
+        if (open1 && open2) {
+            const double q = ug * ia1;
+            pm1 = k.ps - hr137 * (q * q) - 0.5 * (Rv1 * ug + srate * (Lg1 * dug));
+        }
+        const double fm1 = d1lg * pm1;
+        double pm2 = 0.0;
+        if (open1) {
+            if (open2)
+                pm2 = pm1 - (0.5 * (Rv1 + Rv2) * ug + srate * ((Lg1 + Lg2) * dug)) - hr * (ug * ug) * (ia2s - ia1s);
+            else
+                pm2 = k.ps;
+        }
+        const double fm2 = d2lg * pm2;
+        const int c1 = x1c + g1 < 0.0, c2 = x2c + g2 < 0.0;
+        const double e1 = g1 + x1c, e2 = g2 + x2c;
+        const double s1 = k1e * (x1c * x1c * x1c) + (c1 ? k.h1 : 0.0) * (g1 + k.etah1 * (e1 * e1 * e1));
+        const double s2 = k2e * (x2c * x2c * x2c) + (c2 ? k.h2 : 0.0) * (g2 + k.etah2 * (e2 * e2 * e2));
+        const double b1 = b1c[c1] * x1c - k.m1 * k.x1_old + (fm1 - s1) * is2;
+        const double b2 = b2c[c2] * x2c - k.m2 * k.x2_old + (fm2 - s2) * is2;
+        const double id = idet[c1][c2];
+        const double x1n = (a22[c2] * b1 - a12 * b2) * id;
+        const double x2n = (a11[c1] * b2 - a12 * b1) * id;
+        const double Ag1 = k.Ag01 + two_lg * x1n;
+        const double Ag2 = k.Ag02 + two_lg * x2n;
+        double ugn = 0.0;
+        if (!(Ag1 < 0 || Ag2 < 0)) {
+            const double ja1 = 1.0 / Ag1, ja2 = 1.0 / Ag2;
+            const double ja1s = ja1 * ja1, ja2s = ja2 * ja2;
+            const double r = Ag2 * iA1;
+            const double Rtot = hr * std::fabs(ug) * (0.37 * ja1s + (1.0 - 2.0 * r * (1.0 - r)) * ja2s) +
+                                c12 * (k.d1 * (ja1s * ja1) + k.d2 * (ja2s * ja2));
+            const double Ltot = cL1 * ja1 + cL2 * ja2;
+            ugn = ((k.ps - p1) * isr + Ltot * ug) / (Rtot * isr + Ltot);
+        }
+        k.x1_old = x1c; k.x1_curr = x1n;
+        k.x2_old = x2c; k.x2_curr = x2n;
+        k.ug_old = ug; k.ug_curr = ugn;
+        return ugn;
+    }
+};
+
 /* ---- the time loop ---------------------------------------------------------
  * FDTDEngineCPU::startSolverEngine (FDTDEngineCPU.cpp:222-304) with its three
  * passes (:306-433), the full-frame wall ODE and the PV_N = PV_Nplus1 copy.
@@ -797,8 +901,10 @@ int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long ste
     source_table<T>(p, steps, (double)G.k.dt, src);
     TwoMass<T> tmm;
     tmm.init(p->tmm_ps_pa);
-    TwoMass<double> tmm64;                /* tmm_f64: the model in double, fields in T */
+    TwoMass<double> tmm64;                /* tmm_f64 with double fields: the literal model in double */
     tmm64.init(p->tmm_ps_pa);
+    TwoMassR tmmR;                        /* tmm_f64 with float fields: the GPU's arrangement */
+    tmmR.init(p->tmm_ps_pa, p->srate_mul);
     T K1, K2;
     if (sizeof(T) == 4) { K1 = (T)G.K1; K2 = (T)G.K2; }
     else {
@@ -814,7 +920,9 @@ int run_engine(const vs_params* p, const Grid& G, const Coeffs& C, long long ste
 
     for (long long ts = 0; ts < steps; ts++) {
         T exeV;
-        if (p->source_type == VS_SRC_TMM && p->tmm_f64) {
+        if (p->source_type == VS_SRC_TMM && p->tmm_f64 && sizeof(T) == 4) {
+            exeV = (T)tmmR.step((double)PN[exc].Pr);
+        } else if (p->source_type == VS_SRC_TMM && p->tmm_f64) {
             tmm64.p1 = (double)PN[exc].Pr;
             tmm64.step(p->srate_mul);
             exeV = (T)tmm64.ug_next;
@@ -1046,6 +1154,14 @@ int orc_tmm_f64(float ps, int srate_mul, const double* p1, long long n, double* 
     TwoMass<double> m;
     m.init(ps);
     for (long long i = 0; i < n; i++) { m.p1 = p1[i]; m.step(srate_mul); ug[i] = m.ug_next; }
+    return VS_OK;
+}
+
+/* The tmm_f64 option's arrangement of the double model (TwoMassR). */
+int orc_tmm_f64r(float ps, int srate_mul, const double* p1, long long n, double* ug) {
+    TwoMassR m;
+    m.init(ps, srate_mul);
+    for (long long i = 0; i < n; i++) ug[i] = m.step(p1[i]);
     return VS_OK;
 }
 

@@ -59,6 +59,20 @@ def test_two_mass_model_free_oscillation(mul):
     assert ug.max() > 1e-4          # the folds oscillate and let air through
 
 
+@pytest.mark.parametrize("mul", [15, 30])
+def test_double_model_arrangement_tracks_the_literal_double_model(mul):
+    """The tmm_f64 option's arrangement of the double model (per-model
+    reciprocals, three divisions a step) against the model's literal
+    expressions in double: the same flows to rounding, driven by the golden
+    random pressures and in free oscillation over 20 000 steps."""
+    for p1 in (G[f"tmm_p1_{mul}"].astype(np.float64), np.zeros(20000)):
+        lit = O.tmm(686.46, mul, p1, "f64")
+        arr = O.tmm(686.46, mul, p1, "f64r")
+        assert np.abs(lit).max() > 1e-4
+        assert np.linalg.norm(arr - lit) <= 1e-9 * np.linalg.norm(lit)
+        assert np.abs(arr - lit).max() <= 1e-9 * np.abs(lit).max()
+
+
 def test_double_two_mass_model_tracks_the_fp64_restatement():
     """FP32 fields with the two-mass model in double (tmm_f64) stay within
     1e-4 relative L2 of the all-double run; the reference's float model

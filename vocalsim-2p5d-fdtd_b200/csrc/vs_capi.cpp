@@ -866,6 +866,7 @@ void create_batch(int n, const vs_params* params, const vs_geometry* geoms, vs_b
         for (int k = 0; k < 13; ++k) t.sigma[k] = g.sigma[k];
         t.tmmc = g.tmmc;
         t.tmmd = g.tmmd;
+        t.tmmx = g.tmmx;
     }
     ck(cudaMalloc(&b->d_tubes, n * sizeof(TubeDev)), "cudaMalloc(tubes)");
     ck(cudaMalloc(&b->d_rs, sizeof(RunState)), "cudaMalloc(run state)");

@@ -137,78 +137,77 @@ __device__ __noinline__ float tmm_step(const TmmConsts& k, TmmState& s, float p1
     return tmm_finish(o, s, p1);
 }
 
-// The same model step with every quantity in double (tmm_f64), following
-// TwoMassModel.cpp:90-232 operation by operation; the caller's pressure is
-// widened and the flow rounded to float for the field update.
+// The same model step with every quantity in double (tmm_f64): the
+// expressions of TwoMassModel.cpp:90-232 with the per-tube constants taken
+// from TmmDerived64 (reciprocals of the sample rate, the thresholds, the
+// displacement-update matrix and its inverse determinant per contact state),
+// so that a step divides only by the glottal openings before and after the
+// displacement update and by the flow denominator.  The order of operations
+// is the model's own (it is this build's option, not the reference's float
+// arithmetic): the FP32 oracle's tmm_f64 path performs the same operations,
+// and the FP64 oracle keeps the literal expressions as the accuracy reference.
+// The caller's pressure is widened and the flow rounded to float for the
+// field update.
 struct TmmPrep64 {
     double x1, x1n, x2, x2n, ug;
-    double Lug, den, srate, ps;     // ugn = ((ps - p1) / srate + Lug) / den
+    double Lug, den, isr, ps;       // ugn = ((ps - p1) isr + Lug) / den
     bool closed;
 };
 
-__device__ __forceinline__ TmmPrep64 tmm_prepare64(const TmmConsts64& k, const TmmState64& s) {
-    const double srate = k.srate, ss = srate * srate;
+__device__ __forceinline__ TmmPrep64 tmm_prepare64(const TmmConsts64& k, const TmmDerived64& d,
+                                                   const TmmState64& s) {
     const double x1c = s.x1_curr, x2c = s.x2_curr, ug = s.ug_curr, ugo = s.ug_old;
-    double Ag1 = k.Ag01 + 2 * k.lg * x1c;
-    double Ag2 = k.Ag02 + 2 * k.lg * x2c;
-    const double Rv1 = (12 * k.mu * k.lg * k.lg * k.d1) / (Ag1 * Ag1 * Ag1);
-    const double Lg1 = (k.rho * k.d1) / Ag1;
-    const double Rv2 = (12 * k.mu * k.lg * k.lg * k.d2) / (Ag2 * Ag2 * Ag2);
-    const double Lg2 = (k.rho * k.d2) / Ag2;
-    double pm1, pm2;
-    if (x1c > -k.Ag01 / (2 * k.lg) && x2c > -k.Ag02 / (2 * k.lg))
-        pm1 = k.ps - 1.37 * (k.rho / 2) * (ug / Ag1) * (ug / Ag1) - 0.5 * (Rv1 * ug + Lg1 * srate * (ug - ugo));
-    else
-        pm1 = k.ps;
-    const double fm1 = pm1 * k.d1 * k.lg;
-    if (x1c > -k.Ag01 / (2 * k.lg)) {
-        if (x2c > -k.Ag02 / (2 * k.lg))
-            pm2 = pm1 - (0.5 * (Rv1 + Rv2) * ug + (Lg1 + Lg2) * (ug - ugo) * srate) -
-                  (k.rho / 2 * ug * ug) * (1 / (Ag2 * Ag2) - 1 / (Ag1 * Ag1));
-        else
-            pm2 = k.ps;
-    } else {
-        pm2 = 0;
+    const double ia1 = 1.0 / (k.Ag01 + d.two_lg * x1c);
+    const double ia2 = 1.0 / (k.Ag02 + d.two_lg * x2c);
+    const double ia1s = ia1 * ia1, ia2s = ia2 * ia2;
+    const double Rv1 = d.cR1 * (ia1s * ia1), Lg1 = d.cL1 * ia1;
+    const double Rv2 = d.cR2 * (ia2s * ia2), Lg2 = d.cL2 * ia2;
+    const double dug = ug - ugo;
+    const bool open1 = x1c > -d.g1, open2 = x2c > -d.g2;
+    double pm1 = k.ps;
+    if (open1 && open2) {
+        const double q = ug * ia1;
+        pm1 = k.ps - d.hr137 * (q * q) - 0.5 * (Rv1 * ug + k.srate * (Lg1 * dug));
     }
-    const double fm2 = pm2 * k.d2 * k.lg;
-    double h1u, r1u, h2u, r2u;
-    if (x1c + k.Ag01 / (2 * k.lg) < 0) { h1u = k.h1; r1u = k.r1c; } else { h1u = 0; r1u = k.r1o; }
-    if (x2c + k.Ag02 / (2 * k.lg) < 0) { h2u = k.h2; r2u = k.r2c; } else { h2u = 0; r2u = k.r2o; }
-    const double a11 = (k.k1 + h1u + k.kc) / ss + r1u / srate + k.m1;
-    const double a12 = -k.kc / ss;
-    const double a21 = a12;
-    const double a22 = (k.k2 + h2u + k.kc) / ss + r2u / srate + k.m2;
-    const double g1 = k.Ag01 / (2 * k.lg), g2 = k.Ag02 / (2 * k.lg);
-    const double s1 = k.k1 * k.etak1 * x1c * x1c * x1c + h1u * (g1 + k.etah1 * (g1 + x1c) * (g1 + x1c) * (g1 + x1c));
-    const double s2 = k.k2 * k.etak2 * x2c * x2c * x2c + h2u * (g2 + k.etah2 * (g2 + x2c) * (g2 + x2c) * (g2 + x2c));
-    const double b1 = (2 * k.m1 + r1u / srate) * x1c - k.m1 * s.x1_old - s1 / ss + fm1 / ss;
-    const double b2 = (2 * k.m2 + r2u / srate) * x2c - k.m2 * s.x2_old - s2 / ss + fm2 / ss;
-    double det = a11 * a22 - a21 * a12;
-    if (det == 0) det = 1;
-    const double x1n = (a22 * b1 - a12 * b2) / det;
-    const double x2n = (a11 * b2 - a21 * b1) / det;
+    const double fm1 = d.d1lg * pm1;
+    double pm2 = 0.0;
+    if (open1)
+        pm2 = open2 ? pm1 - (0.5 * (Rv1 + Rv2) * ug + k.srate * ((Lg1 + Lg2) * dug)) - d.hr * (ug * ug) * (ia2s - ia1s)
+                    : k.ps;
+    const double fm2 = d.d2lg * pm2;
+    const int c1 = x1c + d.g1 < 0.0, c2 = x2c + d.g2 < 0.0;
+    const double e1 = d.g1 + x1c, e2 = d.g2 + x2c;
+    const double s1 = d.k1e * (x1c * x1c * x1c) + (c1 ? k.h1 : 0.0) * (d.g1 + k.etah1 * (e1 * e1 * e1));
+    const double s2 = d.k2e * (x2c * x2c * x2c) + (c2 ? k.h2 : 0.0) * (d.g2 + k.etah2 * (e2 * e2 * e2));
+    const double b1 = d.b1c[c1] * x1c - k.m1 * s.x1_old + (fm1 - s1) * d.is2;
+    const double b2 = d.b2c[c2] * x2c - k.m2 * s.x2_old + (fm2 - s2) * d.is2;
+    const double idet = d.idet[c1][c2];
+    const double x1n = (d.a22[c2] * b1 - d.a12 * b2) * idet;
+    const double x2n = (d.a11[c1] * b2 - d.a12 * b1) * idet;
     TmmPrep64 o;
     o.x1 = x1c; o.x1n = x1n; o.x2 = x2c; o.x2n = x2n; o.ug = ug;
-    o.srate = srate; o.ps = k.ps;
-    Ag1 = k.Ag01 + 2 * k.lg * x1n;
-    Ag2 = k.Ag02 + 2 * k.lg * x2n;
+    o.isr = d.isr; o.ps = k.ps;
+    const double Ag1 = k.Ag01 + d.two_lg * x1n;
+    const double Ag2 = k.Ag02 + d.two_lg * x2n;
     o.closed = Ag1 < 0 || Ag2 < 0;
     o.Lug = 0;
     o.den = 1;
     if (!o.closed) {
-        const double Rtot = (k.rho / 2) * fabs(ug) *
-                                ((0.37 / (Ag1 * Ag1)) + (1 - 2 * (Ag2 / k.A1) * (1 - Ag2 / k.A1)) / (Ag2 * Ag2)) +
-                            (12 * k.mu * k.lg * k.lg * (k.d1 / (Ag1 * Ag1 * Ag1) + k.d2 / (Ag2 * Ag2 * Ag2)));
-        const double Ltot = k.rho * (k.d1 / Ag1 + k.d2 / Ag2);
+        const double ja1 = 1.0 / Ag1, ja2 = 1.0 / Ag2;
+        const double ja1s = ja1 * ja1, ja2s = ja2 * ja2;
+        const double r = Ag2 * d.iA1;
+        const double Rtot = d.hr * fabs(ug) * (0.37 * ja1s + (1.0 - 2.0 * r * (1.0 - r)) * ja2s) +
+                            d.c12 * (k.d1 * (ja1s * ja1) + k.d2 * (ja2s * ja2));
+        const double Ltot = d.cL1 * ja1 + d.cL2 * ja2;
         o.Lug = Ltot * ug;
-        o.den = Rtot / srate + Ltot;
+        o.den = Rtot * d.isr + Ltot;
     }
     return o;
 }
 
 __device__ __forceinline__ float tmm_finish64(const TmmPrep64& o, TmmState64& s, float p1f) {
     const double p1 = (double)p1f;
-    const double ugn = o.closed ? 0.0 : ((o.ps - p1) / o.srate + o.Lug) / o.den;
+    const double ugn = o.closed ? 0.0 : ((o.ps - p1) * o.isr + o.Lug) / o.den;
     s.x1_old = o.x1; s.x1_curr = o.x1n;
     s.x2_old = o.x2; s.x2_curr = o.x2n;
     s.ug_old = o.ug;
@@ -216,8 +215,8 @@ __device__ __forceinline__ float tmm_finish64(const TmmPrep64& o, TmmState64& s,
     return (float)ugn;
 }
 
-__device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, float p1f) {
-    const TmmPrep64 o = tmm_prepare64(k, s);
+__device__ __noinline__ float tmm_step64(const TmmConsts64& k, const TmmDerived64& d, TmmState64& s, float p1f) {
+    const TmmPrep64 o = tmm_prepare64(k, d, s);
     return tmm_finish64(o, s, p1f);
 }
 
@@ -227,7 +226,7 @@ __device__ __noinline__ float tmm_step64(const TmmConsts64& k, TmmState64& s, fl
 __device__ __noinline__ float glottal_step(const TubeDev* T, int par, float p1, bool store, double* hist) {
     if (T->flags & TUBE_TMM64) {
         TmmState64 s = T->tmm64[par];
-        const float e = tmm_step64(T->tmmd, s, p1);
+        const float e = tmm_step64(T->tmmd, T->tmmx, s, p1);
         if (store) {
             T->tmm64[par ^ 1] = s;
             if (hist) {
@@ -265,9 +264,9 @@ __device__ __noinline__ float2 glottal_two_steps(const TubeDev* T, int par, bool
     float2 e;
     if (T->flags & TUBE_TMM64) {
         TmmState64 s = from_x ? *T->tmm64_x : T->tmm64[par];
-        e.x = tmm_step64(T->tmmd, s, p1);
+        e.x = tmm_step64(T->tmmd, T->tmmx, s, p1);
         if (store && hist) tmm_to_hist(s, hist);
-        e.y = tmm_step64(T->tmmd, s, p2);
+        e.y = tmm_step64(T->tmmd, T->tmmx, s, p2);
         if (store && hist) tmm_to_hist(s, hist + 6);
         if (store) *(from_x ? &T->tmm64[par] : T->tmm64_x) = s;
     } else {

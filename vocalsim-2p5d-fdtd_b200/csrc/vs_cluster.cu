@@ -179,7 +179,7 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
         else s32 = T->tmm[par0];
     }
     auto tmm_prepare_next = [&]() {
-        if (tmm64) prep64 = tmm_prepare64(T->tmmd, s64);
+        if (tmm64) prep64 = tmm_prepare64(T->tmmd, T->tmmx, s64);
         else prep32 = tmm_prepare(T->tmmc, s32);
     };
     auto tmm_finish_next = [&](float p1) -> float {
@@ -373,7 +373,7 @@ struct TmmSlot {
 };
 
 __device__ __noinline__ void tmm_slot_prepare(const TubeDev* __restrict__ T, TmmSlot* slot, bool tmm64) {
-    if (tmm64) slot->prep64 = tmm_prepare64(T->tmmd, slot->s64);
+    if (tmm64) slot->prep64 = tmm_prepare64(T->tmmd, T->tmmx, slot->s64);
     else slot->prep32 = tmm_prepare(T->tmmc, slot->s32);
 }
 

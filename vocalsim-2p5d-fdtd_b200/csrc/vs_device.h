@@ -62,6 +62,7 @@ struct TubeDev {
     TmmState64* tmm64_x;
     TmmConsts tmmc;
     TmmConsts64 tmmd;     // the double model's constants, else tmmc widened (adjoint)
+    TmmDerived64 tmmx;    // the double model's derived constants
     // state history for the adjoint's recomputation (strip kernel with
     // history capture only): the state after step n goes to slot
     // n + 1 - RunState::run_start, slot = [P, Vx, Vy] planes, `plane` apart

@@ -646,10 +646,48 @@ static TmmConsts64 widen(const TmmConsts& c) {
             c.etah2, c.Ag01, c.Ag02, c.lg, c.r1o, c.r2o, c.r1c, c.r2c, c.A1, c.ps, c.srate};
 }
 
+TmmDerived64 tmm_derived(const TmmConsts64& k) {
+    TmmDerived64 d{};
+    d.isr = 1.0 / k.srate;
+    d.is2 = d.isr * d.isr;
+    d.two_lg = 2.0 * k.lg;
+    d.g1 = k.Ag01 / d.two_lg;
+    d.g2 = k.Ag02 / d.two_lg;
+    d.c12 = 12.0 * k.mu * k.lg * k.lg;
+    d.cR1 = d.c12 * k.d1;
+    d.cR2 = d.c12 * k.d2;
+    d.cL1 = k.rho * k.d1;
+    d.cL2 = k.rho * k.d2;
+    d.hr = k.rho / 2.0;
+    d.hr137 = 1.37 * d.hr;
+    d.d1lg = k.d1 * k.lg;
+    d.d2lg = k.d2 * k.lg;
+    d.iA1 = 1.0 / k.A1;
+    d.k1e = k.k1 * k.etak1;
+    d.k2e = k.k2 * k.etak2;
+    for (int c = 0; c < 2; ++c) {
+        const double h1u = c ? k.h1 : 0.0, r1u = c ? k.r1c : k.r1o;
+        const double h2u = c ? k.h2 : 0.0, r2u = c ? k.r2c : k.r2o;
+        d.a11[c] = (k.k1 + h1u + k.kc) * d.is2 + r1u * d.isr + k.m1;
+        d.a22[c] = (k.k2 + h2u + k.kc) * d.is2 + r2u * d.isr + k.m2;
+        d.b1c[c] = 2.0 * k.m1 + r1u * d.isr;
+        d.b2c[c] = 2.0 * k.m2 + r2u * d.isr;
+    }
+    d.a12 = -k.kc * d.is2;
+    for (int c1 = 0; c1 < 2; ++c1)
+        for (int c2 = 0; c2 < 2; ++c2) {
+            double det = d.a11[c1] * d.a22[c2] - d.a12 * d.a12;
+            if (det == 0.0) det = 1.0;
+            d.idet[c1][c2] = 1.0 / det;
+        }
+    return d;
+}
+
 static void fill_tmm(const vs_params* p, TubeGrid& out) {
     out.tmmc = tmm_consts<float>(p->tmm_ps_pa, p->srate_mul);
     out.tmm64 = p->source_type == VS_SRC_TMM && p->tmm_f64 != 0;
     out.tmmd = out.tmm64 ? tmm_consts<double>(p->tmm_ps_pa, p->srate_mul) : widen(out.tmmc);
+    out.tmmx = tmm_derived(out.tmmd);
 }
 
 void build_tube(const vs_params* p, const vs_geometry* g, TubeGrid& out, int64_t steps_for_source) {

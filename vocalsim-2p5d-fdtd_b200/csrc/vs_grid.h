@@ -32,6 +32,18 @@ struct TmmConstsT {
 using TmmConsts = TmmConstsT<float>;
 using TmmConsts64 = TmmConstsT<double>;
 
+// Per-tube constants of the double two-mass model (tmm_f64), derived once
+// from its TmmConsts64 by tmm_derived(): reciprocals of the sample rate and of
+// its square, the opening thresholds, the products the step multiplies by,
+// and the matrix of the displacement update with its inverse determinant for
+// each contact state of the two masses ([0] open, [1] closed).  With them a
+// step divides only by the two glottal openings, before and after the update,
+// and by the flow denominator.
+struct TmmDerived64 {
+    double isr, is2, two_lg, g1, g2, c12, cR1, cR2, cL1, cL2, hr, hr137, d1lg, d2lg, iA1, k1e, k2e;
+    double a11[2], a22[2], a12, b1c[2], b2c[2], idet[2][2];
+};
+
 // Two-mass model state carried from step to step (the members the reference
 // reads before writing in runTwoMassModel).
 template <class F>
@@ -65,6 +77,7 @@ struct TubeGrid {
     TmmConsts tmmc{};
     bool tmm64 = false;               // two-mass model in double (vs_params::tmm_f64)
     TmmConsts64 tmmd{};               // double constants: the double model's, else tmmc widened
+    TmmDerived64 tmmx{};              // the double model's derived constants
     vs_params src_params{};           // parameters the source table is rebuilt from
     // tube rasterisation (empty for the open-space domain)
     std::vector<int32_t> upper, lower, colseg;   // per tube column: wall rows, 0-based segment
@@ -111,5 +124,8 @@ void build_source(const vs_params* p, float dt, int64_t n, std::vector<float>& o
 // pressure, in float (the reference's) or double.
 template <class F>
 TmmConstsT<F> tmm_consts(float ps, int srate_mul);
+
+// The double model's derived constants (TmmDerived64) of constants k.
+TmmDerived64 tmm_derived(const TmmConsts64& k);
 
 }  // namespace vsb

@@ -221,6 +221,7 @@ extern "C" int vs_run_noalloc(const vs_params* p, const vs_dims* dims, const int
     for (int j = 0; j < 13; ++j) t.sigma[j] = k.sigma[j];
     t.tmmc = k.tmmc;
     t.tmmd = k.tmmd;
+    t.tmmx = k.tmmx;
 
     RunState rs;
     std::memset(&rs, 0, sizeof(rs));
