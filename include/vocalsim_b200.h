@@ -236,12 +236,13 @@ int vs_batch_set_stream(vs_batch* b, void* cuda_stream);
 
 /* Select the tile shape used by the step kernel (index into the compiled
  * shape table, see vs_tile_shape) or -1 for the default choice.  The last
- * shape of the table is the cluster kernel: a batch of one tube without the
- * coupled wall oscillator keeps its state in the shared memory of one
- * thread-block cluster (up to 16 CTAs, one band of rows each, halo rows
- * exchanged through distributed shared memory) and runs every step of a
- * vs_batch_run / vs_run call in one launch; it is the default for such
- * batches when the band fits a CTA's shared memory. */
+ * shape of the table is the cluster kernel: each tube of a batch without the
+ * coupled wall oscillator (up to 64 tubes, each with at least one interior
+ * row per CTA) keeps its state on its own thread-block cluster (up to 16
+ * CTAs, one band of rows each, halo rows exchanged through distributed shared
+ * memory; the configuration sized for the largest frame) and runs every step
+ * of a vs_batch_run / vs_run call in one launch.  It is the default for a
+ * single tube, and for a batch whose clusters are all resident at once. */
 int vs_batch_set_tile(vs_batch* b, int32_t tile_index);
 
 /* Device time of the last vs_batch_adjoint call, split into the segments'

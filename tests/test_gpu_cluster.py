@@ -110,3 +110,60 @@ def test_cluster_full_length_config1_equals_step_kernels(cuda_ok):
     b = r.run(33075)[0]
     assert np.array_equal(a, b)
     assert np.all(np.isfinite(a)) and np.abs(a).max() > 0
+
+
+BATCH_KWS = [dict(cross_sectional_shape=2),
+             dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0),
+             dict(cross_sectional_shape=2, source_type=2, tmm_ps_pa=800.0, tmm_f64=1),
+             dict(cross_sectional_shape=1, mouth_radiation_cond=1),
+             dict(cross_sectional_shape=2, engine=2),
+             dict(cross_sectional_shape=1, source_type=0)]
+
+
+@pytest.mark.parametrize("fast", [0, 1])
+def test_cluster_batch_equals_the_step_kernels(fast, cuda_ok):
+    """A small batch on the cluster shape: every tube on its own thread-block
+    cluster in one launch (the configuration sized for the largest frame),
+    with table and two-mass sources (float and double model), a Dirichlet
+    mouth and the Eigen denominator mixed.  Runs split over several calls of
+    odd and even lengths give the step kernels' traces and final fields bit
+    for bit (reference arithmetic and fast_math)."""
+    tubes = [S.batch_tube(i)[:2] for i in range(len(BATCH_KWS))]
+    ps = [V.params(fast_math=fast, **k) for k in BATCH_KWS]
+    gs = [V.Geometry(L, A) for L, A in tubes]
+    segments = [1, 300, 2, 129, 40]
+    out = {}
+    for shape in (CLUSTER, 0 if not fast else 17):
+        b = V.Batch(ps, gs)
+        b.set_tile(shape)
+        tr = np.concatenate([b.run(m) for m in segments], axis=1)
+        out[shape] = (tr, [b.fields(i) for i in range(len(ps))])
+        b.close()
+    (ca, fa), (sa, fb) = out.values()
+    assert np.array_equal(ca, sa), f"tube {int(np.argmax(np.any(ca != sa, axis=1)))}"
+    for x, y in zip(fa, fb):
+        for a, c in zip(x, y):
+            assert np.array_equal(a, c)
+    assert np.all(np.abs(ca).max(axis=1) > 0)
+    if not fast:
+        for i in (0, 1, 2):
+            o = O.run(O.params(**BATCH_KWS[i]), O.Geometry(*tubes[i]), sum(segments), "f32")
+            assert np.array_equal(ca[i], o), f"tube {i} against the oracle"
+
+
+def test_cluster_batch_more_tubes_than_resident_clusters(cuda_ok):
+    """More tubes than clusters fit on the device at once: the clusters of
+    later waves start from the same step (the step counter advances after the
+    launch) and every tube's trace equals the step kernels'."""
+    n = 40
+    tubes = [S.batch_tube(i % 12)[:2] for i in range(n)]
+    ps = [V.params(cross_sectional_shape=2, fast_math=1) for _ in range(n)]
+    gs = [V.Geometry(L, A) for L, A in tubes]
+    res = []
+    for shape in (CLUSTER, 17):
+        b = V.Batch(ps, gs)
+        b.set_tile(shape)
+        res.append(np.concatenate([b.run(257), b.run(64)], axis=1))
+        b.close()
+    assert np.array_equal(res[0], res[1])
+    assert np.all(np.abs(res[0]).max(axis=1) > 0)

@@ -92,7 +92,7 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
     cg::cluster_group cluster = cg::this_cluster();
     const int C = (int)cluster.num_blocks();
     const int k = (int)cluster.block_rank();
-    const TubeDev* __restrict__ T = Tp;
+    const TubeDev* __restrict__ T = Tp + blockIdx.y;          // one cluster per tube of the batch
     const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
     const ClusterLayout L = cluster_layout(pitch, R, FAST);
     float* sf = reinterpret_cast<float*>(c_smem);
@@ -113,7 +113,7 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
     const int Rk = r1 - r0 + 1;
     const int64_t n0 = rs->step;
     const int64_t run_start = rs->run_start;
-    float* __restrict__ trace = rs->trace;
+    float* __restrict__ trace = rs->trace + (int64_t)blockIdx.y * rs->trace_stride;
     const int par0 = (int)(n0 & 1);
     const int64_t pl = T->plane;
     const float* __restrict__ gP = T->P[0] + par0 * pl;
@@ -325,7 +325,6 @@ cluster_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, int64_
         if (tmm64) T->tmm64[pe] = s64;
         else T->tmm[pe] = s32;
     }
-    if (k == 0 && tid == 0) rs->step = n_end;    // every CTA read rs->step before the first cluster barrier
 }
 
 // ---------------------------------------------------------------------------
@@ -454,7 +453,7 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     cg::cluster_group cluster = cg::this_cluster();
     const int C = (int)cluster.num_blocks();
     const int k = (int)cluster.block_rank();
-    const TubeDev* __restrict__ T = Tp;
+    const TubeDev* __restrict__ T = Tp + blockIdx.y;          // one cluster per tube of the batch
     const int H = T->H, W = T->W, pitch = T->pitch, flags = T->flags;
     const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
     // point to point with the two-mass source: the last warp runs the model
@@ -481,7 +480,7 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
     const int Rk = r1 - r0 + 1;                               // 1 .. RMAX
     const int64_t n0 = rs->step;
     const int64_t run_start = rs->run_start;
-    float* __restrict__ trace = rs->trace;
+    float* __restrict__ trace = rs->trace + (int64_t)blockIdx.y * rs->trace_stride;
     const int par0 = (int)(n0 & 1);
     const int64_t pl = T->plane;
     const float* __restrict__ gP = T->P[0] + par0 * pl;
@@ -860,7 +859,6 @@ cluster_reg_kernel(const TubeDev* __restrict__ Tp, RunState* __restrict__ rs, in
         if (tmm64) T->tmm64[pe] = slot->s64;
         else T->tmm[pe] = slot->s32;
     }
-    if (k == 0 && tid == 0) rs->step = n_end;
 }
 
 }  // namespace
@@ -958,6 +956,7 @@ bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig*
         out->smem = smem;
         out->form = form;
         out->rmax = rmax;
+        out->nclusters = nclusters;
         return true;
     }
     cudaGetLastError();
@@ -965,31 +964,39 @@ bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig*
 }
 
 cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps, bool fast, const ClusterConfig& c,
-                               cudaStream_t stream) {
-    if (steps <= 0) return cudaSuccess;
+                               cudaStream_t stream, int ntubes) {
+    if (steps <= 0 || ntubes <= 0) return cudaSuccess;
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = c.ctas;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(c.ctas);
+    cfg.gridDim = dim3(c.ctas, ntubes);                      // clusters along x, a tube per grid row
     cfg.blockDim = dim3(c.threads);
     cfg.dynamicSmemBytes = c.smem;
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    cudaError_t e;
     if (c.form == 1)
-        return fast ? launch_reg<true, 0>(cfg, c.rmax, c.cols, tube, rs, steps)
-                    : launch_reg<false, 0>(cfg, c.rmax, c.cols, tube, rs, steps);
-    if (c.form == 2)
-        return fast ? launch_reg<true, 1>(cfg, c.rmax, c.cols, tube, rs, steps)
-                    : launch_reg<false, 1>(cfg, c.rmax, c.cols, tube, rs, steps);
-    if (c.form == 3)
-        return fast ? launch_reg<true, 2>(cfg, c.rmax, c.cols, tube, rs, steps)
-                    : launch_reg<false, 2>(cfg, c.rmax, c.cols, tube, rs, steps);
-    if (fast) return cudaLaunchKernelEx(&cfg, cluster_kernel<true>, tube, rs, steps, c.rows_max);
-    return cudaLaunchKernelEx(&cfg, cluster_kernel<false>, tube, rs, steps, c.rows_max);
+        e = fast ? launch_reg<true, 0>(cfg, c.rmax, c.cols, tube, rs, steps)
+                 : launch_reg<false, 0>(cfg, c.rmax, c.cols, tube, rs, steps);
+    else if (c.form == 2)
+        e = fast ? launch_reg<true, 1>(cfg, c.rmax, c.cols, tube, rs, steps)
+                 : launch_reg<false, 1>(cfg, c.rmax, c.cols, tube, rs, steps);
+    else if (c.form == 3)
+        e = fast ? launch_reg<true, 2>(cfg, c.rmax, c.cols, tube, rs, steps)
+                 : launch_reg<false, 2>(cfg, c.rmax, c.cols, tube, rs, steps);
+    else if (fast)
+        e = cudaLaunchKernelEx(&cfg, cluster_kernel<true>, tube, rs, steps, c.rows_max);
+    else
+        e = cudaLaunchKernelEx(&cfg, cluster_kernel<false>, tube, rs, steps, c.rows_max);
+    // the step counter advances after every cluster has run: a cluster of a
+    // later wave reads RunState::step when it starts
+    for (int64_t left = steps; e == cudaSuccess && left > 0; left -= INT32_MAX)
+        e = launch_advance(rs, (int)std::min<int64_t>(left, INT32_MAX), stream);
+    return e;
 }
 
 }  // namespace vsb

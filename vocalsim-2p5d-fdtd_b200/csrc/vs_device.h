@@ -202,6 +202,7 @@ struct ClusterConfig {
                           // cluster barrier per step; 2: the same, neighbour-to-neighbour exchange;
                           // 3: form 2 with the two-mass model in an extra warp
     int rmax = 0;
+    int nclusters = 0;    // clusters of this configuration resident on the device at once
 };
 // Cluster size (16, 8 or 4 CTAs), threads and shared memory for a tube of
 // H x W cells (row pitch `pitch`) on the current device, or false when none
@@ -209,11 +210,13 @@ struct ClusterConfig {
 // two-mass source (its excitation value reaches every CTA each step, which
 // the cluster barrier form does faster than the neighbour exchange).
 bool cluster_config(int H, int W, int pitch, bool fast, bool tmm, ClusterConfig* out);
-// `steps` time steps of the tube at `tube` (device) from RunState::step, in
-// one launch; RunState::step advances by `steps`.  The state must be in its
-// parity set (bsel = 0) and stays there.
+// `steps` time steps of the `ntubes` tubes from `tube` on (device), one
+// thread-block cluster per tube (configuration c, sized for the largest of
+// them), from RunState::step, in one launch; then RunState::step advances by
+// `steps` (a separate launch).  The states must be in their parity sets
+// (bsel = 0) and stay there.
 cudaError_t launch_cluster_run(const TubeDev* tube, RunState* rs, int64_t steps, bool fast, const ClusterConfig& c,
-                               cudaStream_t stream);
+                               cudaStream_t stream, int ntubes = 1);
 
 // Launch one time step (local index `local` after RunState::step) of every
 // strip or band in `tiles` with the compiled shape `shape`; `wall` selects
