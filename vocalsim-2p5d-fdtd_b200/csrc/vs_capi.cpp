@@ -317,10 +317,11 @@ int single_step_shape(const vs_batch* b) {
 
 int default_shape(const vs_batch* b) {
     // a single tube keeps its state on one thread-block cluster for the whole
-    // run, and so does every tube of a batch whose clusters are resident at
-    // once (measured, fast_math: 2 and 4 tubes 1.36 us per step against 2.6
-    // on the strips; past one wave of clusters the strips win)
-    if (shape_fits(b, cluster_shape()) && (int)b->grids.size() <= std::max(1, b->cluster.nclusters))
+    // run, and so does every tube of a batch whose clusters (register form)
+    // are resident at once (measured, fast_math: 2 and 4 tubes 1.36 us per
+    // step against 2.6 on the strips; past one wave of clusters the strips win)
+    const int n = (int)b->grids.size();
+    if (shape_fits(b, cluster_shape()) && (n == 1 || (b->cluster.form != 0 && n <= b->cluster.nclusters)))
         return cluster_shape();
     int64_t cells = 0;
     for (const TubeGrid& g : b->grids) cells += g.dims.interior_cells;
