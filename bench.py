@@ -516,12 +516,14 @@ def run_b200(args, rank, world):
         # per-column data (wall rows, gap-fill extents, segment ids: 20 B per
         # tube column, 4 B per section's minor axis); the descriptor plane
         # (1 B per padded cell) and tables (8 KiB) go up (every batch without
-        # the coupled wall has them, in either arithmetic); the source table
-        # (4 B per step) goes up; the code plane (1 B per padded cell) and the
-        # traces come back
+        # the coupled wall has them, in either arithmetic); each distinct
+        # source table (4 B per step; the tubes here share one) goes up once;
+        # the code plane (1 B per padded cell) and the traces come back
         padded = [d["frame_h"] * ((d["frame_w"] + 31) // 32 * 32) for d in batch.dims]
-        h2d = sum(20 * d["tube_length_cells"] + 4 * g.struct.n_sections + 4 * sim_steps + pc + 8192
-                  for d, g, pc in zip(batch.dims, gs, padded))
+        sources = {(p.source_type, p.srate_mul, p.gauss_peak_s, p.gauss_width_s, p.gauss_amp, p.sine_freq_hz,
+                    p.sine_amp) for p in ps}
+        h2d = 4 * sim_steps * len(sources) + sum(20 * d["tube_length_cells"] + 4 * g.struct.n_sections + pc + 8192
+                                                 for d, g, pc in zip(batch.dims, gs, padded))
         d2h = 4 * sim_steps * args.tubes + sum(padded)
         e2e = {"value": round(job_cells * sim_steps / (e2e_step / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_step, 2)}

@@ -333,6 +333,25 @@ def test_exact_two_step_small_and_open_frames(cuda_ok):
     assert np.all(np.isfinite(ref)) and np.all(np.abs(ref).max(axis=1) > 0)
 
 
+def test_batch_tubes_keep_their_own_source_tables(cuda_ok):
+    """Tubes with the same source parameters, time step and run length share
+    one device table; any difference (source type, Gaussian width, sine,
+    sample rate) gives a tube its own.  Every row equals the FP32 oracle."""
+    kws = [dict(cross_sectional_shape=2),
+           dict(cross_sectional_shape=2),
+           dict(cross_sectional_shape=2, source_type=0),
+           dict(cross_sectional_shape=2, source_type=3, gauss_peak_s=5e-4, gauss_width_s=1e-4),
+           dict(cross_sectional_shape=2, srate_mul=30),
+           dict(cross_sectional_shape=2, gauss_width_s=2e-4)]
+    tubes = [S.batch_tube(i)[:2] for i in range(len(kws))]
+    b = V.Batch([V.params(**k) for k in kws], [V.Geometry(L, A) for L, A in tubes])
+    tr = b.run(300)
+    b.close()
+    for i, k in enumerate(kws):
+        assert np.array_equal(tr[i], O.run(O.params(**k), O.Geometry(*tubes[i]), 300, "f32")), f"tube {i}"
+    assert not np.array_equal(tr[0], tr[5])
+
+
 def test_batch_creation_reports_a_bad_tube_among_many(cuda_ok):
     """The host builds the tubes' maps on several threads; an unusable area
     function in the middle of a batch still fails the creation with

@@ -20,6 +20,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <map>
 #include <vector>
 
 namespace vsb {
@@ -231,12 +232,30 @@ void upload_sources(vs_batch* b, int64_t need) {
         std::memcpy(&p, &g.src_params, sizeof(p));
         build_source(&p, g.dt, need, g.source);
     });
+    // identical tables (the same source type and parameters, time step and
+    // length) are uploaded once and shared by their tubes
     size_t total = 0;
     std::vector<size_t> off(b->grids.size(), 0);
+    std::vector<bool> upload(b->grids.size(), false);
+    std::map<std::string, size_t> offset_of;
     for (size_t i = 0; i < b->grids.size(); ++i) {
         const TubeGrid& g = b->grids[i];
         if (g.tmm) continue;
+        vs_params p;
+        std::memcpy(&p, &g.src_params, sizeof(p));
+        const float key_f[7] = {p.sine_amp, p.sine_freq_hz, p.gauss_amp, p.gauss_peak_s, p.gauss_width_s, g.dt,
+                                (float)p.source_type};
+        const int64_t len = (int64_t)g.source.size();
+        std::string key(reinterpret_cast<const char*>(key_f), sizeof(key_f));
+        key.append(reinterpret_cast<const char*>(&len), sizeof(len));
+        const auto it = offset_of.find(key);
+        if (it != offset_of.end()) {
+            off[i] = it->second;
+            continue;
+        }
         off[i] = total;
+        offset_of.emplace(key, total);
+        upload[i] = true;
         total += align_up(g.source.size() * sizeof(float));
     }
     if (b->src_arena) { cudaFree(b->src_arena); b->src_arena = nullptr; }
@@ -246,8 +265,9 @@ void upload_sources(vs_batch* b, int64_t need) {
         TubeDev& t = b->h_tubes[i];
         if (g.tmm) { t.src = nullptr; t.src_len = 0; b->src_len[i] = INT64_MAX; continue; }
         float* dst = (float*)((char*)b->src_arena + off[i]);
-        ck(cudaMemcpy(dst, g.source.data(), g.source.size() * sizeof(float), cudaMemcpyHostToDevice),
-           "upload source table");
+        if (upload[i])
+            ck(cudaMemcpy(dst, g.source.data(), g.source.size() * sizeof(float), cudaMemcpyHostToDevice),
+               "upload source table");
         t.src = dst;
         t.src_len = (int64_t)g.source.size();
         b->src_len[i] = t.src_len;
