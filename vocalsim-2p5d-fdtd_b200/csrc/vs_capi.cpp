@@ -142,7 +142,7 @@ struct vs_batch {
     size_t exc_bytes = 0;
     Tile* d_hist_tiles = nullptr;
     int n_hist_tiles = 0;
-    Tile* d_hist2_tiles = nullptr;         // two-step history shape (fast_math)
+    Tile* d_hist2_tiles = nullptr;         // two-step history shape (fast_math batches)
     int n_hist2_tiles = 0;
     Tile* d_odd_tiles = nullptr;           // single-step tiles beside a two-step shape
     char* x_mem = nullptr;                 // third state set of the two-step shapes (TubeDev::X, tmm_x)

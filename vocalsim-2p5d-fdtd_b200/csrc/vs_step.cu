@@ -630,8 +630,9 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 }
 
 // ---------------------------------------------------------------------------
-// Two-step quad-strip kernel (fast_math, no coupled wall):
-// every strip advances TWO time steps per launch.  A lane holds NC adjacent
+// Two-step quad-strip kernel (no coupled wall; fast_math, and with EXACT the
+// reference arithmetic): every strip advances TWO time steps per launch.  A
+// lane holds NC adjacent
 // columns (NC = 4 or 2), a warp 32 NC columns, of which lanes 1..30 commit.
 // Step n runs the quad-strip row pipeline over rows r0-2 .. rlast+1 and all
 // columns of the warp; step n+1 follows one row behind on the values step n
@@ -642,7 +643,10 @@ quad_kernel(const TubeDev* __restrict__ tubes, const Tile* __restrict__ items, i
 // and written once.  The step n+2 state goes to the other of two buffer sets
 // (the parity set of step n and a third set TubeDev::X, alternating per
 // launch); per cell and step the arithmetic is that of the quad-strip kernel
-// in the reciprocal form, so the values are those of two single steps.
+// in the reciprocal form, or with EXACT that of the strip kernel (the IEEE
+// divides, the neighbourhood's factors from the descriptor tables, on the
+// rows the tile's p_rows / v_beta1 masks mark), so the values are those of
+// two single steps.
 // Tile masks classify the extended region (rows from r0-2 / r0-1, columns
 // c0 + NC/2 .. c0 + 32 NC - NC/2 - 1): bit j of v_generic = row r0-1+j.
 // HIST: the adjoint's segment recomputation; the committed cells' state
