@@ -44,7 +44,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 def workload_config(n_tubes: int = N_TUBES, sim_steps: int = SIM_STEPS) -> dict:
-    """The workload both arms measure."""
+    """The workload both arms measure: the 256-tube batch, 50 ms at fs = 44100 x 15."""
     return {"workload": f"batched forward, {n_tubes} seeded tubes 12-20 cm x 2-4 cm, 3:1 elliptical, Gaussian, PML 6, "
                         f"{sim_steps} steps (50 ms) at fs 661.5 kHz; one step = one full forward",
             "tubes": n_tubes, "sim_steps": sim_steps}
@@ -528,7 +528,7 @@ def run_b200(args, rank, world):
         e2e = {"value": round(job_cells * sim_steps / (e2e_step / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_step, 2)}
 
-    # ---- plain single-tube GPU path for the batched-vs-single ratio
+    # ---- plain single-tube GPU path (the uniform 17.5 x 3 cm tube) for the batched-vs-single ratio
     single = None
     if not args.no_single:
         from vocalsim_b200 import synthetic as S
@@ -576,8 +576,8 @@ def run_b200(args, rank, world):
         single["step_kernels_shape"] = best_k
         single["cluster_speedup"] = round(best_ms / sms, 2)
 
-    # ---- BASELINE config 2: a 1 s vowel tube with the two-mass source (800 Pa)
-    config2 = None
+    # ---- a 1 s vowel tube with the two-mass source (800 Pa)
+    vowel_1s = None
     if not args.no_single:
         from vocalsim_b200 import synthetic as S
         n2 = 661500
@@ -592,7 +592,7 @@ def run_b200(args, rank, world):
         b.record(stream)
         torch.cuda.synchronize()
         ms2 = a.elapsed_time(b)
-        config2 = {"workload": "vowel tube (seed 0, 44 sections, 3:1 elliptical), two-mass source 800 Pa in double, "
+        vowel_1s = {"workload": "vowel tube (seed 0, 44 sections, 3:1 elliptical), two-mass source 800 Pa in double, "
                                f"1 s simulated ({n2} steps), one cluster-kernel launch",
                    "interior_cells": s2.dims["interior_cells"],
                    "value": round(s2.dims["interior_cells"] * n2 / (ms2 / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
@@ -653,7 +653,7 @@ def run_b200(args, rank, world):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "single_tube": single,
-        "config2": config2,
+        "vowel_1s": vowel_1s,
         # against the library's default single-tube path (the cluster kernel), and
         # against the same step kernels the batch uses, run on the one tube
         "batched_vs_single": round(value / world / single["value"], 2) if single else None,

@@ -1,4 +1,4 @@
-"""BASELINE config 3 at full length, in the arithmetic the bench measures.
+"""The 256-tube batch workload at full length (50 ms), in the arithmetic the bench measures.
 
 Eight tubes of the 256-tube batch -- the two shortest, the two longest, the
 two narrowest and the two widest (seeds 156, 31, 222, 125, 183, 161, 166,
@@ -43,7 +43,7 @@ def runs(cuda_ok):
 
 
 @pytest.mark.parametrize("i", range(len(SEEDS)), ids=[f"seed{s}" for s in SEEDS])
-def test_config3_tube_rel_l2_vs_double(runs, i):
+def test_batch256_tube_rel_l2_vs_double(runs, i):
     gpu, ref = runs
     a, b = gpu[i].astype(np.float64), ref[i]
     err = float(np.linalg.norm(a - b) / np.linalg.norm(b))
@@ -51,7 +51,7 @@ def test_config3_tube_rel_l2_vs_double(runs, i):
 
 
 @pytest.mark.parametrize("i", range(len(SEEDS)), ids=[f"seed{s}" for s in SEEDS])
-def test_config3_tube_formants_within_1hz(runs, i):
+def test_batch256_tube_formants_within_1hz(runs, i):
     gpu, ref = runs
     got = formants_bw(gpu[i].astype(np.float64), FS, 4)[1]
     want = formants_bw(ref[i], FS, 4)[1]

@@ -101,7 +101,7 @@ def test_cluster_fast_math_equals_the_strip_kernels(name, cuda_ok):
     assert np.array_equal(got, ref), f"differs from step {int(np.argmax(got != ref))}"
 
 
-def test_cluster_full_length_config1_equals_step_kernels(cuda_ok):
+def test_cluster_full_length_uniform_tube_equals_step_kernels(cuda_ok):
     """The uniform 17.5 x 3 cm tube over 33 075 steps: cluster == strip kernel, bit for bit."""
     kw, geo = CASES["uniform_gauss"]
     a = cluster_batch(kw, geo).run(33075)[0]

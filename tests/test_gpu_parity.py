@@ -32,7 +32,7 @@ def both(kw, L=None, A=None):
 
 
 CASES = {
-    # BASELINE config 1 geometry: 17.5 cm x 3 cm, uniform 2 cm depth, mu 0.005
+    # the uniform tube: 17.5 cm x 3 cm, uniform 2 cm depth, mu 0.005
     "uniform_gauss": (dict(mu3d=0.005, uniform_depth_m=0.02), S.uniform_tube()),
     "uniform_gauss_std_explicit_listener": (
         dict(mu3d=0.005, uniform_depth_m=0.02, source_type=3, gauss_peak_s=5e-4, gauss_width_s=1e-4,
@@ -117,37 +117,37 @@ def test_batch_rows_equal_single_tubes_and_oracle(cuda_ok):
         assert np.array_equal(tr[i], O.run(O.params(**kws[i]), O.Geometry(*tubes[i]), 600, "f32"))
 
 
-CONFIG1 = dict(mu3d=0.005, uniform_depth_m=0.02, num_steps=33075)
+UNIFORM_TUBE = dict(mu3d=0.005, uniform_depth_m=0.02, num_steps=33075)
 _REF64 = {}
 
 
-def _config1_ref64():
+def _uniform_tube_ref64():
     if "tr" not in _REF64:
         L, A = S.uniform_tube()
-        _REF64["tr"] = O.run(O.params(**CONFIG1), O.Geometry(L, A), 33075, "f64")
+        _REF64["tr"] = O.run(O.params(**UNIFORM_TUBE), O.Geometry(L, A), 33075, "f64")
     return _REF64["tr"]
 
 
 @pytest.mark.parametrize("fast", [0, 1])
-def test_config1_full_length_rel_l2_vs_double(fast, cuda_ok):
+def test_uniform_tube_full_length_rel_l2_vs_double(fast, cuda_ok):
     """The uniform 17.5 x 3 cm tube with 2 cm depth, 33 075 steps (50 ms):
     FP32 GPU trace vs the FP64 restatement, in the reference arithmetic and
     in the reciprocal form (fast_math)."""
     L, A = S.uniform_tube()
-    tr = V.Solver(V.params(fast_math=fast, **CONFIG1), V.Geometry(L, A)).run(33075)
-    assert rel_l2(tr, _config1_ref64()) <= REL_L2_TOL
+    tr = V.Solver(V.params(fast_math=fast, **UNIFORM_TUBE), V.Geometry(L, A)).run(33075)
+    assert rel_l2(tr, _uniform_tube_ref64()) <= REL_L2_TOL
 
 
 @pytest.mark.parametrize("fast", [0, 1])
-def test_config1_formants_within_1hz(fast, cuda_ok):
+def test_uniform_tube_formants_within_1hz(fast, cuda_ok):
     """F1-F4 of the 50 ms trace (the reference's get_formants_bw, restated in
     oracle/formants.py) against those of the FP64 trace: within 1 Hz."""
     from formants import formants_bw
     L, A = S.uniform_tube()
-    tr = V.Solver(V.params(fast_math=fast, **CONFIG1), V.Geometry(L, A)).run(33075)
+    tr = V.Solver(V.params(fast_math=fast, **UNIFORM_TUBE), V.Geometry(L, A)).run(33075)
     fs = 44100.0 * 15
     got = formants_bw(tr.astype(np.float64), fs, 4)[1]
-    ref = formants_bw(_config1_ref64(), fs, 4)[1]
+    ref = formants_bw(_uniform_tube_ref64(), fs, 4)[1]
     assert np.all(got > 0) and np.all(np.abs(got - ref) <= 1.0), (got, ref)
 
 

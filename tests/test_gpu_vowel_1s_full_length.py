@@ -1,4 +1,4 @@
-"""BASELINE config 2 at full length: the 1 s vowel tube (seed 0, 44 sections,
+"""The 1 s vowel tube at full length (seed 0, 44 sections,
 3:1 elliptical, two-mass source at 800 Pa), 661 500 steps, on the default
 single-tube path (the cluster kernel).
 
@@ -58,7 +58,7 @@ def runs(cuda_ok):
 
 
 @pytest.mark.parametrize("tmm64", [0, 1])
-def test_config2_gpu_equals_the_fp32_system_for_one_second(runs, tmm64):
+def test_vowel_1s_gpu_equals_the_fp32_system_for_one_second(runs, tmm64):
     gpu, orc = runs
     ref = orc["f32_tmm64" if tmm64 else "f32_tmm32"]
     got = gpu[(tmm64, 0)]
@@ -66,7 +66,7 @@ def test_config2_gpu_equals_the_fp32_system_for_one_second(runs, tmm64):
     assert np.all(np.isfinite(got)) and np.abs(got).max() > 0
 
 
-def test_config2_double_model_formants_within_1hz(runs):
+def test_vowel_1s_double_model_formants_within_1hz(runs):
     gpu, orc = runs
     want = formants_bw(orc["f64"], FS, 4)[1]
     for fast in (0, 1):
@@ -74,7 +74,7 @@ def test_config2_double_model_formants_within_1hz(runs):
         assert np.all(want > 0) and np.all(np.abs(got - want) <= 1.0), (fast, got, want)
 
 
-def test_config2_precision_floor(runs):
+def test_vowel_1s_precision_floor(runs):
     gpu, orc = runs
     d = orc["f64"]
     floor = rel(orc["f32_tmm64"], d)

@@ -71,7 +71,7 @@ def test_synthetic_tubes(seed):
     compare(dict(cross_sectional_shape=2, source_type=2), Lv, Av)
 
 
-def test_uniform_tube_config1():
+def test_uniform_tube_maps():
     L, A = S.uniform_tube()
     m = compare(dict(mu3d=0.005, uniform_depth_m=0.02), L, A)
     d = m["dims"]
